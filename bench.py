@@ -1,0 +1,337 @@
+"""Benchmark: Mpixel/s of Voronoi + Delaunay + per-pixel assignment, bit-exact.
+
+Workload (one step = one image through the whole pipeline):
+  4096 x 4096 image, 200 000 distinct uniform random seeds (seeded), border
+  padding 16 (detection canvas 4128 x 4128), reference-CUDA Voronoi
+  semantics -- the plain GPU drop-in configuration.  A clustered variant
+  (64 Gaussian blobs, sigma 40 px) of the same size is timed too and reported
+  beside it.
+
+  value  device-resident throughput: seeds already on the device, (H, W, 3)
+         output left on the device (idl_triangulate_device), CUDA events on the
+         library's stream around K steps.
+  e2e    the public drop-in call triangulate(W, H, seeds, as_arrays=True) with
+         seeds in pinned host memory: host->device copy of the seeds, all
+         stages, device->host copy of the (H, W, 3) grid and the triangles.
+
+Multi-GPU (torchrun): every rank triangulates its own image per step (replicas,
+no collective on the data path); the time is the max over ranks.
+
+`--impl reference` times the reference algorithm on the host CPU cores (the
+oracle port of src/cuda/voronoi.cu + triangulation.cu, OpenMP) on a bounded
+sample of the same workload, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W = H = 4096
+N_SEEDS = 200_000
+PADDING = 16
+MODE = "reference"
+METRIC = "Mpixel/s Voronoi+Delaunay+assign (bit-exact)"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(sample_rows: int = 0):
+    """Reference algorithm on the host cores: full Jacobi + detection on the
+    padded canvas, the reference's per-pixel assignment on a sample of rows,
+    extrapolated to the image.  Returns (Mpix/s, seconds, description)."""
+    import oracle
+    from integer_delauney_b200.workloads import uniform
+
+    threads = oracle.num_threads()
+    rows = sample_rows or max(4, min(64, threads))
+    seeds = uniform(W, H, N_SEEDS, seed=0)
+    s = oracle.sort_seeds(seeds, W, H)
+    xs, ys = np.ascontiguousarray(s[:, 0]), np.ascontiguousarray(s[:, 1])
+    Wd, Hd = W + 2 * PADDING, H + 2 * PADDING
+    t0 = time.perf_counter()
+    lab = np.full((Hd, Wd), -1, dtype=np.int32)
+    lab[ys + PADDING, xs + PADDING] = np.arange(len(s), dtype=np.int32)
+    lab, passes = oracle.jacobi_from(Wd, Hd, xs + PADDING, ys + PADDING, lab)
+    t1 = time.perf_counter()
+    tris = oracle.detect(lab, xs + PADDING, ys + PADDING, PADDING)
+    t2 = time.perf_counter()
+    y0 = H // 2 - rows // 2
+    oracle.assign_rows(W, H, xs, ys, tris, y0, y0 + rows)
+    t3 = time.perf_counter()
+    est = (t1 - t0) + (t2 - t1) + (t3 - t2) * (H / rows)
+    desc = (f"oracle port, {threads} threads: full Jacobi ({passes} passes) + detection on the "
+            f"{Wd}x{Hd} canvas, reference per-pixel assignment on {rows} of {H} rows "
+            f"(extrapolated); measured {t3 - t0:.1f} s")
+    return W * H / est / 1e6, est, desc, threads
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        cpu_baseline(args.ref_rows)
+    vals, secs = [], []
+    desc, threads = "", 0
+    for _ in range(args.steps):
+        v, est, desc, threads = cpu_baseline(args.ref_rows)
+        vals.append(v)
+        secs.append(est)
+    value = statistics.median(vals)
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": statistics.median(secs) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": f"triangulate {W}x{H}, {N_SEEDS} uniform seeds, P={PADDING}, reference mode",
+                   "parallelism": f"replicas x{world}"},
+        "cpu_baseline": {"value": value, "unit": "Mpixel/s", "cores": threads, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world):
+    import torch
+
+    from integer_delauney_b200 import _capi
+    from integer_delauney_b200 import _delauney_cuda as cu
+    from integer_delauney_b200.workloads import clustered, uniform
+
+    dev = rank % max(1, torch.cuda.device_count())
+    torch.cuda.set_device(dev)
+    lib = _capi.load()
+    ctx = _capi.context_for(dev)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+
+    def device_case(seeds_np):
+        d_seeds = torch.from_numpy(seeds_np).cuda()
+        d_out = torch.empty((H, W, 3), dtype=torch.int32, device="cuda")
+        return d_seeds, d_out
+
+    def step_device(d_seeds, d_out):
+        _capi.check(lib.idl_triangulate_device(ctx.handle, W, H, d_seeds.data_ptr(), d_seeds.shape[0], PADDING,
+                                               _capi.mode_id(MODE), d_out.data_ptr(), None))
+
+    def time_device(seeds_np, steps, warmup, profile=False):
+        d_seeds, d_out = device_case(seeds_np)
+        for _ in range(warmup):
+            step_device(d_seeds, d_out)
+        ctx.set_profiling(profile)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        profs = []
+        launches0 = lib.idl_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(dev) as clk:
+            e0.record(stream)
+            for _ in range(steps):
+                step_device(d_seeds, d_out)
+                if profile:
+                    profs.append(ctx.last_profile())
+            e1.record(stream)
+            torch.cuda.synchronize()
+        launches = lib.idl_launch_count() - launches0
+        ms = e0.elapsed_time(e1)
+        ctx.set_profiling(False)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, profs, clk.summary(), launches
+
+    seeds_u = uniform(W, H, N_SEEDS, seed=rank)
+    ms, profs, clocks, launches = time_device(seeds_u, args.steps, args.warmup, profile=True)
+    value = world * W * H * args.steps / (ms / 1e3) / 1e6
+
+    # stage breakdown and roofline of the dominant stage
+    keys = ["seeds_ms", "propagate_ms", "detect_ms", "dedup_ms", "assign_ms", "compose_ms"]
+    stage = {k: statistics.mean(p[k] for p in profs) for k in keys}
+    p0 = profs[-1]
+    hbm, peak_kind = _peaks()
+    inner_px = p0["tile_w"] * p0["tile_h"]
+    # propagation: 8 B per canvas pixel per HBM round trip (read + write a
+    # 4-byte label), over the tiles the rounds actually processed
+    prop_bytes = 8.0 * inner_px * statistics.mean(p["tiles"] for p in profs)
+    prop_gbs = prop_bytes / (stage["propagate_ms"] / 1e3) / 1e9
+    canvas = p0["canvas_px"]
+    detect_gbs = 4.0 * canvas / (stage["detect_ms"] / 1e3) / 1e9
+    assign_gbs = 8.0 * W * H / (stage["assign_ms"] / 1e3) / 1e9
+    compose_gbs = 20.0 * W * H / (stage["compose_ms"] / 1e3) / 1e9
+    dominant = max(keys, key=lambda k: stage[k])
+    roof = {"propagate_ms": prop_gbs, "detect_ms": detect_gbs, "assign_ms": assign_gbs,
+            "compose_ms": compose_gbs}
+    dom_kernel = dominant if dominant in roof else "propagate_ms"
+    achieved = roof[dom_kernel]
+
+    # clustered variant (same size), device path
+    seeds_c = clustered(W, H, N_SEEDS, seed=rank)
+    c_steps = max(1, args.steps // 2)
+    ms_c, profs_c, _, _ = time_device(seeds_c, c_steps, 1, profile=True)
+    value_c = world * W * H * c_steps / (ms_c / 1e3) / 1e6
+
+    # end to end through the public drop-in call, pinned host seeds
+    pinned = torch.from_numpy(seeds_u).pin_memory()
+    seeds_host = pinned.numpy()
+    for _ in range(max(1, args.warmup)):
+        cu.triangulate(W, H, seeds_host, PADDING, as_arrays=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n_tri = 0
+    e_steps = max(1, args.steps // 2)
+    e0.record(stream)
+    for _ in range(e_steps):
+        verts, grid = cu.triangulate(W, H, seeds_host, PADDING, as_arrays=True)
+        n_tri = len(verts)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms_e], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_e = float(t.item())
+    e2e = world * W * H * e_steps / (ms_e / 1e3) / 1e6
+
+    if rank != 0:
+        return
+    base = None
+    if not args.no_cpu_baseline:
+        v, est, desc, threads = cpu_baseline(args.ref_rows)
+        base = {"value": v, "unit": "Mpixel/s", "cores": threads, "kind": "port", "sample": desc}
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": f"triangulate {W}x{H}, {N_SEEDS} uniform seeds (rng = rank), P={PADDING}, "
+                               f"voronoi_mode={MODE}",
+                   "global_batch": world, "parallelism": f"replicas x{world}",
+                   "l2": "working set > L2 (label planes 2 x 68 MB, output 201 MB); no flush"},
+        "stages_ms": {k[:-3]: round(v, 4) for k, v in stage.items()},
+        "propagation": {"passes": p0["passes"], "rounds": p0["rounds"], "tiles": p0["tiles"],
+                        "tile": [p0["tile_w"], p0["tile_h"]], "steps_per_round": p0["steps_per_round"]},
+        "roofline": {"bound": "hbm", "kernel": dom_kernel[:-3], "achieved": achieved, "peak": hbm,
+                     "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
+                     "per_stage_gbs": {k[:-3]: v for k, v in roof.items()}},
+        "clustered": {"value": value_c, "unit": "Mpixel/s", "ms_per_step": ms_c / c_steps,
+                      "passes": profs_c[-1]["passes"], "rounds": profs_c[-1]["rounds"],
+                      "stages_ms": {k[:-3]: round(statistics.mean(p[k] for p in profs_c), 4) for k in keys}},
+        "e2e": {"value": e2e, "unit": "Mpixel/s", "ms_per_step": ms_e / e_steps,
+                "h2d_bytes_per_step": int(seeds_u.nbytes),
+                "d2h_bytes_per_step": int(W * H * 12 + n_tri * 20)},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "cpu_baseline": base,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--ref-rows", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

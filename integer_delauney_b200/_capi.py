@@ -1,0 +1,174 @@
+"""ctypes binding of the C ABI in include/idelaunay.h.
+
+Loads the in-tree libidelaunay.so.  There is no fallback: if the library is
+missing, importing anything that needs it raises ImportError naming the build
+command, the same way ``from delauney import _delauney_cuda`` fails when the
+reference's extension was not built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libidelaunay.so")
+
+IDL_OK = 0
+IDL_ERR_INVALID = 1
+IDL_ERR_CUDA = 2
+IDL_ERR_STATE = 3
+IDL_ERR_INTERNAL = 4
+
+MODE_REFERENCE = 0
+MODE_NUMPY = 1
+MODE_EXACT = 2
+MODES = {"reference": MODE_REFERENCE, "numpy": MODE_NUMPY, "exact": MODE_EXACT}
+
+AUTO_BORDER_PADDING = -1
+DEFAULT_BORDER_PADDING = 16
+
+T_DETECT_MS, T_DEDUP_MS, T_ASSIGN_MS, T_BFS_MS, T_BFS_ITERS, T_COUNT = range(6)
+
+_vp = ctypes.c_void_p
+_i32 = ctypes.c_int
+_i64 = ctypes.c_int64
+_pi64 = ctypes.POINTER(ctypes.c_int64)
+
+# name -> (restype, argtypes); every declaration of include/idelaunay.h
+SIGNATURES = {
+    "idl_last_error": (ctypes.c_char_p, []),
+    "idl_version": (_i32, []),
+    "idl_launch_count": (ctypes.c_longlong, []),
+    "idl_context_create": (_i32, [_i32, ctypes.POINTER(_vp)]),
+    "idl_context_destroy": (_i32, [_vp]),
+    "idl_context_set_stream": (_i32, [_vp, _vp]),
+    "idl_context_synchronize": (_i32, [_vp]),
+    "idl_context_workspace_bytes": (_i32, [_vp, _pi64]),
+    "idl_context_set_profiling": (_i32, [_vp, _i32]),
+    "idl_context_last_profile": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _i32]),
+    "idl_voronoi": (_i32, [_vp, _i32, _i32, _vp, _i64, _i32, _vp, _pi64]),
+    "idl_triangulate": (_i32, [_vp, _i32, _i32, _vp, _i64, _vp, _i32, _i32, _vp, _pi64, _vp, _vp]),
+    "idl_get_triangles": (_i32, [_vp, _vp, _i64]),
+    "idl_triangulate_device": (_i32, [_vp, _i32, _i32, _vp, _i64, _i32, _i32, _vp, _pi64]),
+    "idl_triangles_device": (_i32, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
+}
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def load():
+    """Load libidelaunay.so (once) and declare every entry point."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is not built; run `python -m integer_delauney_b200.build` "
+                "(nvcc, sm_100a) first")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name, None)
+            if fn is None:
+                continue
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def last_error() -> str:
+    msg = load().idl_last_error()
+    return msg.decode(errors="replace") if msg else ""
+
+
+def check(status: int) -> None:
+    """Map a status code to the reference's exception types."""
+    if status == IDL_OK:
+        return
+    msg = last_error()
+    if status == IDL_ERR_INVALID:
+        raise ValueError(msg)
+    raise RuntimeError(msg)
+
+
+def mode_id(mode) -> int:
+    if isinstance(mode, str):
+        try:
+            return MODES[mode]
+        except KeyError:
+            raise ValueError(f"voronoi_mode must be one of {sorted(MODES)}, not {mode!r}") from None
+    return int(mode)
+
+
+def ptr(a) -> int | None:
+    """Raw data pointer of a numpy array or torch tensor (None for None)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+class Context:
+    """One idl_context: a device, a stream and the grow-only workspace."""
+
+    def __init__(self, device: int = -1):
+        self._lib = load()
+        h = _vp()
+        check(self._lib.idl_context_create(int(device), ctypes.byref(h)))
+        self.handle = h
+        self.lock = threading.RLock()
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        check(self._lib.idl_context_set_stream(self.handle, _vp(stream_handle or 0)))
+
+    def synchronize(self) -> None:
+        check(self._lib.idl_context_synchronize(self.handle))
+
+    def set_profiling(self, enable: bool) -> None:
+        check(self._lib.idl_context_set_profiling(self.handle, 1 if enable else 0))
+
+    PROFILE_KEYS = ("seeds_ms", "propagate_ms", "detect_ms", "dedup_ms", "assign_ms", "compose_ms", "rounds",
+                    "tiles", "passes", "tile_w", "tile_h", "steps_per_round", "canvas_px", "image_px",
+                    "n_triangles")
+
+    def last_profile(self) -> dict:
+        buf = (ctypes.c_double * len(self.PROFILE_KEYS))()
+        check(self._lib.idl_context_last_profile(self.handle, buf, len(self.PROFILE_KEYS)))
+        return {k: float(buf[i]) for i, k in enumerate(self.PROFILE_KEYS)}
+
+    def workspace_bytes(self) -> int:
+        v = ctypes.c_int64(0)
+        check(self._lib.idl_context_workspace_bytes(self.handle, ctypes.byref(v)))
+        return int(v.value)
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self._lib.idl_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_contexts: dict[int, Context] = {}
+_ctx_lock = threading.Lock()
+
+
+def context_for(device: int) -> Context:
+    with _ctx_lock:
+        c = _contexts.get(device)
+        if c is None:
+            c = Context(device)
+            _contexts[device] = c
+        return c

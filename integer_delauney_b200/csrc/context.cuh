@@ -1,0 +1,187 @@
+// Per-device context: stream, grow-only device workspace and the small block
+// of device-side counters one pipeline run uses.
+//
+// The reference allocates every intermediate per call and frees it on return
+// (src/cuda/voronoi.cu:87-91, src/cuda/triangulation.cu:271-351); a cudaFree
+// synchronises the device, so that design pays a full drain per buffer.  A
+// context instead keeps each workspace buffer at its high-water mark and
+// reuses it, so a steady stream of calls allocates nothing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+
+#include "common.cuh"
+
+namespace idl {
+
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+
+    template <class T>
+    T* as() const { return static_cast<T*>(ptr); }
+
+    // Grow to at least `need` bytes (contents are not preserved).
+    void ensure(size_t need)
+    {
+        if (need <= bytes) return;
+        release();
+        if (need == 0) return;
+        IDL_CUDA(cudaMalloc(&ptr, need));
+        bytes = need;
+    }
+    void release() noexcept
+    {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+// Device-side counters and flags of one pipeline run.  Lives in device memory;
+// a pinned host mirror receives it when the host needs a count.
+struct Scalars {
+    int64_t n_triangles;      // unique triangles after dedup
+    int64_t n_inserted;       // keys inserted into the hash table
+    int64_t last_change;      // last propagation step (0-based) that changed a cell
+    int32_t err_oob;          // a seed lay outside the canvas
+    int32_t err_dup;          // two seeds share a pixel
+    int32_t err_label;        // a caller-supplied label was outside [-1, n)
+    int32_t overflow;         // hash table over its load limit or probe bound
+    int32_t max_side;         // longest triangle side, float-truncated (triangulation.cu:355-368)
+    int32_t pad_;
+};
+
+struct Timing {
+    cudaEvent_t ev[8] = {};
+    bool on = false;
+};
+
+// Stage boundaries of the last pipeline run, recorded on the context's stream
+// when profiling is enabled (idl_context_set_profiling).
+enum ProfMark { PM_START = 0, PM_SEEDS, PM_PROPAGATE, PM_DETECT, PM_DEDUP, PM_ASSIGN, PM_COMPOSE, PM_COUNT };
+
+struct Profile {
+    bool enabled = false;
+    bool valid = false;
+    cudaEvent_t ev[PM_COUNT] = {};
+    bool recorded[PM_COUNT] = {};
+    int64_t rounds = 0;           // propagation rounds launched with work
+    int64_t tiles = 0;            // tiles processed over all rounds
+    int64_t passes = 0;           // propagation passes (reference semantics)
+    int64_t canvas_px = 0;        // detection canvas pixels
+    int64_t image_px = 0;         // output pixels
+    int64_t n_triangles = 0;
+    int tile_w = 0, tile_h = 0, steps_per_round = 0;
+};
+
+struct Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 148;
+
+    // seeds
+    DevBuf seeds_in;      // n x 2 int32 as the caller passed them
+    DevBuf xs, ys;        // sorted seed coordinates (image space)
+    DevBuf pos;           // sorted seed positions on the detection canvas, packed
+    DevBuf bitmap;        // canvas occupancy bits, column major, for the (x, y) sort
+    DevBuf scan_a, scan_b, scan_c;  // scan scratch
+
+    // propagation
+    DevBuf lab[2];        // label planes, pitch x Hd int32, ping-pong
+    DevBuf tiles[2];      // active tile lists
+    DevBuf stamps;        // per-tile "already listed for round r" marks
+    DevBuf counts;        // per-round list lengths
+    int32_t stamp_epoch = 0;
+
+    // topology
+    DevBuf hkeys, hvals;  // hash table of triangle keys -> first witness
+    DevBuf ukeys, uvals;  // compacted unique keys
+    DevBuf cnt, off, fill, grp;  // group-by-smallest-vertex ranking
+    DevBuf tris;          // n_tri x 5 int32 (x, y, a, b, c)
+    int64_t hash_cap = 0;
+
+    // assignment / output
+    DevBuf tgrid;         // W x H int32 triangle ids
+    DevBuf vgrid;         // caller-supplied Voronoi grid (GridTriangulation at P = 0)
+    DevBuf outgrid;       // H x W x 3 staging for host-pointer calls
+    DevBuf padded;        // padded Voronoi grid for compute_debug
+
+    DevBuf scalars;       // one Scalars
+    Scalars* host_sc = nullptr;  // pinned mirror
+
+    int64_t last_n_tri = 0;      // triangles of the last triangulation (host copy)
+    bool have_result = false;
+
+    Timing timing;
+    Profile prof;
+
+    void mark(ProfMark m)
+    {
+        if (!prof.enabled) return;
+        if (!prof.ev[m]) IDL_CUDA(cudaEventCreate(&prof.ev[m]));
+        IDL_CUDA(cudaEventRecord(prof.ev[m], stream));
+        prof.recorded[m] = true;
+    }
+
+    Scalars* sc() const { return scalars.as<Scalars>(); }
+    size_t workspace_bytes() const;
+    void fetch_scalars();        // D2H of the Scalars block + stream sync
+    ~Context();
+};
+
+// RAII: make the context's device current for the duration of a call.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) IDL_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// ---- pipeline pieces (one .cu each) -----------------------------------
+
+// Exclusive scan of n int32 values in place semantics: out[i] = sum(in[0..i)),
+// and out[n] = total.  `out` must hold n + 1 values.  Uses ctx scan scratch.
+void exclusive_scan(Context& C, const int32_t* in, int32_t* out, int64_t n);
+
+// Validate and sort seeds on the device (seeds.cu).  Reads C.seeds_in (n x 2),
+// writes C.xs / C.ys (sorted, image space) and C.pos (detection canvas, shifted
+// by P).  Throws IDL_ERR_INVALID with the reference's messages.
+void sort_seeds_device(Context& C, int W, int H, int64_t n, int P);
+
+// Stage (a) on the Wd x Hd detection canvas whose labels are in C.lab[0]
+// (both planes must hold the same starting state).  Returns the pass count
+// (propagate.cu).  `first_tiles`: nullptr = every tile starts active;
+// otherwise a device list of `n_first` tile ids.
+struct Canvas {
+    int Wd, Hd, pitch;
+};
+int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos);
+
+// Seed the label planes: fill with UNDEF and write seed ids (propagate.cu).
+void init_labels(Context& C, const Canvas& cv, const uint32_t* pos, int64_t n);
+
+// Stage (b): detect + dedup + canonical numbering on the label plane
+// (topology.cu).  Leaves the triangles in C.tris and their count in
+// C.sc()->n_triangles; returns nothing to the host.
+// `mid` (may be nullptr) is recorded between detection and deduplication.
+void detect_triangles(Context& C, const Canvas& cv, const int32_t* labels, const uint32_t* pos, int64_t n,
+                      int shift, cudaEvent_t mid = nullptr);
+
+// Stage (d): per-pixel max triangle id over a W x H image (raster.cu).
+void assign_pixels(Context& C, int W, int H, const int32_t* xs, const int32_t* ys, int32_t* tgrid,
+                   int64_t max_tri);
+
+void ensure_scalars(Context& C);
+
+}  // namespace idl
