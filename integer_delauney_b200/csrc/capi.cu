@@ -22,7 +22,7 @@ void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 size_t Context::workspace_bytes() const
 {
     const DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
-                           &tiles[0], &tiles[1], &stamps, &counts, &hkeys, &hvals, &ukeys, &uvals, &cnt,
+                           &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &hkeys, &hvals, &ukeys, &uvals, &cnt,
                            &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded, &scalars};
     size_t s = 0;
     for (const DevBuf* b : all) s += b->bytes;
@@ -38,7 +38,7 @@ void Context::fetch_scalars()
 Context::~Context()
 {
     DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
-                     &tiles[0], &tiles[1], &stamps, &counts, &hkeys, &hvals, &ukeys, &uvals, &cnt,
+                     &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &hkeys, &hvals, &ukeys, &uvals, &cnt,
                      &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded, &scalars};
     for (DevBuf* b : all) b->release();
     if (host_sc) cudaFreeHost(host_sc);

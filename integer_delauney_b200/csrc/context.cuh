@@ -94,6 +94,8 @@ struct Context {
     DevBuf tiles[2];      // active tile lists
     DevBuf stamps;        // per-tile "already listed for round r" marks
     DevBuf counts;        // per-round list lengths
+    DevBuf gsync;         // grid barrier state of the persistent propagation kernel
+    DevBuf bits;          // work-list dedup bitmaps of the persistent propagation kernel
     int32_t stamp_epoch = 0;
 
     // topology
@@ -167,6 +169,12 @@ struct Canvas {
     int Wd, Hd, pitch;
 };
 int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos);
+
+// Reference-semantics propagation as one persistent kernel (sparse_jacobi.cu).
+int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos);
+
+// Reserve a range of per-item stamp values for `steps` steps (propagate.cu).
+int32_t claim_stamps(Context& C, int n_items, int64_t steps);
 
 // Seed the label planes: fill with UNDEF and write seed ids (propagate.cu).
 void init_labels(Context& C, const Canvas& cv, const uint32_t* pos, int64_t n);

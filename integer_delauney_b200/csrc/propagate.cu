@@ -35,119 +35,232 @@
 // holds the same state in both planes, so reads of the frozen neighbours of an
 // active tile are always current, and at convergence the planes agree.
 #include "context.cuh"
+#include "stencil.cuh"
 
 #include <vector>
 
 namespace idl {
 namespace {
 
-constexpr int32_t OUTSIDE = -2;   // halo cell beyond the canvas edge
+// CTA geometry: a 64 x 64 region = the 48 x 48 tile plus an 8-cell halo.
+// 8 warps own 8 rows each; lane l owns columns 2l and 2l+1 of its warp's rows,
+// so each thread keeps 16 cells (label and squared distance) in registers.
+// Horizontal neighbours come from the adjacent lane by shuffle, vertical ones
+// from the thread's own registers, and only each warp's top and bottom rows go
+// through shared memory to the warps above and below.
+constexpr int RW = 64, RH = 64, KSTEPS = 8;
+constexpr int TW = RW - 2 * KSTEPS, TH = RH - 2 * KSTEPS;   // 48 x 48 inner tile
+constexpr int WARPS = 8, ROWS = RH / WARPS;
+constexpr int THREADS = WARPS * 32;
+static_assert(ROWS * 2 <= 32, "cell mask must fit 32 bits");
 
-template <int TW, int TH, int K>
-struct TileShape {
-    static constexpr int RW = TW + 2 * K;
-    static constexpr int RH = TH + 2 * K;
-    static constexpr int RN = RW * RH;
+struct Edges {
+    int32_t lab[2][WARPS][2][RW];   // [parity][warp][0 = top row, 1 = bottom row][column]
+    uint32_t chg[2][WARPS][2][2];   // [parity][warp][top/bottom][column 0/1 of each lane]: lane ballots
 };
 
-// One Jacobi step for the cell at region index i (rules of geometry_device.cuh:40-66).
-__device__ __forceinline__ int32_t jacobi_cell(const int32_t* __restrict__ B, int i, int cx, int cy, int RW,
-                                               int RH, int gx, int gy, const uint32_t* __restrict__ pos)
+__device__ __forceinline__ void publish(Edges& E, int par, int warp, int lane, const int32_t (&L)[ROWS][2],
+                                        uint32_t chg)
 {
-    const int32_t c = B[i];
-    if (c == OUTSIDE) return c;
-    const int32_t nb[4] = {cx > 0 ? B[i - 1] : OUTSIDE, cx < RW - 1 ? B[i + 1] : OUTSIDE,
-                           cy > 0 ? B[i - RW] : OUTSIDE, cy < RH - 1 ? B[i + RW] : OUTSIDE};
-    int32_t best = c;
-    int32_t bd = -1;   // distance of `best`, computed on demand
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int32_t n = nb[k];
-        if (n < 0 || n == c || n == best) continue;
-        const int32_t nd = dist2(gx, gy, __ldg(&pos[n]));
-        if (best < 0) { best = n; bd = nd; continue; }
-        if (bd < 0) bd = dist2(gx, gy, __ldg(&pos[best]));
-        if (nd < bd || (nd == bd && n > best)) { best = n; bd = nd; }
+    E.lab[par][warp][0][2 * lane] = L[0][0];
+    E.lab[par][warp][0][2 * lane + 1] = L[0][1];
+    E.lab[par][warp][1][2 * lane] = L[ROWS - 1][0];
+    E.lab[par][warp][1][2 * lane + 1] = L[ROWS - 1][1];
+    const uint32_t t0 = __ballot_sync(FULL, chg & 1u), t1 = __ballot_sync(FULL, chg & 2u);
+    const uint32_t b0 = __ballot_sync(FULL, chg & (1u << (2 * ROWS - 2)));
+    const uint32_t b1 = __ballot_sync(FULL, chg & (1u << (2 * ROWS - 1)));
+    if (lane == 0) {
+        E.chg[par][warp][0][0] = t0;
+        E.chg[par][warp][0][1] = t1;
+        E.chg[par][warp][1][0] = b0;
+        E.chg[par][warp][1][1] = b1;
     }
-    return best;
 }
 
-// One directional sub-step of the NumPy sweep (voronoi.py:136-154).
-__device__ __forceinline__ int32_t sweep_cell(int32_t c, int32_t n, int gx, int gy, const uint32_t* __restrict__ pos)
-{
-    if (c == OUTSIDE || n < 0 || n == c) return c;
-    if (c == UNDEF) return n;
-    const int32_t cd = dist2(gx, gy, __ldg(&pos[n]));
-    const int32_t dc = dist2(gx, gy, __ldg(&pos[c]));
-    return (cd < dc || (cd == dc && n > c)) ? n : c;
-}
-
-template <int TW, int TH, int K, int MODE>
-__global__ void __launch_bounds__(256)
+template <int MODE>
+__global__ void __launch_bounds__(THREADS, 3)
 k_round(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pitch, int Wd, int Hd,
         const uint32_t* __restrict__ pos, const int32_t* __restrict__ list_in, const int32_t* __restrict__ count_in,
         int32_t* __restrict__ list_out, int32_t* __restrict__ count_out, int32_t* __restrict__ stamp,
         int32_t stamp_next, int tiles_x, int tiles_y, long long step_base, long long* __restrict__ last_change)
 {
-    using S = TileShape<TW, TH, K>;
-    constexpr int RW = S::RW, RH = S::RH, RN = S::RN;
-    __shared__ int32_t buf[2][RN];
+    __shared__ Edges E;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int cx0 = 2 * lane, cy0 = warp * ROWS;
+
+    // cells of this thread that lie in the inner tile: bit 2r + c
+    uint32_t inner = 0;
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+            if (cx0 + c >= KSTEPS && cx0 + c < KSTEPS + TW && cy0 + r >= KSTEPS && cy0 + r < KSTEPS + TH)
+                inner |= 1u << (2 * r + c);
 
     const int n_items = *count_in;
     for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
         const int t = list_in[item];
         const int tx = t % tiles_x, ty = t / tiles_x;
-        const int gx0 = tx * TW - K, gy0 = ty * TH - K;
+        const int gx = tx * TW - KSTEPS + cx0;   // canvas column of this thread's column 0
+        const int gyb = ty * TH - KSTEPS + cy0;  // canvas row of this thread's row 0
 
-        for (int i = threadIdx.x; i < RN; i += blockDim.x) {
-            const int cx = i % RW, cy = i / RW;
-            const int gx = gx0 + cx, gy = gy0 + cy;
-            buf[0][i] = (gx >= 0 && gx < Wd && gy >= 0 && gy < Hd) ? src[(size_t)gy * pitch + gx] : OUTSIDE;
-        }
-        __syncthreads();
-
-        int cur = 0;
-        int last_step = -1;
-        for (int s = 0; s < K; ++s) {
-            bool inner_changed = false;
-            if (MODE == IDL_MODE_REFERENCE) {
-                for (int i = threadIdx.x; i < RN; i += blockDim.x) {
-                    const int cx = i % RW, cy = i / RW;
-                    const int32_t v = jacobi_cell(buf[cur], i, cx, cy, RW, RH, gx0 + cx, gy0 + cy, pos);
-                    buf[cur ^ 1][i] = v;
-                    if (v != buf[cur][i] && cx >= K && cx < K + TW && cy >= K && cy < K + TH) inner_changed = true;
-                }
-                cur ^= 1;
-                if (__syncthreads_or(inner_changed)) last_step = s;
-            } else {
-                // left, right, up, down neighbour, each a synchronous sub-step
-#pragma unroll 1
-                for (int dir = 0; dir < 4; ++dir) {
-                    const int32_t* B = buf[cur];
-                    for (int i = threadIdx.x; i < RN; i += blockDim.x) {
-                        const int cx = i % RW, cy = i / RW;
-                        int32_t n;
-                        if (dir == 0) n = cx > 0 ? B[i - 1] : OUTSIDE;
-                        else if (dir == 1) n = cx < RW - 1 ? B[i + 1] : OUTSIDE;
-                        else if (dir == 2) n = cy > 0 ? B[i - RW] : OUTSIDE;
-                        else n = cy < RH - 1 ? B[i + RW] : OUTSIDE;
-                        const int32_t c = B[i];
-                        const int32_t v = sweep_cell(c, n, gx0 + cx, gy0 + cy, pos);
-                        buf[cur ^ 1][i] = v;
-                        if (v != c && cx >= K && cx < K + TW && cy >= K && cy < K + TH) inner_changed = true;
-                    }
-                    cur ^= 1;
-                    __syncthreads();
-                }
-                if (__syncthreads_or(inner_changed)) last_step = s;
+        int32_t L[ROWS][2], D[ROWS][2];
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r) {
+            const int gy = gyb + r;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const bool in = gx + c >= 0 && gx + c < Wd && gy >= 0 && gy < Hd;
+                const int32_t l = in ? src[(size_t)gy * pitch + gx + c] : OUTSIDE;
+                L[r][c] = l;
+                D[r][c] = l >= 0 ? dist2(gx + c, gy, __ldg(&pos[l])) : FAR;
             }
         }
+        publish(E, 1, warp, lane, L, 0xFFFFFFFFu);
+        __syncthreads();
 
-        for (int i = threadIdx.x; i < TW * TH; i += blockDim.x) {
-            const int ix = i % TW, iy = i / TW;
-            const int gx = tx * TW + ix, gy = ty * TH + iy;
-            if (gx < Wd && gy < Hd) dst[(size_t)gy * pitch + gx] = buf[cur][(iy + K) * RW + ix + K];
+        uint32_t chg = 0;
+        int last_step = -1;
+        int par = 1;   // parity of the last publication
+#pragma unroll 1
+        for (int s = 0; s < KSTEPS; ++s) {
+            uint32_t new_chg = 0;
+            if (MODE == IDL_MODE_REFERENCE) {
+                // ---- one Jacobi step (voronoi.cu:32-53) ----
+                const int pp = par;
+                int32_t up0 = warp > 0 ? E.lab[pp][warp - 1][1][cx0] : OUTSIDE;
+                int32_t up1 = warp > 0 ? E.lab[pp][warp - 1][1][cx0 + 1] : OUTSIDE;
+                const int32_t dn0 = warp < WARPS - 1 ? E.lab[pp][warp + 1][0][cx0] : OUTSIDE;
+                const int32_t dn1 = warp < WARPS - 1 ? E.lab[pp][warp + 1][0][cx0 + 1] : OUTSIDE;
+                // a cell can change only if a cell of its closed neighbourhood changed in the previous step
+                uint32_t dirty;
+                if (s == 0) {
+                    dirty = (1u << (2 * ROWS)) - 1u;
+                } else {
+                    dirty = chg | (chg << 2) | (chg >> 2) | ((chg & 0x55555555u) << 1) | ((chg & 0xAAAAAAAAu) >> 1);
+                    const uint32_t lc = __shfl_up_sync(FULL, chg, 1), rc = __shfl_down_sync(FULL, chg, 1);
+                    if (lane > 0) dirty |= (lc & 0xAAAAAAAAu) >> 1;
+                    if (lane < 31) dirty |= (rc & 0x55555555u) << 1;
+                    if (warp > 0) {
+                        dirty |= (E.chg[pp][warp - 1][1][0] >> lane) & 1u;
+                        dirty |= ((E.chg[pp][warp - 1][1][1] >> lane) & 1u) << 1;
+                    }
+                    if (warp < WARPS - 1) {
+                        dirty |= ((E.chg[pp][warp + 1][0][0] >> lane) & 1u) << (2 * ROWS - 2);
+                        dirty |= ((E.chg[pp][warp + 1][0][1] >> lane) & 1u) << (2 * ROWS - 1);
+                    }
+                    dirty &= (1u << (2 * ROWS)) - 1u;
+                }
+                if (__any_sync(FULL, dirty != 0)) {
+#pragma unroll
+                    for (int r = 0; r < ROWS; ++r) {
+                        const int32_t o0 = L[r][0], o1 = L[r][1];
+                        int32_t left = __shfl_up_sync(FULL, o1, 1);
+                        int32_t right = __shfl_down_sync(FULL, o0, 1);
+                        if (lane == 0) left = OUTSIDE;
+                        if (lane == 31) right = OUTSIDE;
+                        const int32_t b0 = r + 1 < ROWS ? L[r + 1][0] : dn0;
+                        const int32_t b1 = r + 1 < ROWS ? L[r + 1][1] : dn1;
+                        const int gy = gyb + r;
+                        if (((dirty >> (2 * r)) & 1u) && o0 != OUTSIDE) {
+                            int32_t bl = o0, bd = D[r][0];
+                            relax(bl, bd, left, gx, gy, pos);
+                            relax(bl, bd, o1, gx, gy, pos);
+                            relax(bl, bd, up0, gx, gy, pos);
+                            relax(bl, bd, b0, gx, gy, pos);
+                            if (bl != o0) {
+                                L[r][0] = bl;
+                                D[r][0] = bd;
+                                new_chg |= 1u << (2 * r);
+                            }
+                        }
+                        if (((dirty >> (2 * r + 1)) & 1u) && o1 != OUTSIDE) {
+                            int32_t bl = o1, bd = D[r][1];
+                            relax(bl, bd, o0, gx + 1, gy, pos);
+                            relax(bl, bd, right, gx + 1, gy, pos);
+                            relax(bl, bd, up1, gx + 1, gy, pos);
+                            relax(bl, bd, b1, gx + 1, gy, pos);
+                            if (bl != o1) {
+                                L[r][1] = bl;
+                                D[r][1] = bd;
+                                new_chg |= 1u << (2 * r + 1);
+                            }
+                        }
+                        up0 = o0;
+                        up1 = o1;
+                    }
+                }
+                par ^= 1;
+                publish(E, par, warp, lane, L, new_chg);
+            } else {
+                // ---- one NumPy iteration (voronoi.py:113-157): left, right, up, down ----
+#pragma unroll
+                for (int r = 0; r < ROWS; ++r) {   // neighbour on the left
+                    const int32_t o0 = L[r][0], o1 = L[r][1];
+                    int32_t left = __shfl_up_sync(FULL, o1, 1);
+                    if (lane == 0) left = OUTSIDE;
+                    const int gy = gyb + r;
+                    if (o0 != OUTSIDE) relax(L[r][0], D[r][0], left, gx, gy, pos);
+                    if (o1 != OUTSIDE) relax(L[r][1], D[r][1], o0, gx + 1, gy, pos);
+                    new_chg |= (uint32_t(L[r][0] != o0) << (2 * r)) | (uint32_t(L[r][1] != o1) << (2 * r + 1));
+                }
+#pragma unroll
+                for (int r = 0; r < ROWS; ++r) {   // neighbour on the right
+                    const int32_t o0 = L[r][0], o1 = L[r][1];
+                    int32_t right = __shfl_down_sync(FULL, o0, 1);
+                    if (lane == 31) right = OUTSIDE;
+                    const int gy = gyb + r;
+                    if (o0 != OUTSIDE) relax(L[r][0], D[r][0], o1, gx, gy, pos);
+                    if (o1 != OUTSIDE) relax(L[r][1], D[r][1], right, gx + 1, gy, pos);
+                    new_chg |= (uint32_t(L[r][0] != o0) << (2 * r)) | (uint32_t(L[r][1] != o1) << (2 * r + 1));
+                }
+                par ^= 1;
+                publish(E, par, warp, lane, L, 0u);
+                __syncthreads();
+                {   // neighbour above: rows bottom-up read not-yet-updated rows
+                    const int32_t up0 = warp > 0 ? E.lab[par][warp - 1][1][cx0] : OUTSIDE;
+                    const int32_t up1 = warp > 0 ? E.lab[par][warp - 1][1][cx0 + 1] : OUTSIDE;
+#pragma unroll
+                    for (int r = ROWS - 1; r >= 0; --r) {
+                        const int32_t o0 = L[r][0], o1 = L[r][1];
+                        const int32_t n0 = r > 0 ? L[r - 1][0] : up0, n1 = r > 0 ? L[r - 1][1] : up1;
+                        const int gy = gyb + r;
+                        if (o0 != OUTSIDE) relax(L[r][0], D[r][0], n0, gx, gy, pos);
+                        if (o1 != OUTSIDE) relax(L[r][1], D[r][1], n1, gx + 1, gy, pos);
+                        new_chg |= (uint32_t(L[r][0] != o0) << (2 * r)) | (uint32_t(L[r][1] != o1) << (2 * r + 1));
+                    }
+                }
+                par ^= 1;
+                publish(E, par, warp, lane, L, 0u);
+                __syncthreads();
+                {   // neighbour below: rows top-down read not-yet-updated rows
+                    const int32_t dn0 = warp < WARPS - 1 ? E.lab[par][warp + 1][0][cx0] : OUTSIDE;
+                    const int32_t dn1 = warp < WARPS - 1 ? E.lab[par][warp + 1][0][cx0 + 1] : OUTSIDE;
+#pragma unroll
+                    for (int r = 0; r < ROWS; ++r) {
+                        const int32_t o0 = L[r][0], o1 = L[r][1];
+                        const int32_t n0 = r + 1 < ROWS ? L[r + 1][0] : dn0, n1 = r + 1 < ROWS ? L[r + 1][1] : dn1;
+                        const int gy = gyb + r;
+                        if (o0 != OUTSIDE) relax(L[r][0], D[r][0], n0, gx, gy, pos);
+                        if (o1 != OUTSIDE) relax(L[r][1], D[r][1], n1, gx + 1, gy, pos);
+                        new_chg |= (uint32_t(L[r][0] != o0) << (2 * r)) | (uint32_t(L[r][1] != o1) << (2 * r + 1));
+                    }
+                }
+                par ^= 1;
+                publish(E, par, warp, lane, L, 0u);
+            }
+            chg = new_chg;
+            if (__syncthreads_or((new_chg & inner) != 0u)) last_step = s;
         }
+
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+                if ((inner >> (2 * r + c)) & 1u) {
+                    const int gy = gyb + r;
+                    if (gx + c < Wd && gy < Hd) dst[(size_t)gy * pitch + gx + c] = L[r][c];
+                }
 
         if (last_step >= 0) {
             if (threadIdx.x == 0) atomicMax(last_change, step_base + last_step);
@@ -186,8 +299,6 @@ __global__ void k_write_seeds(int32_t* __restrict__ a, int32_t* __restrict__ b, 
     b[o] = (int32_t)i;
 }
 
-constexpr int TW = 32, TH = 32, KSTEPS = 8;
-
 }  // namespace
 
 void init_labels(Context& C, const Canvas& cv, const uint32_t* pos, int64_t n)
@@ -204,8 +315,27 @@ void init_labels(Context& C, const Canvas& cv, const uint32_t* pos, int64_t n)
     }
 }
 
+// Reserve a fresh range of stamp values for a run of `steps` steps over
+// `n_items` work items (stamps never need clearing between runs).
+int32_t claim_stamps(Context& C, int n_items, int64_t steps)
+{
+    if (C.stamps.bytes < (size_t)n_items * 4) {
+        C.stamps.ensure((size_t)n_items * 4);
+        IDL_CUDA(cudaMemsetAsync(C.stamps.ptr, 0, C.stamps.bytes, C.stream));
+        C.stamp_epoch = 0;
+    }
+    if (C.stamp_epoch > (1 << 30) - steps - 8) {
+        IDL_CUDA(cudaMemsetAsync(C.stamps.ptr, 0, C.stamps.bytes, C.stream));
+        C.stamp_epoch = 0;
+    }
+    const int32_t epoch = C.stamp_epoch;
+    C.stamp_epoch += int32_t(steps + 4);
+    return epoch;
+}
+
 int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos)
 {
+    if (mode == IDL_MODE_REFERENCE) return propagate_sparse(C, cv, pos);
     const int tiles_x = ceil_div(cv.Wd, TW), tiles_y = ceil_div(cv.Hd, TH);
     const int n_tiles = tiles_x * tiles_y;
     // Bound on rounds: far above any real run (a pass count beyond the canvas
@@ -215,17 +345,7 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos)
 
     C.tiles[0].ensure((size_t)n_tiles * 4);
     C.tiles[1].ensure((size_t)n_tiles * 4);
-    if (C.stamps.bytes < (size_t)n_tiles * 4) {
-        C.stamps.ensure((size_t)n_tiles * 4);
-        IDL_CUDA(cudaMemsetAsync(C.stamps.ptr, 0, (size_t)n_tiles * 4, C.stream));
-        C.stamp_epoch = 0;
-    }
-    if (C.stamp_epoch > (1 << 30) - max_rounds - 8) {
-        IDL_CUDA(cudaMemsetAsync(C.stamps.ptr, 0, C.stamps.bytes, C.stream));
-        C.stamp_epoch = 0;
-    }
-    const int32_t epoch = C.stamp_epoch;
-    C.stamp_epoch += int32_t(max_rounds + 4);
+    const int32_t epoch = claim_stamps(C, n_tiles, max_rounds);
 
     const size_t count_len = (size_t)max_rounds + 2;
     C.counts.ensure(count_len * 4);
@@ -238,7 +358,7 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos)
     k_set_i64<<<1, 1, 0, C.stream>>>(last, -1);
     IDL_LAUNCH();
 
-    const int grid = std::min(n_tiles, C.num_sms * 8);
+    const int grid = std::min(n_tiles, C.num_sms * 3);
     int64_t r = 0;
     int group = 2;
     for (;;) {
@@ -250,11 +370,11 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos)
             const long long base = (long long)r * KSTEPS;
             const int32_t stamp_next = epoch + int32_t(r) + 1;
             if (mode == IDL_MODE_NUMPY)
-                k_round<TW, TH, KSTEPS, IDL_MODE_NUMPY><<<grid, 256, 0, C.stream>>>(
+                k_round<IDL_MODE_NUMPY><<<grid, THREADS, 0, C.stream>>>(
                     srcp, dstp, cv.pitch, cv.Wd, cv.Hd, pos, lin, counts + r, lout, counts + r + 1,
                     C.stamps.as<int32_t>(), stamp_next, tiles_x, tiles_y, base, last);
             else
-                k_round<TW, TH, KSTEPS, IDL_MODE_REFERENCE><<<grid, 256, 0, C.stream>>>(
+                k_round<IDL_MODE_REFERENCE><<<grid, THREADS, 0, C.stream>>>(
                     srcp, dstp, cv.pitch, cv.Wd, cv.Hd, pos, lin, counts + r, lout, counts + r + 1,
                     C.stamps.as<int32_t>(), stamp_next, tiles_x, tiles_y, base, last);
             IDL_LAUNCH();

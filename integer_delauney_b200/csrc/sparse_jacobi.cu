@@ -1,0 +1,339 @@
+// Stage (a), reference semantics: the synchronous Jacobi fixed point of
+// src/cuda/voronoi.cu:32-53,100-113, computed by one persistent cooperative
+// kernel that steps only the parts of the canvas that can still change.
+//
+// Why sparse.  At 4096 x 4096 with 200 000 uniform seeds the reference runs
+// 51 full-canvas passes (51 x 17 M cell updates) but only 18 M labels ever
+// change and only 68 M cell evaluations have a changed neighbour; the
+// clustered case runs 1 100 passes with a thin moving front.  A cell can only
+// change in pass t+1 if a cell of its closed 4-neighbourhood changed in pass t
+// (keys only improve, and a pass is a pure function of the neighbourhood), so
+// per pass only the 8 x 8 micro-tiles holding or bordering a change need work.
+//
+// How.  Pass t reads label plane t%2 and writes plane (t+1)%2.  The
+// micro-tiles to run in pass t form work list t%2.  A micro-tile whose cells
+// change lists itself, and the neighbour across any edge whose row or column
+// changed, for pass t+1; bitmap (t+1)%2 deduplicates them (each task clears
+// its own bit of bitmap t%2, which is then pass t+1's target).  A processed
+// micro-tile always writes all its cells, so any micro-tile not being
+// processed holds the same state in both planes (by induction), and the
+// 1-cell border reads of an active micro-tile are always current.  Passes are
+// separated by a grid-wide barrier with a bounded wait; no host round trip
+// happens until the list runs empty.  Each warp advances GROUP micro-tiles at
+// once, with all loads issued before any compute, and next-pass list entries
+// are staged per block so the list counter sees one atomic per block per pass.
+//
+// Coherence: planes, lists and bitmaps are rewritten by other blocks between
+// passes, so they are read with ld.global.cg (L2), never through L1 or the
+// read-only path; barrier arrival and departure are release/acquire.
+#include "context.cuh"
+#include "stencil.cuh"
+
+#include <cuda/atomic>
+#include <vector>
+
+namespace idl {
+namespace {
+
+constexpr int MT = 8;                       // micro-tile side
+constexpr int SJ_THREADS = 1024;
+constexpr int SJ_WARPS = SJ_THREADS / 32;
+constexpr int GROUP = 2;                    // micro-tiles a warp advances together
+constexpr unsigned SPIN_LIMIT = 1u << 24;   // barrier polls before giving up
+constexpr int STAGE = 6144;                 // per-block staging of next-pass list entries
+
+struct GridSync {
+    unsigned count;
+    unsigned gen;
+    int error;
+    int passes;   // passes run (the last one changed nothing)
+};
+
+// Grid-wide barrier with a bounded wait.  On timeout the error flag is raised
+// and every block leaves the kernel, so a bug cannot hang the GPU.
+__device__ __forceinline__ bool grid_sync(GridSync* gs, unsigned nblocks, unsigned& gen_local)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(gs->count), gen(gs->gen);
+        cuda::atomic_ref<int, cuda::thread_scope_device> err(gs->error);
+        const unsigned target = gen_local + 1;
+        int ok = 1;
+        if (cnt.fetch_add(1u, cuda::memory_order_acq_rel) == nblocks - 1) {
+            cnt.store(0u, cuda::memory_order_relaxed);
+            gen.store(target, cuda::memory_order_release);
+        } else {
+            unsigned spins = 0;
+            while (gen.load(cuda::memory_order_acquire) != target) {
+                if (++spins > SPIN_LIMIT) {
+                    err.fetch_or(1, cuda::memory_order_relaxed);
+                    ok = 0;
+                    break;
+                }
+                if (spins > 32) __nanosleep(20);
+            }
+        }
+        if (err.load(cuda::memory_order_relaxed)) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    ++gen_local;
+    return s_ok != 0;
+}
+
+// The Jacobi update of one cell owned by `b` from its four neighbours' owners
+// (geometry_device.cuh:40-66).  The owner's and the candidates' distances are
+// gathered together so the seed-table loads overlap; the choice is then pure
+// arithmetic.
+__device__ __forceinline__ void best_of4(int32_t& b, int32_t n0, int32_t n1, int32_t n2, int32_t n3, int x, int y,
+                                         const uint32_t* __restrict__ pos)
+{
+    const int32_t own = b;
+    const int32_t n[4] = {n0, n1, n2, n3};
+    int32_t d[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) d[j] = (n[j] >= 0 && n[j] != own) ? dist2(x, y, __ldg(&pos[n[j]])) : FAR;
+    int32_t bd = own >= 0 ? dist2(x, y, __ldg(&pos[own])) : FAR;
+    int32_t bl = own;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (n[j] < 0 || n[j] == own) continue;
+        if (d[j] < bd || (d[j] == bd && n[j] > bl)) {
+            bl = n[j];
+            bd = d[j];
+        }
+    }
+    b = bl;
+}
+
+struct Stage {
+    int32_t* list;
+    int* n;
+};
+
+// Advance `cnt` (<= GROUP, warp-uniform) micro-tiles by one Jacobi pass and
+// list the micro-tiles pass t+1 must run.
+__device__ __forceinline__ void advance(const int (&ids)[GROUP], int cnt, const int32_t* cur, int32_t* nxt,
+                                        int pitch, int Wd, int Hd, int mt_x, int mt_y,
+                                        const uint32_t* __restrict__ pos, uint32_t* bin, uint32_t* bout,
+                                        int32_t* lout, int32_t* count_out, Stage st, int lane)
+{
+    const int r = lane >> 2, c0 = (lane & 3) * 2;
+    int32_t a0[GROUP], a1[GROUP], u0[GROUP], u1[GROUP], d0[GROUP], d1[GROUP], lf[GROUP], rt[GROUP];
+    int gx[GROUP], gy[GROUP];
+    bool in0[GROUP], in1[GROUP];
+    // loads: own two cells and, on the micro-tile's edges, the cells across
+#pragma unroll
+    for (int k = 0; k < GROUP; ++k) {
+        a0[k] = a1[k] = u0[k] = u1[k] = d0[k] = d1[k] = lf[k] = rt[k] = OUTSIDE;
+        in0[k] = in1[k] = false;
+        gx[k] = gy[k] = 0;
+        if (k < cnt) {
+            if (lane == 0) atomicAnd(&bin[ids[k] >> 5], ~(1u << (ids[k] & 31)));
+            const int mx = ids[k] % mt_x, my = ids[k] / mt_x;
+            gx[k] = mx * MT + c0;
+            gy[k] = my * MT + r;
+            const bool row_in = gy[k] < Hd;
+            in0[k] = row_in && gx[k] < Wd;
+            in1[k] = row_in && gx[k] + 1 < Wd;
+            const size_t o = (size_t)gy[k] * pitch + gx[k];
+            if (in1[k]) {
+                const int2 v = __ldcg(reinterpret_cast<const int2*>(cur + o));
+                a0[k] = v.x;
+                a1[k] = v.y;
+            } else if (in0[k]) {
+                a0[k] = __ldcg(&cur[o]);
+            }
+            if (r == 0 && gy[k] > 0) {
+                if (in0[k]) u0[k] = __ldcg(&cur[o - pitch]);
+                if (in1[k]) u1[k] = __ldcg(&cur[o - pitch + 1]);
+            }
+            if (r == MT - 1 && gy[k] + 1 < Hd) {
+                if (in0[k]) d0[k] = __ldcg(&cur[o + pitch]);
+                if (in1[k]) d1[k] = __ldcg(&cur[o + pitch + 1]);
+            }
+            if ((lane & 3) == 0 && in0[k] && gx[k] > 0) lf[k] = __ldcg(&cur[o - 1]);
+            if ((lane & 3) == 3 && in1[k] && gx[k] + 2 < Wd) rt[k] = __ldcg(&cur[o + 2]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < GROUP; ++k) {
+        if (k >= cnt) break;
+        // neighbours inside the micro-tile come from the lanes that own them
+        const int32_t su0 = __shfl_up_sync(FULL, a0[k], 4), su1 = __shfl_up_sync(FULL, a1[k], 4);
+        const int32_t sd0 = __shfl_down_sync(FULL, a0[k], 4), sd1 = __shfl_down_sync(FULL, a1[k], 4);
+        const int32_t sl = __shfl_up_sync(FULL, a1[k], 1), sr = __shfl_down_sync(FULL, a0[k], 1);
+        if (r != 0) { u0[k] = su0; u1[k] = su1; }
+        if (r != MT - 1) { d0[k] = sd0; d1[k] = sd1; }
+        if ((lane & 3) != 0) lf[k] = sl;
+        if ((lane & 3) != 3) rt[k] = sr;
+
+        int32_t b0 = a0[k], b1 = a1[k];
+        if (in0[k] && (lf[k] != b0 || a1[k] != b0 || u0[k] != b0 || d0[k] != b0))
+            best_of4(b0, lf[k], a1[k], u0[k], d0[k], gx[k], gy[k], pos);
+        if (in1[k] && (a0[k] != b1 || rt[k] != b1 || u1[k] != b1 || d1[k] != b1))
+            best_of4(b1, a0[k], rt[k], u1[k], d1[k], gx[k] + 1, gy[k], pos);
+        const size_t o = (size_t)gy[k] * pitch + gx[k];
+        if (in1[k]) *reinterpret_cast<int2*>(nxt + o) = make_int2(b0, b1);
+        else if (in0[k]) nxt[o] = b0;
+
+        const bool ch0 = b0 != a0[k], ch1 = b1 != a1[k];
+        const unsigned any = __ballot_sync(FULL, ch0 || ch1);
+        if (any) {
+            const unsigned left = __ballot_sync(FULL, ch0 && (lane & 3) == 0);
+            const unsigned right = __ballot_sync(FULL, ch1 && (lane & 3) == 3);
+            const int mt = ids[k], mx = mt % mt_x, my = mt / mt_x;
+            int target = -1;
+            if (lane == 0) target = mt;
+            if (lane == 1 && (any & 0xFu) && my > 0) target = mt - mt_x;
+            if (lane == 2 && (any & 0xF0000000u) && my + 1 < mt_y) target = mt + mt_x;
+            if (lane == 3 && left && mx > 0) target = mt - 1;
+            if (lane == 4 && right && mx + 1 < mt_x) target = mt + 1;
+            bool fresh = false;
+            if (target >= 0) {
+                const uint32_t bit = 1u << (target & 31);
+                fresh = !(atomicOr(&bout[target >> 5], bit) & bit);
+            }
+            const unsigned fb = __ballot_sync(FULL, fresh);
+            if (fb) {
+                const int m = __popc(fb);
+                int base = 0;
+                if (lane == 0) base = atomicAdd(st.n, m);
+                base = __shfl_sync(FULL, base, 0);
+                const int rank = __popc(fb & ((1u << lane) - 1u));
+                if (base + m <= STAGE) {
+                    if (fresh) st.list[base + rank] = target;
+                } else {
+                    int gbase = 0;
+                    if (lane == 0) gbase = atomicAdd(count_out, m);
+                    gbase = __shfl_sync(FULL, gbase, 0);
+                    if (fresh) lout[gbase + rank] = target;
+                }
+            }
+        }
+    }
+}
+
+// counts[t]: micro-tiles listed for pass t.  Pass t runs list t%2 and appends
+// pass t+1's micro-tiles to list (t+1)%2.
+__global__ void __launch_bounds__(SJ_THREADS, 1)
+k_sparse_jacobi(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, const uint32_t* __restrict__ pos,
+                uint32_t* bits0, uint32_t* bits1, int32_t* list0, int32_t* list1, int32_t* counts, int max_steps,
+                int mt_x, int mt_y, GridSync* gs)
+{
+    __shared__ int32_t s_list[STAGE];
+    __shared__ int s_n, s_base, s_m;
+    const int lane = threadIdx.x & 31;
+    const int gwarp = blockIdx.x * SJ_WARPS + (threadIdx.x >> 5);
+    const int nwarps = gridDim.x * SJ_WARPS;
+    unsigned gen_local = 0;
+    int t = 0;
+    for (; t < max_steps; ++t) {
+        const int n = *reinterpret_cast<volatile int32_t*>(&counts[t]);
+        if (n == 0) break;
+        if (threadIdx.x == 0) s_n = 0;
+        __syncthreads();
+        const int32_t* cur = (t & 1) ? plane1 : plane0;
+        int32_t* nxt = (t & 1) ? plane0 : plane1;
+        uint32_t* bin = (t & 1) ? bits1 : bits0;
+        uint32_t* bout = (t & 1) ? bits0 : bits1;
+        const int32_t* lin = (t & 1) ? list1 : list0;
+        int32_t* lout = (t & 1) ? list0 : list1;
+        for (int i0 = gwarp * GROUP; i0 < n; i0 += nwarps * GROUP) {
+            int ids[GROUP];
+            const int cnt = min(GROUP, n - i0);
+#pragma unroll
+            for (int k = 0; k < GROUP; ++k) ids[k] = k < cnt ? __ldcg(&lin[i0 + k]) : 0;
+            advance(ids, cnt, cur, nxt, pitch, Wd, Hd, mt_x, mt_y, pos, bin, bout, lout, counts + t + 1,
+                    Stage{s_list, &s_n}, lane);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int m = min(s_n, STAGE);
+            s_m = m;
+            s_base = m ? atomicAdd(&counts[t + 1], m) : 0;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < s_m; i += blockDim.x) lout[s_base + i] = s_list[i];
+        if (!grid_sync(gs, gridDim.x, gen_local)) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) gs->passes = t;
+}
+
+__global__ void k_iota_list(int32_t* __restrict__ list, int n, int32_t* __restrict__ count)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) list[i] = i;
+    if (i == 0) *count = n;
+}
+
+__global__ void k_fill_bits(uint32_t* __restrict__ bits, int n_words, int n_items)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= n_words) return;
+    const int k = n_items - w * 32;
+    bits[w] = k >= 32 ? 0xFFFFFFFFu : (k <= 0 ? 0u : ((1u << k) - 1u));
+}
+
+}  // namespace
+
+int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos)
+{
+    const int mt_x = ceil_div(cv.Wd, MT), mt_y = ceil_div(cv.Hd, MT);
+    const int n_mt = mt_x * mt_y;
+    const int n_words = ceil_div(n_mt, 32);
+    // bound on passes: far above any real run; only stops a runaway loop
+    const int max_steps = (int)std::min<int64_t>((int64_t)4 * (cv.Wd + cv.Hd) + 64, (1 << 29));
+    C.tiles[0].ensure((size_t)n_mt * 4);
+    C.tiles[1].ensure((size_t)n_mt * 4);
+    C.bits.ensure((size_t)n_words * 2 * 4);
+    uint32_t* b0 = C.bits.as<uint32_t>();
+    uint32_t* b1 = b0 + n_words;
+    k_fill_bits<<<(unsigned)((n_words + 255) / 256), 256, 0, C.stream>>>(b0, n_words, n_mt);
+    IDL_LAUNCH();
+    IDL_CUDA(cudaMemsetAsync(b1, 0, (size_t)n_words * 4, C.stream));
+    C.counts.ensure(((size_t)max_steps + 2) * 4);
+    IDL_CUDA(cudaMemsetAsync(C.counts.ptr, 0, ((size_t)max_steps + 2) * 4, C.stream));
+    int32_t* counts = C.counts.as<int32_t>();
+    int32_t* l0 = C.tiles[0].as<int32_t>();
+    int32_t* l1 = C.tiles[1].as<int32_t>();
+    k_iota_list<<<(unsigned)((n_mt + 255) / 256), 256, 0, C.stream>>>(l0, n_mt, counts);
+    IDL_LAUNCH();
+    C.gsync.ensure(sizeof(GridSync));
+    IDL_CUDA(cudaMemsetAsync(C.gsync.ptr, 0, sizeof(GridSync), C.stream));
+
+    int per_sm = 0;
+    IDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sparse_jacobi, SJ_THREADS, 0));
+    if (per_sm < 1) throw Error(IDL_ERR_INTERNAL, "propagation kernel cannot be resident");
+    const int grid = per_sm * C.num_sms;
+    int32_t* p0 = C.lab[0].as<int32_t>();
+    int32_t* p1 = C.lab[1].as<int32_t>();
+    GridSync* gs = C.gsync.as<GridSync>();
+    int pitch = cv.pitch, Wd = cv.Wd, Hd = cv.Hd, ms = max_steps, mx = mt_x, my = mt_y;
+    void* args[] = {&p0, &p1, &pitch, &Wd, &Hd, (void*)&pos, &b0, &b1, &l0, &l1, &counts, &ms, &mx, &my, &gs};
+    IDL_CUDA(cudaLaunchCooperativeKernel((const void*)k_sparse_jacobi, dim3(grid), dim3(SJ_THREADS), args, 0,
+                                         C.stream));
+    count_launch();
+    GridSync h{};
+    IDL_CUDA(cudaMemcpyAsync(&h, gs, sizeof(GridSync), cudaMemcpyDeviceToHost, C.stream));
+    IDL_CUDA(cudaStreamSynchronize(C.stream));
+    if (h.error) throw Error(IDL_ERR_INTERNAL, "Voronoi propagation: grid barrier timed out");
+    const int64_t passes = h.passes;
+    if (passes >= max_steps) throw Error(IDL_ERR_INTERNAL, "Voronoi propagation did not converge");
+    if (C.prof.enabled) {
+        std::vector<int32_t> hc((size_t)passes + 1);
+        IDL_CUDA(cudaMemcpy(hc.data(), counts, hc.size() * 4, cudaMemcpyDeviceToHost));
+        int64_t tiles = 0;
+        for (int32_t c : hc) tiles += c;
+        C.prof.tiles = tiles;
+        C.prof.rounds = passes;
+        C.prof.passes = passes;
+        C.prof.tile_w = MT;
+        C.prof.tile_h = MT;
+        C.prof.steps_per_round = 1;
+    }
+    return passes;
+}
+
+}  // namespace idl
