@@ -169,6 +169,28 @@ IDL_API int idl_triangulate_device(idl_context* ctx, int width, int height, cons
  * Valid until the next triangulation call on this context. */
 IDL_API int idl_triangles_device(idl_context* ctx, const int32_t** d_tris, const int64_t** d_count);
 
+/* ---- Voronoi().compute without any memory allocation ---------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * code with a latency budget that a cudaMalloc/cudaFree stall or device
+ * synchronisation would break, processes whose device memory is fixed in
+ * advance (a per-tenant quota, a pool they must stay inside), and hosts that
+ * embed the library under an allocator of their own.  Same result as
+ * idl_voronoi, but with device pointers, on `stream` (a cudaStream_t, NULL =
+ * legacy default stream) and the current device, and all workspace taken
+ * from one static device array of about 9.8 MB that every GPU loading the
+ * library reserves until the process exits.
+ *   limits   width, height <= 1024 and n_seeds <= 65536 (larger is rejected
+ *            with IDL_ERR_INVALID); modes IDL_MODE_REFERENCE, IDL_MODE_NUMPY.
+ *   d_seeds_xy  device n_seeds * 2 int32, any order.
+ *   d_grid_out  device height * width * 2 int32 (seed id, squared distance).
+ * The first call on a device looks up the array's device address and should
+ * therefore come before any stream capture starts.  All calls share the one
+ * array: calls whose GPU work overlaps race and must not be issued.  The call
+ * waits for its stream twice (seed validation, convergence) and returns with
+ * the output grid written or in flight on `stream`. */
+IDL_API int idl_voronoi_noalloc(int width, int height, const int32_t* d_seeds_xy, int64_t n_seeds, int mode,
+                                int32_t* d_grid_out, void* stream, int64_t* passes_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,7 @@ SIGNATURES = {
     "idl_get_triangles": (_i32, [_vp, _vp, _i64]),
     "idl_triangulate_device": (_i32, [_vp, _i32, _i32, _vp, _i64, _i32, _i32, _vp, _pi64]),
     "idl_triangles_device": (_i32, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
+    "idl_voronoi_noalloc": (_i32, [_i32, _i32, _vp, _i64, _i32, _vp, _vp, _pi64]),
 }
 
 _lib = None

@@ -41,7 +41,7 @@ Context::~Context()
                      &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &hkeys, &hvals, &ukeys, &uvals, &cnt,
                      &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded, &scalars};
     for (DevBuf* b : all) b->release();
-    if (host_sc) cudaFreeHost(host_sc);
+    if (host_sc && !host_sc_borrowed) cudaFreeHost(host_sc);
     for (auto& e : timing.ev)
         if (e) cudaEventDestroy(e);
 }

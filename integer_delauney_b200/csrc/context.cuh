@@ -19,6 +19,7 @@ namespace idl {
 struct DevBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
+    bool fixed = false;   // borrowed memory of fixed size: never allocated or freed here
 
     template <class T>
     T* as() const { return static_cast<T*>(ptr); }
@@ -27,14 +28,21 @@ struct DevBuf {
     void ensure(size_t need)
     {
         if (need <= bytes) return;
+        if (fixed) invalid("request exceeds the fixed workspace of this entry point");
         release();
         if (need == 0) return;
         IDL_CUDA(cudaMalloc(&ptr, need));
         bytes = need;
     }
+    void borrow(void* p, size_t n)
+    {
+        ptr = p;
+        bytes = n;
+        fixed = true;
+    }
     void release() noexcept
     {
-        if (ptr) cudaFree(ptr);
+        if (ptr && !fixed) cudaFree(ptr);
         ptr = nullptr;
         bytes = 0;
     }
@@ -113,6 +121,7 @@ struct Context {
 
     DevBuf scalars;       // one Scalars
     Scalars* host_sc = nullptr;  // pinned mirror
+    bool host_sc_borrowed = false;  // host_sc points at static storage, not cudaMallocHost memory
 
     int64_t last_n_tri = 0;      // triangles of the last triangulation (host copy)
     bool have_result = false;

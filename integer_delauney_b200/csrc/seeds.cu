@@ -85,24 +85,29 @@ __global__ void k_set_total(int32_t* __restrict__ out, int64_t n, const int32_t*
 
 void exclusive_scan(Context& C, const int32_t* in, int32_t* out, int64_t n)
 {
-    // level sizes
-    std::vector<int64_t> lens;
+    // level sizes (fixed-size bookkeeping: no host allocation on this path;
+    // 4096^8 items is far beyond any int32 count)
+    constexpr int MAX_LEVELS = 8;
+    int64_t lens[MAX_LEVELS];
+    int nlev = 0;
     int64_t m = n;
     for (;;) {
         const int64_t nb = (m + SCAN_TILE - 1) / SCAN_TILE;
-        lens.push_back(nb > 0 ? nb : 1);
+        if (nlev == MAX_LEVELS) throw Error(IDL_ERR_INTERNAL, "scan too large");
+        lens[nlev++] = nb > 0 ? nb : 1;
         if (nb <= 1) break;
         m = nb;
     }
     // scratch: per level, block sums (nb) and their scan (nb + 1)
     size_t need = 0;
-    for (int64_t nb : lens) need += size_t(2 * nb + 1);
+    for (int l = 0; l < nlev; ++l) need += size_t(2 * lens[l] + 1);
     C.scan_a.ensure(need * sizeof(int32_t));
     int32_t* arena = C.scan_a.as<int32_t>();
 
-    std::vector<int32_t*> sums(lens.size()), scans(lens.size());
+    int32_t* sums[MAX_LEVELS];
+    int32_t* scans[MAX_LEVELS];
     size_t at = 0;
-    for (size_t l = 0; l < lens.size(); ++l) {
+    for (int l = 0; l < nlev; ++l) {
         sums[l] = arena + at;  at += lens[l];
         scans[l] = arena + at; at += lens[l] + 1;
     }
@@ -110,7 +115,7 @@ void exclusive_scan(Context& C, const int32_t* in, int32_t* out, int64_t n)
     const int32_t* lin = in;
     int32_t* lout = out;
     int64_t len = n;
-    for (size_t l = 0; l < lens.size(); ++l) {
+    for (int l = 0; l < nlev; ++l) {
         const int64_t nb = lens[l];
         k_scan_block<<<(unsigned)nb, SCAN_THREADS, 0, C.stream>>>(lin, lout, len, sums[l]);
         IDL_LAUNCH();
@@ -124,7 +129,7 @@ void exclusive_scan(Context& C, const int32_t* in, int32_t* out, int64_t n)
         len = nb;
     }
     // up: add scanned block offsets back, deepest first
-    for (int l = int(lens.size()) - 2; l >= 0; --l) {
+    for (int l = nlev - 2; l >= 0; --l) {
         int32_t* target = (l == 0) ? out : scans[l - 1];
         const int64_t tlen = (l == 0) ? n : lens[l - 1];
         k_scan_add<<<(unsigned)((tlen + 255) / 256), 256, 0, C.stream>>>(target, tlen, scans[l]);
