@@ -54,6 +54,18 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def reduce_max(value: float, world: int) -> float:
+    """Max of a per-rank timing over all ranks (identity for one rank)."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -208,12 +220,8 @@ def run_ours(args, rank, world):
             e1.record(stream)
             torch.cuda.synchronize()
         launches = lib.idl_launch_count() - launches0
-        ms = e0.elapsed_time(e1)
+        ms = reduce_max(e0.elapsed_time(e1), world)
         ctx.set_profiling(False)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
         return ms, profs, clk.summary(), launches
 
     seeds_u = uniform(W, H, N_SEEDS, seed=rank)
@@ -263,11 +271,7 @@ def run_ours(args, rank, world):
         n_tri = len(verts)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_e = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms_e], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_e = float(t.item())
+    ms_e = reduce_max(e0.elapsed_time(e1), world)
     e2e = world * W * H * e_steps / (ms_e / 1e3) / 1e6
 
     if rank != 0:
