@@ -67,59 +67,66 @@ def reduce_max(value: float, world: int) -> float:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and throttle reasons of one GPU, polled through NVML (read
+    only) every few milliseconds while the timed region runs, plus one sample
+    on entry and one on exit so that even a short region is covered."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_S = 0.002
+    # NVML clocks-event reason bits (nvml.h): the ones a bench line must report.
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap"}
 
     def __init__(self, index: int):
         self.index = index
-        self.proc = None
-        self.lines = []
+        self.sm = []
+        self.mask = 0
+        self.max_mhz = None
+        self.nv = None
+        self.stop = threading.Event()
+
+    def _sample(self):
+        nv = self.nv
+        self.sm.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+        self.mask |= int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+
+    def _loop(self):
+        while not self.stop.wait(self.PERIOD_S):
+            try:
+                self._sample()
+            except Exception:
+                return
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nv = nv
+            self.h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            self._sample()
+            self.thread = threading.Thread(target=self._loop, daemon=True)
             self.thread.start()
         except Exception:
-            self.proc = None
+            self.nv = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except Exception:
-                self.proc.kill()
+        if self.nv is None:
+            return
+        self.stop.set()
+        self.thread.join(timeout=2)
+        try:
+            self._sample()
+            self.nv.nvmlShutdown()
+        except Exception:
+            pass
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        if not sm:
+        if not self.sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = sorted(nm for bit, nm in self.REASONS.items() if self.mask & bit)
+        return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.sm)}
 
 
 def cpu_baseline(sample_rows: int = 0):
@@ -225,8 +232,11 @@ def run_ours(args, rank, world):
         return ms, profs, clk.summary(), launches
 
     seeds_u = uniform(W, H, N_SEEDS, seed=rank)
-    ms, profs, clocks, launches = time_device(seeds_u, args.steps, args.warmup, profile=True)
+    # headline: K plain steps; the per-stage events are recorded in a second
+    # timed run, since profiling reads counters back between stages
+    ms, _, clocks, launches = time_device(seeds_u, args.steps, args.warmup, profile=False)
     value = world * W * H * args.steps / (ms / 1e3) / 1e6
+    _, profs, _, _ = time_device(seeds_u, args.steps, 1, profile=True)
 
     # stage breakdown and roofline of the dominant stage
     keys = ["seeds_ms", "propagate_ms", "detect_ms", "dedup_ms", "assign_ms", "compose_ms"]

@@ -170,6 +170,11 @@ void exclusive_scan(Context& C, const int32_t* in, int32_t* out, int64_t n);
 // by P).  Throws IDL_ERR_INVALID with the reference's messages.
 void sort_seeds_device(Context& C, int W, int H, int64_t n, int P);
 
+// (x asc, y asc) rank of n distinct, validated seeds given in insertion
+// order, and their coordinates scattered into sorted order (seeds.cu).
+void rank_seeds_device(Context& C, int W, int H, const int32_t* xs, const int32_t* ys, int64_t n, int32_t* rank,
+                       int32_t* xs_sorted, int32_t* ys_sorted);
+
 // Stage (a) on the Wd x Hd detection canvas whose labels are in C.lab[0]
 // (both planes must hold the same starting state).  Returns the pass count
 // (propagate.cu).  `first_tiles`: nullptr = every tile starts active;
@@ -177,10 +182,15 @@ void sort_seeds_device(Context& C, int W, int H, int64_t n, int P);
 struct Canvas {
     int Wd, Hd, pitch;
 };
-int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos);
+int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos = nullptr,
+                  int64_t n_new = 0);
 
 // Reference-semantics propagation as one persistent kernel (sparse_jacobi.cu).
-int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos);
+// `seed_pos` (may be nullptr): the state is a fixed point except at these
+// n_new freshly written seed cells (packed canvas positions), so only the
+// micro-tiles around them start active; otherwise every micro-tile does.
+int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos = nullptr,
+                         int64_t n_new = 0);
 
 // Reserve a range of per-item stamp values for `steps` steps (propagate.cu).
 int32_t claim_stamps(Context& C, int n_items, int64_t steps);
@@ -192,8 +202,10 @@ void init_labels(Context& C, const Canvas& cv, const uint32_t* pos, int64_t n);
 // (topology.cu).  Leaves the triangles in C.tris and their count in
 // C.sc()->n_triangles; returns nothing to the host.
 // `mid` (may be nullptr) is recorded between detection and deduplication.
+// `rank` (may be nullptr): labels are raw ids (the block rule runs on them);
+// keys, numbering and the recorded vertex ids use rank[label] instead.
 void detect_triangles(Context& C, const Canvas& cv, const int32_t* labels, const uint32_t* pos, int64_t n,
-                      int shift, cudaEvent_t mid = nullptr);
+                      int shift, cudaEvent_t mid = nullptr, const int32_t* rank = nullptr);
 
 // Stage (d): per-pixel max triangle id over a W x H image (raster.cu).
 void assign_pixels(Context& C, int W, int H, const int32_t* xs, const int32_t* ys, int32_t* tgrid,

@@ -333,9 +333,10 @@ int32_t claim_stamps(Context& C, int n_items, int64_t steps)
     return epoch;
 }
 
-int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos)
+int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
+                  int64_t n_new)
 {
-    if (mode == IDL_MODE_REFERENCE) return propagate_sparse(C, cv, pos);
+    if (mode == IDL_MODE_REFERENCE) return propagate_sparse(C, cv, pos, seed_pos, n_new);
     const int tiles_x = ceil_div(cv.Wd, TW), tiles_y = ceil_div(cv.Hd, TH);
     const int n_tiles = tiles_x * tiles_y;
     // Bound on rounds: far above any real run (a pass count beyond the canvas

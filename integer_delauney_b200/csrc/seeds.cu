@@ -183,7 +183,51 @@ __global__ void k_seed_rank(const int32_t* __restrict__ xy, int64_t n, int W, in
     pos[r] = pack_pos(x + P, y + P);
 }
 
+__global__ void k_mark_xy(const int32_t* __restrict__ xs, const int32_t* __restrict__ ys, int64_t n, int H,
+                          uint32_t* __restrict__ bitmap)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t bit = (int64_t)xs[i] * H + ys[i];
+    atomicOr(&bitmap[bit >> 5], 1u << (bit & 31));
+}
+
+__global__ void k_rank_xy(const int32_t* __restrict__ xs, const int32_t* __restrict__ ys, int64_t n, int H,
+                          const uint32_t* __restrict__ bitmap, const int32_t* __restrict__ word_rank,
+                          int32_t* __restrict__ rank, int32_t* __restrict__ xs_sorted, int32_t* __restrict__ ys_sorted)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t bit = (int64_t)xs[i] * H + ys[i];
+    const uint32_t below = bitmap[bit >> 5] & ((1u << (bit & 31)) - 1u);
+    const int32_t r = word_rank[bit >> 5] + __popc(below);
+    rank[i] = r;
+    xs_sorted[r] = xs[i];
+    ys_sorted[r] = ys[i];
+}
+
 }  // namespace
+
+void rank_seeds_device(Context& C, int W, int H, const int32_t* xs, const int32_t* ys, int64_t n, int32_t* rank,
+                       int32_t* xs_sorted, int32_t* ys_sorted)
+{
+    if (n <= 0) return;
+    const int64_t nwords = ((int64_t)W * H + 31) / 32;
+    C.bitmap.ensure(size_t(nwords) * 4);
+    C.scan_b.ensure(size_t(nwords) * 4);
+    C.scan_c.ensure(size_t(nwords + 1) * 4);
+    IDL_CUDA(cudaMemsetAsync(C.bitmap.ptr, 0, size_t(nwords) * 4, C.stream));
+    const unsigned gs = (unsigned)((n + 255) / 256);
+    k_mark_xy<<<gs, 256, 0, C.stream>>>(xs, ys, n, H, C.bitmap.as<uint32_t>());
+    IDL_LAUNCH();
+    k_popc<<<(unsigned)((nwords + 255) / 256), 256, 0, C.stream>>>(C.bitmap.as<uint32_t>(), nwords,
+                                                                  C.scan_b.as<int32_t>());
+    IDL_LAUNCH();
+    exclusive_scan(C, C.scan_b.as<int32_t>(), C.scan_c.as<int32_t>(), nwords);
+    k_rank_xy<<<gs, 256, 0, C.stream>>>(xs, ys, n, H, C.bitmap.as<uint32_t>(), C.scan_c.as<int32_t>(), rank,
+                                        xs_sorted, ys_sorted);
+    IDL_LAUNCH();
+}
 
 void sort_seeds_device(Context& C, int W, int H, int64_t n, int P)
 {

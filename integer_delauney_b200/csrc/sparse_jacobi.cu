@@ -268,6 +268,26 @@ __global__ void k_iota_list(int32_t* __restrict__ list, int n, int32_t* __restri
     if (i == 0) *count = n;
 }
 
+// Initial work list of a continued propagation: the micro-tiles holding a new
+// seed cell or one of its 4 neighbours (the only cells pass 0 can change).
+__global__ void k_seed_tiles(const uint32_t* __restrict__ seed_pos, int n_new, int Wd, int Hd, int mt_x,
+                             uint32_t* __restrict__ bits, int32_t* __restrict__ list, int32_t* __restrict__ count)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_new) return;
+    const uint32_t p = seed_pos[i];
+    const int x = pos_x(p), y = pos_y(p);
+    const int dx[5] = {0, -1, 1, 0, 0}, dy[5] = {0, 0, 0, -1, 1};
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+        const int cx = x + dx[j], cy = y + dy[j];
+        if (cx < 0 || cy < 0 || cx >= Wd || cy >= Hd) continue;
+        const int mt = (cy / MT) * mt_x + cx / MT;
+        const uint32_t bit = 1u << (mt & 31);
+        if (!(atomicOr(&bits[mt >> 5], bit) & bit)) list[atomicAdd(count, 1)] = mt;
+    }
+}
+
 __global__ void k_fill_bits(uint32_t* __restrict__ bits, int n_words, int n_items)
 {
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
@@ -278,7 +298,8 @@ __global__ void k_fill_bits(uint32_t* __restrict__ bits, int n_words, int n_item
 
 }  // namespace
 
-int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos)
+int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
+                         int64_t n_new)
 {
     const int mt_x = ceil_div(cv.Wd, MT), mt_y = ceil_div(cv.Hd, MT);
     const int n_mt = mt_x * mt_y;
@@ -290,16 +311,24 @@ int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos)
     C.bits.ensure((size_t)n_words * 2 * 4);
     uint32_t* b0 = C.bits.as<uint32_t>();
     uint32_t* b1 = b0 + n_words;
-    k_fill_bits<<<(unsigned)((n_words + 255) / 256), 256, 0, C.stream>>>(b0, n_words, n_mt);
-    IDL_LAUNCH();
-    IDL_CUDA(cudaMemsetAsync(b1, 0, (size_t)n_words * 4, C.stream));
     C.counts.ensure(((size_t)max_steps + 2) * 4);
     IDL_CUDA(cudaMemsetAsync(C.counts.ptr, 0, ((size_t)max_steps + 2) * 4, C.stream));
     int32_t* counts = C.counts.as<int32_t>();
     int32_t* l0 = C.tiles[0].as<int32_t>();
     int32_t* l1 = C.tiles[1].as<int32_t>();
-    k_iota_list<<<(unsigned)((n_mt + 255) / 256), 256, 0, C.stream>>>(l0, n_mt, counts);
-    IDL_LAUNCH();
+    if (seed_pos) {
+        if (n_new == 0) return 0;
+        IDL_CUDA(cudaMemsetAsync(b0, 0, (size_t)n_words * 2 * 4, C.stream));
+        k_seed_tiles<<<(unsigned)((n_new + 255) / 256), 256, 0, C.stream>>>(seed_pos, (int)n_new, cv.Wd, cv.Hd,
+                                                                            mt_x, b0, l0, counts);
+        IDL_LAUNCH();
+    } else {
+        k_fill_bits<<<(unsigned)((n_words + 255) / 256), 256, 0, C.stream>>>(b0, n_words, n_mt);
+        IDL_LAUNCH();
+        IDL_CUDA(cudaMemsetAsync(b1, 0, (size_t)n_words * 4, C.stream));
+        k_iota_list<<<(unsigned)((n_mt + 255) / 256), 256, 0, C.stream>>>(l0, n_mt, counts);
+        IDL_LAUNCH();
+    }
     C.gsync.ensure(sizeof(GridSync));
     IDL_CUDA(cudaMemsetAsync(C.gsync.ptr, 0, sizeof(GridSync), C.stream));
 

@@ -134,8 +134,13 @@ __device__ __forceinline__ void block_rule(int32_t a, int32_t b, int32_t c, int3
 }
 
 // Sorted key plus a 4-bit code of the order the block saw the vertices in.
-__device__ __forceinline__ void make_key(const int32_t o[3], unsigned long long& key, unsigned& code)
+// With a rank map the key and the recorded ids are ranks (the numbering the
+// outputs use) while the rule itself ran on the raw labels.
+__device__ __forceinline__ void make_key(const int32_t in[3], const int32_t* __restrict__ rank, unsigned long long& key,
+                                         unsigned& code)
 {
+    const int32_t o[3] = {rank ? __ldg(&rank[in[0]]) : in[0], rank ? __ldg(&rank[in[1]]) : in[1],
+                          rank ? __ldg(&rank[in[2]]) : in[2]};
     int32_t a = o[0], b = o[1], c = o[2], t;
     if (a > b) { t = a; a = b; b = t; }
     if (b > c) { t = b; b = c; c = t; }
@@ -166,8 +171,8 @@ __device__ __forceinline__ void hash_insert(unsigned long long key, unsigned lon
 
 __global__ void __launch_bounds__(256)
 k_detect(const int32_t* __restrict__ lab, int pitch, int Wd, int Hd, const uint32_t* __restrict__ pos,
-         unsigned long long* __restrict__ keys, unsigned long long* __restrict__ vals, unsigned long long mask,
-         Scalars* __restrict__ sc)
+         const int32_t* __restrict__ rank, unsigned long long* __restrict__ keys,
+         unsigned long long* __restrict__ vals, unsigned long long mask, Scalars* __restrict__ sc)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -182,7 +187,7 @@ k_detect(const int32_t* __restrict__ lab, int pitch, int Wd, int Hd, const uint3
     for (int k = 0; k < e.n; ++k) {
         unsigned long long key;
         unsigned code;
-        make_key(e.o[k], key, code);
+        make_key(e.o[k], rank, key, code);
         hash_insert(key, (blk << 4) | code, keys, vals, mask, sc);
     }
 }
@@ -260,7 +265,7 @@ __global__ void k_rank(const unsigned long long* __restrict__ ukeys, const unsig
 }  // namespace
 
 void detect_triangles(Context& C, const Canvas& cv, const int32_t* labels, const uint32_t* pos, int64_t n,
-                      int shift, cudaEvent_t mid)
+                      int shift, cudaEvent_t mid, const int32_t* rank)
 {
     // Unique triangles of a planar triangulation number under 2n; keep the
     // table at most half full, and grow and redo on the rare overflow.
@@ -277,7 +282,7 @@ void detect_triangles(Context& C, const Canvas& cv, const int32_t* labels, const
 
         dim3 blk(32, 8);
         dim3 grd(ceil_div(std::max(cv.Wd - 1, 1), 32), ceil_div(std::max(cv.Hd - 1, 1), 8));
-        k_detect<<<grd, blk, 0, C.stream>>>(labels, cv.pitch, cv.Wd, cv.Hd, pos, C.hkeys.as<unsigned long long>(),
+        k_detect<<<grd, blk, 0, C.stream>>>(labels, cv.pitch, cv.Wd, cv.Hd, pos, rank, C.hkeys.as<unsigned long long>(),
                                             C.hvals.as<unsigned long long>(), (unsigned long long)(cap - 1), C.sc());
         IDL_LAUNCH();
         if (mid) IDL_CUDA(cudaEventRecord(mid, C.stream));
