@@ -191,6 +191,140 @@ IDL_API int idl_triangles_device(idl_context* ctx, const int32_t** d_tris, const
 IDL_API int idl_voronoi_noalloc(int width, int height, const int32_t* d_seeds_xy, int64_t n_seeds, int mode,
                                 int32_t* d_grid_out, void* stream, int64_t* passes_out);
 
+/* ==== incremental triangulation (stage (c)) ============================
+ * An idl_delaunay holds one growing seed set on a padded canvas and keeps its
+ * Voronoi diagram, triangles and pixel assignment on the device between
+ * calls.  It replaces the reference's class Delaunay (src/cuda/delaunay.cuh,
+ * bound as _delauney_cuda.Delaunay in src/cuda/bindings/py_delaunay.hpp).
+ *
+ * Seed ids.  Internally seeds are numbered in insertion order (0, 1, ...).
+ * Outputs that the reference reports in batch numbering -- the triangle map
+ * and grid of finalise, the Voronoi grid, finalise_device's views -- use the
+ * (x asc, y asc) rank of each seed instead, exactly as the reference
+ * translates through sorted_rank (src/cuda/delaunay_output.cu:39-110);
+ * get_triangles / get_edges / get_seeds keep insertion ids, as there.
+ *
+ * Propagation.  IDL_MODE_REFERENCE continues the Jacobi iteration from the
+ * previous fixed point after writing the new seeds, the reference's own
+ * incremental trajectory (src/cuda/delaunay_voronoi.cu:12-108), ties going to
+ * the higher insertion id.
+ *
+ * Triangles.  Detection runs on the insertion-id grid (the block rule's
+ * lowest-id tie-break sees insertion ids, as in the reference) and triangles
+ * are numbered canonically: triangle id = rank of the sorted triple of batch
+ * ids, so ids are dense, deterministic and equal to the batch pipeline's.
+ * (The reference numbers by registry slot order, src/cuda/delaunay_topology.cu:
+ * 360-414, which depends on the insertion history.)  Pixels take the highest
+ * id of the triangles containing them, over the whole triangle set. */
+typedef struct idl_delaunay idl_delaunay;
+
+/* Per-object info slots (idl_delaunay_info). */
+#define IDL_DI_SEED_COUNT 0
+#define IDL_DI_WIDTH 1
+#define IDL_DI_HEIGHT 2
+#define IDL_DI_BORDER_PADDING 3
+#define IDL_DI_HAS_PENDING 4
+#define IDL_DI_GENERATION 5
+#define IDL_DI_MAX_SEEDS 6
+#define IDL_DI_MODE 7
+#define IDL_DI_HAS_VALUES 8
+#define IDL_DI_COUNT 9
+
+/* Delaunay::Delaunay (src/cuda/delaunay.cu:24-112).  Allocates every canvas-
+ * sized buffer up front; border_padding < 0 selects IDL_DEFAULT_BORDER_PADDING.
+ * Errors: width, height or max_seeds <= 0 -> IDL_ERR_INVALID ("dimensions and
+ * max_seeds must be positive"); an allocation failure -> IDL_ERR_CUDA naming
+ * cudaMalloc and this library's delaunay.cu. */
+IDL_API int idl_delaunay_create(int device, int width, int height, int64_t max_seeds, int border_padding, int mode,
+                                idl_delaunay** out);
+IDL_API int idl_delaunay_destroy(idl_delaunay* d);
+/* Order the object's work on `stream` (a cudaStream_t; NULL = legacy default). */
+IDL_API int idl_delaunay_set_stream(idl_delaunay* d, void* stream);
+
+/* Delaunay::insert_deferred (src/cuda/delaunay.cu:276-323 with apply_batch_,
+ * :184-268): validate and append k seeds (host int32 x, y pairs), write them
+ * into the diagram and propagate.  values: NULL or k host floats, the scalar
+ * field at the new seeds.  timings_out: NULL or IDL_T_COUNT floats; when
+ * given, topology is also brought up to date inside the call so that
+ * IDL_T_DETECT_MS / IDL_T_DEDUP_MS describe this insert.  k == 0 is a no-op.
+ * Errors (nothing is changed): capacity, bounds and duplicate violations ->
+ * IDL_ERR_INVALID with the reference's messages. */
+IDL_API int idl_delaunay_insert(idl_delaunay* d, const int32_t* seeds_xy, int64_t k, const float* values,
+                                float* timings_out);
+
+/* Delaunay::finalise (src/cuda/delaunay.cu:325-347): assign pixels for the
+ * pending changes and write the (height, width, 3) int32 grid (batch seed id,
+ * squared distance, triangle id) to host grid_out (may be NULL).  Reports the
+ * triangle count; idl_delaunay_triangles returns the map.  timings_out: NULL or
+ * IDL_T_COUNT floats (detect/dedup/assign of the work this call did). */
+IDL_API int idl_delaunay_finalise(idl_delaunay* d, int32_t* grid_out, int64_t* n_triangles_out, float* timings_out);
+
+/* Delaunay::finalise_device (src/cuda/delaunay.cu:349-361 and
+ * crop_pixel_arrays_kernel, src/cuda/delaunay_output.cu:120-144): as finalise,
+ * but the per-pixel results stay on the device, as three object-owned arrays
+ * of width*height entries: triangle id (no triangle -> 0), batch seed id, and
+ * a uint8 mask, 1 where no triangle contains the pixel.  They stay valid until
+ * *generation_out changes (any insert, finalise or finalise_device call). */
+IDL_API int idl_delaunay_finalise_device(idl_delaunay* d, int64_t* n_triangles_out, const int32_t** d_pixel_tids,
+                                         const int32_t** d_pixel_seed_ids, const uint8_t** d_outside_mask,
+                                         uint64_t* generation_out);
+
+/* Triangles of the current topology, in triangle-id order.
+ *   ids = 0: 5 int32 per triangle (x, y, a, b, c) in batch seed ids, (x, y)
+ *            the witnessing block in image coordinates -- finalise's map
+ *            (Delaunay::build_tri_map_, src/cuda/delaunay_output.cu:68-84);
+ *   ids = 1: 3 int32 per triangle (a, b, c) in insertion ids --
+ *            Delaunay::get_triangles (src/cuda/delaunay_output.cu:186-200).
+ * Valid between deferred inserts.  *n_out = triangle count; tris_out may be
+ * NULL to query the count; otherwise capacity (int32 entries) must hold it. */
+IDL_API int idl_delaunay_triangles(idl_delaunay* d, int ids, int32_t* tris_out, int64_t capacity, int64_t* n_out);
+
+/* Delaunay::get_edges (src/cuda/delaunay_scalar_field.cu:293-312): distinct
+ * undirected edges (a, b), a < b, insertion ids, ascending by (a, b). */
+IDL_API int idl_delaunay_edges(idl_delaunay* d, int32_t* edges_out, int64_t capacity, int64_t* n_out);
+
+/* Delaunay::edge_scores (src/cuda/delaunay_scalar_field.cu:206-224): per
+ * edge of idl_delaunay_edges, |v[a] - v[b]| * |p[a] - p[b]| computed in
+ * double and rounded to float, 0 for edges shorter than min_length.
+ * IDL_ERR_STATE when no values were ever inserted (and edges exist). */
+IDL_API int idl_delaunay_edge_scores(idl_delaunay* d, double min_length, float* scores_out, int64_t capacity,
+                                     int64_t* n_out);
+
+/* Delaunay::select_midpoints (src/cuda/delaunay_scalar_field.cu:226-291):
+ * midpoints (x, y) of the `count` best edges under (score desc, edge index
+ * asc) among those scoring above threshold, dropping midpoints on existing
+ * seeds and collisions (lowest rank kept), ascending by padded pixel index. */
+IDL_API int idl_delaunay_select_midpoints(idl_delaunay* d, double min_length, int count, float threshold,
+                                          int32_t* xy_out, int64_t capacity, int64_t* n_out);
+
+/* Delaunay::locate (src/cuda/delaunay_query.cu:187-227): triangle id
+ * containing each of n query points (x, y int32 pairs, image coordinates), or
+ * -1.  Valid before any finalise; agrees with the finalised grid. */
+IDL_API int idl_delaunay_locate(idl_delaunay* d, const int32_t* pts_xy, int64_t n, int32_t* tids_out);
+
+/* Delaunay::in_circumsphere (src/cuda/delaunay_query.cu:33-185): for each
+ * query, whether (x, y, t) lies strictly inside the circumsphere of the
+ * triangle containing (x, y) lifted to t = 0 (uint8 0/1), and that triangle. */
+IDL_API int idl_delaunay_in_circumsphere(idl_delaunay* d, const int32_t* pts_xy, const double* t, int64_t n,
+                                         uint8_t* mask_out, int32_t* tids_out);
+
+/* Delaunay::get_seeds / get_values (src/cuda/delaunay_output.cu:202-224):
+ * insertion-order seeds (seed_count x, y pairs) and the values inserted
+ * with them (as many floats as were given; *n_values_out). */
+IDL_API int idl_delaunay_seeds(idl_delaunay* d, int32_t* xy_out, float* values_out, int64_t* n_values_out);
+
+/* Delaunay::sorted_rank (src/cuda/delaunay.cuh:245-247): insertion id ->
+ * batch (x asc, y asc) id, seed_count int32. */
+IDL_API int idl_delaunay_sorted_rank(idl_delaunay* d, int32_t* rank_out);
+
+/* Delaunay::get_voronoi_grid (src/cuda/delaunay_output.cu:162-184): the
+ * (height, width, 2) int32 grid (batch seed id, squared distance); -1, -1
+ * where no seed has reached. */
+IDL_API int idl_delaunay_voronoi(idl_delaunay* d, int32_t* grid_out);
+
+/* Object properties (IDL_DI_* slots; src/cuda/delaunay.cuh:249-254). */
+IDL_API int idl_delaunay_info(idl_delaunay* d, int64_t* info_out, int count);
+
 #ifdef __cplusplus
 }
 #endif

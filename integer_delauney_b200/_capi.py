@@ -55,7 +55,29 @@ SIGNATURES = {
     "idl_triangulate_device": (_i32, [_vp, _i32, _i32, _vp, _i64, _i32, _i32, _vp, _pi64]),
     "idl_triangles_device": (_i32, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "idl_voronoi_noalloc": (_i32, [_i32, _i32, _vp, _i64, _i32, _vp, _vp, _pi64]),
+    # incremental triangulation
+    "idl_delaunay_create": (_i32, [_i32, _i32, _i32, _i64, _i32, _i32, ctypes.POINTER(_vp)]),
+    "idl_delaunay_destroy": (_i32, [_vp]),
+    "idl_delaunay_set_stream": (_i32, [_vp, _vp]),
+    "idl_delaunay_insert": (_i32, [_vp, _vp, _i64, _vp, _vp]),
+    "idl_delaunay_finalise": (_i32, [_vp, _vp, _pi64, _vp]),
+    "idl_delaunay_finalise_device": (_i32, [_vp, _pi64, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
+                                            ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_uint64)]),
+    "idl_delaunay_triangles": (_i32, [_vp, _i32, _vp, _i64, _pi64]),
+    "idl_delaunay_edges": (_i32, [_vp, _vp, _i64, _pi64]),
+    "idl_delaunay_edge_scores": (_i32, [_vp, ctypes.c_double, _vp, _i64, _pi64]),
+    "idl_delaunay_select_midpoints": (_i32, [_vp, ctypes.c_double, _i32, ctypes.c_float, _vp, _i64, _pi64]),
+    "idl_delaunay_locate": (_i32, [_vp, _vp, _i64, _vp]),
+    "idl_delaunay_in_circumsphere": (_i32, [_vp, _vp, _vp, _i64, _vp, _vp]),
+    "idl_delaunay_seeds": (_i32, [_vp, _vp, _vp, _pi64]),
+    "idl_delaunay_sorted_rank": (_i32, [_vp, _vp]),
+    "idl_delaunay_voronoi": (_i32, [_vp, _vp]),
+    "idl_delaunay_info": (_i32, [_vp, _pi64, _i32]),
 }
+
+# idl_delaunay_info slots
+(DI_SEED_COUNT, DI_WIDTH, DI_HEIGHT, DI_BORDER_PADDING, DI_HAS_PENDING, DI_GENERATION, DI_MAX_SEEDS, DI_MODE,
+ DI_HAS_VALUES, DI_COUNT) = range(10)
 
 _lib = None
 _lib_lock = threading.Lock()

@@ -191,3 +191,283 @@ class GridTriangulation:
         tris, grid, _, padded = _triangulate(W, H, s, vg, border_padding, voronoi_mode, debug=True)
         m, g = build_output(tris, grid, False)
         return m, g, padded
+
+
+# ---------------------------------------------------------------------------
+# Incremental triangulation (src/cuda/bindings/py_delaunay.hpp,
+# src/cuda/bindings/py_device_array_view.hpp)
+# ---------------------------------------------------------------------------
+
+def _timings_dict(t) -> dict:
+    """The keys of PyDelaunay::_timings_dict (py_delaunay.hpp:268-277)."""
+    return {"bfs_ms": float(t[_capi.T_BFS_MS]), "bfs_iters": int(t[_capi.T_BFS_ITERS]),
+            "detect_ms": float(t[_capi.T_DETECT_MS]), "dedup_ms": float(t[_capi.T_DEDUP_MS]),
+            "assign_ms": float(t[_capi.T_ASSIGN_MS])}
+
+
+def _points(points) -> np.ndarray:
+    q = np.ascontiguousarray(np.asarray(points), dtype=np.int32)
+    if q.ndim != 2 or q.shape[1] != 2:
+        raise ValueError("points must have shape (N, 2)")
+    return q
+
+
+class DeviceArrayView:
+    """Read-only ``__cuda_array_interface__`` (v3) onto one of a Delaunay
+    object's device arrays (py_device_array_view.hpp:29-89).
+
+    Holds a reference to its Delaunay, so the memory outlives every view; it
+    raises RuntimeError once the Delaunay has moved to a new generation (any
+    insert, finalise or finalise_device after the one that made the view)."""
+
+    def __init__(self, owner, ptr: int, count: int, typestr: str, generation: int):
+        self._owner = owner
+        self._ptr = int(ptr)
+        self._count = int(count)
+        self._typestr = typestr
+        self._generation = int(generation)
+
+    def _check_fresh(self):
+        if self._owner._generation() != self._generation:
+            raise RuntimeError("device view is stale: the mesh was mutated after "
+                               "finalise_device() produced this view")
+
+    @property
+    def __cuda_array_interface__(self) -> dict:
+        self._check_fresh()
+        return {"shape": (self._count,), "typestr": self._typestr, "data": (self._ptr, True),
+                "strides": None, "version": 3}
+
+    def to_host(self) -> np.ndarray:
+        """Host NumPy copy of the view's content."""
+        self._check_fresh()
+        dtype = np.int32 if self._typestr == "<i4" else np.uint8
+        if torch is None:
+            raise RuntimeError("to_host() needs torch for the device copy")
+        out = np.empty(self._count, dtype=dtype)
+        if self._count:
+            # torch refuses read-only interfaces; the copy below only reads
+            inner = type("_Raw", (), {"__cuda_array_interface__": {
+                "shape": (self._count,), "typestr": self._typestr, "data": (self._ptr, False),
+                "strides": None, "version": 3}})()
+            with torch.cuda.device(self._owner._device):
+                torch.cuda.current_stream().synchronize()
+                out[:] = torch.as_tensor(inner, device=f"cuda:{self._owner._device}").cpu().numpy()
+        return out
+
+
+class Delaunay:
+    """Incremental Delaunay triangulator with device-resident state
+    (src/cuda/delaunay.cuh:22-378, bound in py_delaunay.hpp:11-305).
+
+    Seeds keep insertion-order ids internally; the triangle map and grids of
+    insert / finalise and the Voronoi grid use the batch (x asc, y asc) ids,
+    as the reference translates through ``sorted_rank``.  Triangle ids are the
+    batch pipeline's canonical ids (rank of the sorted vertex triple), so
+    they are dense after every call and independent of the insertion history.
+    """
+
+    def __init__(self, width: int, height: int, max_seeds: int, border_padding: int = AUTO_BORDER_PADDING, *,
+                 voronoi_mode="reference"):
+        import threading
+        self._lib = _capi.load()
+        self._h = None
+        self._device = _device()
+        self._lock = threading.Lock()
+        h = ctypes.c_void_p()
+        check(self._lib.idl_delaunay_create(self._device, int(width), int(height), int(max_seeds),
+                                            int(border_padding), mode_id(voronoi_mode), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            try:
+                self._lib.idl_delaunay_destroy(h)
+            except Exception:   # pragma: no cover - interpreter shutdown
+                pass
+
+    # -- plumbing ------------------------------------------------------------
+    def _call(self, name, *args):
+        with self._lock:
+            if torch is not None and torch.cuda.is_available():
+                stream = torch.cuda.current_stream(self._device).cuda_stream
+                check(self._lib.idl_delaunay_set_stream(self._h, stream))
+            check(getattr(self._lib, name)(self._h, *args))
+
+    def _info(self) -> np.ndarray:
+        info = np.zeros(_capi.DI_COUNT, dtype=np.int64)
+        check(self._lib.idl_delaunay_info(self._h, info.ctypes.data_as(_capi._pi64), _capi.DI_COUNT))
+        return info
+
+    def _generation(self) -> int:
+        return int(self._info()[_capi.DI_GENERATION])
+
+    def _tris(self, ids: int) -> np.ndarray:
+        n = ctypes.c_int64(0)
+        self._call("idl_delaunay_triangles", ids, None, 0, ctypes.byref(n))
+        cols = 5 if ids == 0 else 3
+        out = np.empty((n.value, cols), dtype=np.int32)
+        if n.value:
+            self._call("idl_delaunay_triangles", ids, out.ctypes.data, out.size, ctypes.byref(n))
+        return out
+
+    def _insert(self, seeds, values, timings: bool):
+        s = parse_seeds(seeds)
+        v = None
+        if values is not None:
+            v = np.ascontiguousarray(np.asarray(values, dtype=np.float32).reshape(-1))
+            if len(v) != len(s):
+                raise ValueError("values must have one entry per seed in the batch")
+        t = (ctypes.c_float * _capi.T_COUNT)() if timings else None
+        self._call("idl_delaunay_insert", s.ctypes.data if len(s) else None, len(s),
+                   v.ctypes.data if (v is not None and len(v)) else None,
+                   ctypes.cast(t, ctypes.c_void_p) if t is not None else None)
+        return t
+
+    def _finalise(self, as_arrays: bool, timings: bool):
+        H, W = self.height, self.width
+        grid = _host_buffer((H, W, 3))
+        n = ctypes.c_int64(0)
+        t = (ctypes.c_float * _capi.T_COUNT)() if timings else None
+        self._call("idl_delaunay_finalise", grid.ctypes.data, ctypes.byref(n),
+                   ctypes.cast(t, ctypes.c_void_p) if t is not None else None)
+        m, g = build_output(self._tris(0), grid, as_arrays)
+        return m, g, t
+
+    # -- reference API ---------------------------------------------------------
+    def insert(self, seeds, as_arrays: bool = False):
+        """Append a batch and return (triangle_map | verts, grid (H, W, 3))."""
+        self._insert(seeds, None, False)
+        m, g, _ = self._finalise(as_arrays, False)
+        return m, g
+
+    def insert_timed(self, seeds, as_arrays: bool = False):
+        t0 = self._insert(seeds, None, True)
+        m, g, t1 = self._finalise(as_arrays, True)
+        d = _timings_dict(t0)
+        d["assign_ms"] = float(t1[_capi.T_ASSIGN_MS])
+        d["detect_ms"] += float(t1[_capi.T_DETECT_MS])
+        d["dedup_ms"] += float(t1[_capi.T_DEDUP_MS])
+        return m, g, d
+
+    def insert_deferred(self, seeds, values=None) -> None:
+        """Append a batch (and optionally its scalar values) without assigning pixels."""
+        self._insert(seeds, values, False)
+
+    def insert_deferred_timed(self, seeds) -> dict:
+        return _timings_dict(self._insert(seeds, None, True))
+
+    def finalise(self, as_arrays: bool = False):
+        m, g, _ = self._finalise(as_arrays, False)
+        return m, g
+
+    def finalise_timed(self, as_arrays: bool = False):
+        m, g, t = self._finalise(as_arrays, True)
+        return m, g, _timings_dict(t)
+
+    def finalise_device(self):
+        """(verts (N_tri, 3), pixel_tids, pixel_seed_ids, outside_hull_mask) with
+        the three per-pixel arrays as device views (py_delaunay.hpp:65-91)."""
+        n = ctypes.c_int64(0)
+        p_t, p_s, p_m = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        gen = ctypes.c_uint64(0)
+        self._call("idl_delaunay_finalise_device", ctypes.byref(n), ctypes.byref(p_t), ctypes.byref(p_s),
+                   ctypes.byref(p_m), ctypes.byref(gen))
+        verts = np.ascontiguousarray(self._tris(0)[:, 2:5])
+        count = self.width * self.height
+        return (verts, DeviceArrayView(self, p_t.value or 0, count, "<i4", gen.value),
+                DeviceArrayView(self, p_s.value or 0, count, "<i4", gen.value),
+                DeviceArrayView(self, p_m.value or 0, count, "|u1", gen.value))
+
+    def get_triangles(self) -> np.ndarray:
+        """(N_tri, 3) vertex ids in INSERTION order, rows in triangle-id order."""
+        return self._tris(1)
+
+    def get_edges(self) -> np.ndarray:
+        n = ctypes.c_int64(0)
+        self._call("idl_delaunay_edges", None, 0, ctypes.byref(n))
+        out = np.empty((n.value, 2), dtype=np.int32)
+        if n.value:
+            self._call("idl_delaunay_edges", out.ctypes.data, out.size, ctypes.byref(n))
+        return out
+
+    def edge_scores(self, min_length: float = 0.0) -> np.ndarray:
+        n = ctypes.c_int64(0)
+        self._call("idl_delaunay_edge_scores", float(min_length), None, 0, ctypes.byref(n))
+        out = np.empty(n.value, dtype=np.float32)
+        if n.value:
+            self._call("idl_delaunay_edge_scores", float(min_length), out.ctypes.data, out.size, ctypes.byref(n))
+        return out
+
+    def select_midpoints(self, min_length: float, count: int, threshold: float = 0.0) -> np.ndarray:
+        cap = max(int(count), 0)
+        out = np.empty((cap, 2), dtype=np.int32)
+        n = ctypes.c_int64(0)
+        self._call("idl_delaunay_select_midpoints", float(min_length), int(count), float(threshold),
+                   out.ctypes.data if cap else None, out.size, ctypes.byref(n))
+        return out[: n.value].copy()
+
+    def in_circumsphere(self, points, t):
+        q = _points(points)
+        tt = np.ascontiguousarray(np.asarray(t, dtype=np.float64).reshape(-1))
+        if len(tt) != len(q):
+            raise ValueError("t must have one entry per point")
+        mask = np.zeros(len(q), dtype=np.uint8)
+        tids = np.full(len(q), -1, dtype=np.int32)
+        if len(q):
+            self._call("idl_delaunay_in_circumsphere", q.ctypes.data, tt.ctypes.data, len(q), mask.ctypes.data,
+                       tids.ctypes.data)
+        return mask.astype(bool), tids
+
+    def locate(self, points) -> np.ndarray:
+        q = _points(points)
+        out = np.full(len(q), -1, dtype=np.int32)
+        if len(q):
+            self._call("idl_delaunay_locate", q.ctypes.data, len(q), out.ctypes.data)
+        return out
+
+    def get_seeds(self) -> np.ndarray:
+        out = np.empty((self.seed_count, 2), dtype=np.int32)
+        self._call("idl_delaunay_seeds", out.ctypes.data if out.size else None, None, None)
+        return out
+
+    def get_values(self) -> np.ndarray:
+        n = ctypes.c_int64(0)
+        self._call("idl_delaunay_seeds", None, None, ctypes.byref(n))
+        out = np.empty(n.value, dtype=np.float32)
+        if n.value:
+            self._call("idl_delaunay_seeds", None, out.ctypes.data, ctypes.byref(n))
+        return out
+
+    @property
+    def sorted_rank(self) -> np.ndarray:
+        out = np.empty(self.seed_count, dtype=np.int32)
+        if out.size:
+            self._call("idl_delaunay_sorted_rank", out.ctypes.data)
+        return out
+
+    def get_voronoi_grid(self) -> np.ndarray:
+        out = _host_buffer((self.height, self.width, 2))
+        self._call("idl_delaunay_voronoi", out.ctypes.data)
+        return out
+
+    @property
+    def seed_count(self) -> int:
+        return int(self._info()[_capi.DI_SEED_COUNT])
+
+    @property
+    def width(self) -> int:
+        return int(self._info()[_capi.DI_WIDTH])
+
+    @property
+    def height(self) -> int:
+        return int(self._info()[_capi.DI_HEIGHT])
+
+    @property
+    def border_padding(self) -> int:
+        return int(self._info()[_capi.DI_BORDER_PADDING])
+
+    @property
+    def has_pending(self) -> bool:
+        return bool(self._info()[_capi.DI_HAS_PENDING])

@@ -171,9 +171,10 @@ void exclusive_scan(Context& C, const int32_t* in, int32_t* out, int64_t n);
 void sort_seeds_device(Context& C, int W, int H, int64_t n, int P);
 
 // (x asc, y asc) rank of n distinct, validated seeds given in insertion
-// order, and their coordinates scattered into sorted order (seeds.cu).
-void rank_seeds_device(Context& C, int W, int H, const int32_t* xs, const int32_t* ys, int64_t n, int32_t* rank,
-                       int32_t* xs_sorted, int32_t* ys_sorted);
+// order (seeds.cu): rank[i], its inverse inv[rank[i]] = i, and the
+// coordinates plus `off` scattered into sorted order.
+void rank_seeds_device(Context& C, int W, int H, const int32_t* xs, const int32_t* ys, int64_t n, int off,
+                       int32_t* rank, int32_t* inv, int32_t* xs_sorted, int32_t* ys_sorted);
 
 // Stage (a) on the Wd x Hd detection canvas whose labels are in C.lab[0]
 // (both planes must hold the same starting state).  Returns the pass count

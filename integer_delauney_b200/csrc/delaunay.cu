@@ -1,0 +1,899 @@
+// Stage (c): incremental triangulation -- one growing seed set whose Voronoi
+// diagram, triangles and pixel assignment stay on the device between calls.
+// Replaces the reference's class Delaunay (src/cuda/delaunay.cu,
+// delaunay_voronoi.cu, delaunay_topology.cu, delaunay_assign.cu,
+// delaunay_output.cu, delaunay_query.cu, delaunay_scalar_field.cu).
+//
+// State on the device, all sized at construction:
+//   planes   two pitch x Hd int32 label planes of the padded canvas, holding
+//            insertion-order seed ids (both planes equal between calls);
+//   tgrid    Wd x Hd int32 triangle ids of the padded canvas;
+//   seed arrays (max_seeds each): image x, y; packed canvas position; batch
+//            rank and its inverse; canvas x, y in batch order; values;
+//   pixel    W x H triangle id, batch seed id and outside mask for
+//            finalise_device.
+// Triangles and grow-only query scratch live in the embedded Context.
+//
+// An insert writes the new seeds into both planes and continues the Jacobi
+// iteration from the previous fixed point (delaunay_voronoi.cu:60-108) with the
+// persistent sparse kernel, whose first work list is just the micro-tiles
+// around the new seeds: everything else is already a fixed point.  Topology
+// (detection + canonical numbering) and the raster are recomputed lazily, when
+// something reads them, from the whole canvas: detection of a 2080 x 2080
+// canvas is a few tens of microseconds on the device, so a per-insert dirty
+// region and slot registry (delaunay_topology.cu:185-414) would only add host
+// work, and canonical numbering keeps triangle ids dense and history-free.
+#include "context.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_select.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <unordered_set>
+#include <vector>
+
+namespace idl {
+
+struct DelaunayState {
+    Context C;
+    int W = 0, H = 0, P = 0, Wd = 0, Hd = 0, pitch = 0;
+    int64_t max_seeds = 0;
+    int mode = IDL_MODE_REFERENCE;
+    int64_t N = 0;
+    uint64_t generation = 0;
+    bool pending = false;
+    bool rank_dirty = false, topo_dirty = false, raster_dirty = false, edges_dirty = true;
+    bool have_values = false;
+    int64_t n_tri = 0, n_edges = 0;
+
+    // device memory owned by this object (allocated in create)
+    int32_t* planes = nullptr;
+    int32_t* tgrid = nullptr;
+    int32_t* seedmem = nullptr;
+    void* pixmem = nullptr;
+    int32_t *ix = nullptr, *iy = nullptr, *rank = nullptr, *inv = nullptr, *sx = nullptr, *sy = nullptr;
+    uint32_t* pos = nullptr;
+    float* values = nullptr;
+    int32_t *pix_tid = nullptr, *pix_sid = nullptr;
+    uint8_t* pix_out = nullptr;
+
+    // grow-only scratch
+    DevBuf stage, edge_keys, edge_tmp, sort_tmp, num_sel, scores, score_keys, score_sorted, qbuf, qout;
+
+    // host mirrors (insertion order, image coordinates)
+    std::vector<int32_t> hx, hy;
+    std::vector<float> hvals;
+    std::unordered_set<uint64_t> seen;
+
+    Canvas canvas() const { return Canvas{Wd, Hd, pitch}; }
+
+    void free_owned() noexcept
+    {
+        if (planes) cudaFree(planes);
+        if (tgrid) cudaFree(tgrid);
+        if (seedmem) cudaFree(seedmem);
+        if (pixmem) cudaFree(pixmem);
+        planes = tgrid = seedmem = nullptr;
+        pixmem = nullptr;
+        DevBuf* all[] = {&stage, &edge_keys, &edge_tmp, &sort_tmp, &num_sel, &scores, &score_keys, &score_sorted,
+                         &qbuf, &qout};
+        for (DevBuf* b : all) b->release();
+    }
+    ~DelaunayState() { free_owned(); }
+};
+
+}  // namespace idl
+
+struct idl_delaunay : idl::DelaunayState {};
+
+namespace idl {
+namespace {
+
+inline uint64_t pack_xy(int32_t x, int32_t y) { return ((uint64_t)(uint32_t)x << 32) | (uint32_t)y; }
+
+// ---- kernels ------------------------------------------------------------
+
+// New seeds take ids first_id, first_id + 1, ... in both planes
+// (write_seeds_kernel, delaunay_voronoi.cu:12-25).
+__global__ void k_put_seeds(int32_t* __restrict__ a, int32_t* __restrict__ b, int pitch,
+                            const uint32_t* __restrict__ pos, int64_t k, int64_t first_id)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k) return;
+    const uint32_t p = pos[i];
+    const size_t o = (size_t)pos_y(p) * pitch + pos_x(p);
+    a[o] = (int32_t)(first_id + i);
+    b[o] = (int32_t)(first_id + i);
+}
+
+__device__ __forceinline__ void cell_out(const int32_t* __restrict__ lab, int pitch, int P, int x, int y,
+                                         const uint32_t* __restrict__ pos, const int32_t* __restrict__ rank,
+                                         int32_t& sid, int32_t& d)
+{
+    const int32_t l = lab[(size_t)(y + P) * pitch + x + P];
+    sid = l >= 0 ? __ldg(&rank[l]) : UNDEF;
+    d = l >= 0 ? dist2(x + P, y + P, __ldg(&pos[l])) : -1;
+}
+
+// (H, W, 3): batch seed id, squared distance, triangle id
+// (Delaunay::build_outputs_, delaunay_output.cu:86-110).
+__global__ void k_out3(const int32_t* __restrict__ lab, int pitch, int P, int W, int H,
+                       const uint32_t* __restrict__ pos, const int32_t* __restrict__ rank,
+                       const int32_t* __restrict__ tgrid, int Wd, int32_t* __restrict__ out)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    int32_t sid, d;
+    cell_out(lab, pitch, P, x, y, pos, rank, sid, d);
+    int32_t* o = out + ((size_t)y * W + x) * 3;
+    o[0] = sid;
+    o[1] = d;
+    o[2] = tgrid[(size_t)(y + P) * Wd + x + P];
+}
+
+// (H, W, 2): batch seed id, squared distance (delaunay_output.cu:162-184).
+__global__ void k_out2(const int32_t* __restrict__ lab, int pitch, int P, int W, int H,
+                       const uint32_t* __restrict__ pos, const int32_t* __restrict__ rank, int32_t* __restrict__ out)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    int32_t sid, d;
+    cell_out(lab, pitch, P, x, y, pos, rank, sid, d);
+    out[((size_t)y * W + x) * 2] = sid;
+    out[((size_t)y * W + x) * 2 + 1] = d;
+}
+
+// finalise_device's three arrays (crop_pixel_arrays_kernel,
+// delaunay_output.cu:120-144).
+__global__ void k_crop(const int32_t* __restrict__ lab, int pitch, int P, int W, int H,
+                       const int32_t* __restrict__ rank, const int32_t* __restrict__ tgrid, int Wd,
+                       int32_t* __restrict__ tid_out, int32_t* __restrict__ sid_out, uint8_t* __restrict__ mask_out)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W) return;
+    const int32_t l = lab[(size_t)(y + P) * pitch + x + P];
+    const size_t d = (size_t)y * W + x;
+    sid_out[d] = l >= 0 ? __ldg(&rank[l]) : l;
+    const int32_t t = tgrid[(size_t)(y + P) * Wd + x + P];
+    mask_out[d] = t == NO_TRIANGLE ? 1 : 0;
+    tid_out[d] = t == NO_TRIANGLE ? 0 : t;
+}
+
+// Vertex ids of the canonical triangle rows mapped back to insertion ids.
+__global__ void k_tris_insertion(const int32_t* __restrict__ tris, int64_t n, const int32_t* __restrict__ inv,
+                                 int32_t* __restrict__ out)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) out[t * 3 + j] = __ldg(&inv[tris[t * 5 + 2 + j]]);
+}
+
+// Three undirected edge keys a * n + b (a < b, insertion ids) per triangle
+// (build_edge_keys_kernel, delaunay_scalar_field.cu:34-56).
+__global__ void k_edge_keys(const int32_t* __restrict__ tris, int64_t n_tri, const int32_t* __restrict__ inv,
+                            int64_t n_seeds, unsigned long long* __restrict__ keys)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_tri) return;
+    int32_t v[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) v[j] = __ldg(&inv[tris[t * 5 + 2 + j]]);
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const int32_t p = min(v[e], v[(e + 1) % 3]), q = max(v[e], v[(e + 1) % 3]);
+        keys[t * 3 + e] = (unsigned long long)p * (unsigned long long)n_seeds + (unsigned long long)q;
+    }
+}
+
+__global__ void k_edge_unpack(const unsigned long long* __restrict__ keys, int64_t n_edges, int64_t n_seeds,
+                              int32_t* __restrict__ out)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_edges) return;
+    const unsigned long long k = keys[i];
+    out[i * 2] = (int32_t)(k / (unsigned long long)n_seeds);
+    out[i * 2 + 1] = (int32_t)(k % (unsigned long long)n_seeds);
+}
+
+// |dv| * |ab| in double, rounded to float; 0 below min_length
+// (score_edges_kernel, delaunay_scalar_field.cu:84-103).
+__global__ void k_edge_scores(const unsigned long long* __restrict__ keys, int64_t n_edges, int64_t n_seeds,
+                              const int32_t* __restrict__ x, const int32_t* __restrict__ y,
+                              const float* __restrict__ values, double min_len2, float* __restrict__ scores)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_edges) return;
+    const unsigned long long k = keys[e];
+    const int32_t a = (int32_t)(k / (unsigned long long)n_seeds), b = (int32_t)(k % (unsigned long long)n_seeds);
+    const double dx = (double)x[a] - (double)x[b];
+    const double dy = (double)y[a] - (double)y[b];
+    const double len2 = dx * dx + dy * dy;
+    if (len2 < min_len2) {
+        scores[e] = 0.f;
+        return;
+    }
+    const double dv = fabs((double)values[a] - (double)values[b]);
+    scores[e] = (float)(dv * sqrt(len2));
+}
+
+// Best-first sort key: complemented score bits over the edge index; edges at
+// or below the threshold get the all-ones high word (pack_score_keys_kernel,
+// delaunay_scalar_field.cu:105-127).
+__global__ void k_score_keys(const float* __restrict__ scores, int64_t n, float threshold,
+                             unsigned long long* __restrict__ keys)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float s = scores[i];
+    uint32_t hi = 0xFFFFFFFFu;
+    if (s > threshold && s > 0.f) hi = ~__float_as_uint(s);
+    keys[i] = ((unsigned long long)hi << 32) | (uint32_t)i;
+}
+
+// Endpoints (insertion ids) of the first `take` edges in sorted key order.
+__global__ void k_take_edges(const unsigned long long* __restrict__ sorted, int take,
+                             const unsigned long long* __restrict__ edge_keys, int64_t n_seeds,
+                             int32_t* __restrict__ out)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= take) return;
+    const uint32_t e = (uint32_t)(sorted[r] & 0xFFFFFFFFull);
+    const unsigned long long k = edge_keys[e];
+    out[r * 2] = (int32_t)(k / (unsigned long long)n_seeds);
+    out[r * 2 + 1] = (int32_t)(k % (unsigned long long)n_seeds);
+}
+
+// Containing triangle of each query (image coordinates), read from the
+// padded raster, which holds the highest id over every triangle containing
+// the pixel.
+__global__ void k_locate(const int32_t* __restrict__ q, int64_t n, int P, int Wd, int Hd,
+                         const int32_t* __restrict__ tgrid, int32_t* __restrict__ out)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int x = q[i * 2] + P, y = q[i * 2 + 1] + P;
+    out[i] = (x < 0 || y < 0 || x >= Wd || y >= Hd) ? NO_TRIANGLE : tgrid[(size_t)y * Wd + x];
+}
+
+// Lifted in-circle predicate (in_circumsphere_kernel,
+// delaunay_query.cu:33-104): circumcentre in the reference's operation order
+// on padded coordinates, radius = farthest vertex, distances compared (not
+// their squares), all in double.
+__global__ void k_circumsphere(const int32_t* __restrict__ q, const double* __restrict__ qt, int64_t n, int P,
+                               int Wd, int Hd, const int32_t* __restrict__ tgrid, const int32_t* __restrict__ tris,
+                               const int32_t* __restrict__ sx, const int32_t* __restrict__ sy,
+                               uint8_t* __restrict__ mask, int32_t* __restrict__ tid_out)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    mask[i] = 0;
+    const int x = q[i * 2] + P, y = q[i * 2 + 1] + P;
+    if (x < 0 || y < 0 || x >= Wd || y >= Hd) {
+        tid_out[i] = NO_TRIANGLE;
+        return;
+    }
+    const int32_t tid = tgrid[(size_t)y * Wd + x];
+    tid_out[i] = tid;
+    if (tid == NO_TRIANGLE) return;
+    const int32_t* t = tris + (size_t)tid * 5;
+    const double ax = sx[t[2]], ay = sy[t[2]];
+    const double bx = sx[t[3]], by = sy[t[3]];
+    const double cx = sx[t[4]], cy = sy[t[4]];
+    const double abx = bx - ax, aby = by - ay;
+    const double acx = cx - ax, acy = cy - ay;
+    const double nz = abx * acy - aby * acx;
+    double ox, oy;
+    if (nz * nz < 1e-12) {
+        ox = (ax + bx + cx) / 3.0;
+        oy = (ay + by + cy) / 3.0;
+    } else {
+        const double ab2 = abx * abx + aby * aby;
+        const double ac2 = acx * acx + acy * acy;
+        const double den = 2.0 * (nz * nz);
+        const double num_x = ac2 * (-(nz * aby)) + ab2 * (acy * nz);
+        const double num_y = ac2 * (nz * abx) + ab2 * (-(acx * nz));
+        ox = ax + num_x / den;
+        oy = ay + num_y / den;
+    }
+    const double r2 = fmax(fmax((ax - ox) * (ax - ox) + (ay - oy) * (ay - oy),
+                                (bx - ox) * (bx - ox) + (by - oy) * (by - oy)),
+                           (cx - ox) * (cx - ox) + (cy - oy) * (cy - oy));
+    const double dx = (double)x - ox, dy = (double)y - oy, tt = qt[i];
+    mask[i] = sqrt(dx * dx + dy * dy + tt * tt) < sqrt(r2) ? 1 : 0;
+}
+
+// ---- host helpers ---------------------------------------------------------
+
+inline unsigned blocks(int64_t n, int t = 256) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
+
+struct Timer {
+    Context& C;
+    bool on;
+    cudaEvent_t a = nullptr, b = nullptr;
+    Timer(Context& c, bool enabled) : C(c), on(enabled)
+    {
+        if (!on) return;
+        IDL_CUDA(cudaEventCreate(&a));
+        IDL_CUDA(cudaEventCreate(&b));
+        IDL_CUDA(cudaEventRecord(a, C.stream));
+    }
+    float stop()
+    {
+        if (!on) return 0.f;
+        IDL_CUDA(cudaEventRecord(b, C.stream));
+        IDL_CUDA(cudaEventSynchronize(b));
+        float ms = 0.f;
+        IDL_CUDA(cudaEventElapsedTime(&ms, a, b));
+        return ms;
+    }
+    ~Timer()
+    {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
+void ensure_rank(DelaunayState& D)
+{
+    if (!D.rank_dirty) return;
+    rank_seeds_device(D.C, D.W, D.H, D.ix, D.iy, D.N, D.P, D.rank, D.inv, D.sx, D.sy);
+    D.rank_dirty = false;
+}
+
+void ensure_topology(DelaunayState& D, float* timings)
+{
+    if (!D.topo_dirty) return;
+    ensure_rank(D);
+    Context& C = D.C;
+    if (D.N < 3) {
+        D.n_tri = 0;
+    } else {
+        cudaEvent_t e[3] = {};
+        if (timings)
+            for (auto& ev : e) IDL_CUDA(cudaEventCreate(&ev));
+        try {
+            if (timings) IDL_CUDA(cudaEventRecord(e[0], C.stream));
+            detect_triangles(C, D.canvas(), D.planes, D.pos, D.N, D.P, timings ? e[1] : nullptr, D.rank);
+            if (timings) IDL_CUDA(cudaEventRecord(e[2], C.stream));
+            C.fetch_scalars();
+            D.n_tri = C.host_sc->n_triangles;
+            if (timings) {
+                float a = 0.f, b = 0.f;
+                IDL_CUDA(cudaEventElapsedTime(&a, e[0], e[1]));
+                IDL_CUDA(cudaEventElapsedTime(&b, e[1], e[2]));
+                timings[IDL_T_DETECT_MS] += a;
+                timings[IDL_T_DEDUP_MS] += b;
+            }
+        } catch (...) {
+            for (auto& ev : e)
+                if (ev) cudaEventDestroy(ev);
+            throw;
+        }
+        for (auto& ev : e)
+            if (ev) cudaEventDestroy(ev);
+    }
+    D.topo_dirty = false;
+}
+
+// The padded canvas raster: every pixel's highest containing triangle id
+// (the batch rule of triangulation.cu:101-137 over the whole triangle set).
+void ensure_raster(DelaunayState& D, float* timings)
+{
+    ensure_topology(D, timings);
+    if (!D.raster_dirty) return;
+    Timer T(D.C, timings != nullptr);
+    assign_pixels(D.C, D.Wd, D.Hd, D.sx, D.sy, D.tgrid, D.n_tri);
+    const float ms = T.stop();
+    if (timings) timings[IDL_T_ASSIGN_MS] += ms;
+    D.raster_dirty = false;
+}
+
+void ensure_edges(DelaunayState& D)
+{
+    ensure_topology(D, nullptr);
+    if (!D.edges_dirty) return;
+    Context& C = D.C;
+    D.n_edges = 0;
+    if (D.n_tri > 0) {
+        const int64_t m = D.n_tri * 3;
+        D.edge_tmp.ensure((size_t)m * 8);
+        D.edge_keys.ensure((size_t)m * 8);
+        D.num_sel.ensure(8);
+        auto* raw = D.edge_tmp.as<unsigned long long>();
+        auto* srt = D.edge_keys.as<unsigned long long>();
+        k_edge_keys<<<blocks(D.n_tri), 256, 0, C.stream>>>(C.tris.as<int32_t>(), D.n_tri, D.inv, D.N, raw);
+        IDL_LAUNCH();
+        const unsigned long long top = (unsigned long long)D.N * (unsigned long long)D.N;
+        int end_bit = 1;
+        while (end_bit < 64 && (top >> end_bit) != 0) ++end_bit;
+        size_t need_sort = 0, need_uniq = 0;
+        IDL_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, need_sort, raw, srt, (int)m, 0, end_bit, C.stream));
+        IDL_CUDA(cub::DeviceSelect::Unique(nullptr, need_uniq, srt, raw, D.num_sel.as<int>(), (int)m, C.stream));
+        D.sort_tmp.ensure(std::max(need_sort, need_uniq));
+        size_t tb = D.sort_tmp.bytes;
+        IDL_CUDA(cub::DeviceRadixSort::SortKeys(D.sort_tmp.ptr, tb, raw, srt, (int)m, 0, end_bit, C.stream));
+        tb = D.sort_tmp.bytes;
+        IDL_CUDA(cub::DeviceSelect::Unique(D.sort_tmp.ptr, tb, srt, raw, D.num_sel.as<int>(), (int)m, C.stream));
+        int n = 0;
+        IDL_CUDA(cudaMemcpyAsync(&n, D.num_sel.ptr, sizeof(int), cudaMemcpyDeviceToHost, C.stream));
+        IDL_CUDA(cudaStreamSynchronize(C.stream));
+        std::swap(D.edge_tmp, D.edge_keys);   // unique keys now in edge_keys
+        D.n_edges = n;
+    }
+    D.edges_dirty = false;
+}
+
+void compute_scores(DelaunayState& D, double min_length)
+{
+    D.scores.ensure((size_t)std::max<int64_t>(1, D.n_edges) * 4);
+    k_edge_scores<<<blocks(D.n_edges), 256, 0, D.C.stream>>>(D.edge_keys.as<unsigned long long>(), D.n_edges, D.N,
+                                                             D.ix, D.iy, D.values, min_length * min_length,
+                                                             D.scores.as<float>());
+    IDL_LAUNCH();
+}
+
+const int32_t* upload_queries(DelaunayState& D, const int32_t* pts, int64_t n)
+{
+    D.qbuf.ensure((size_t)n * 2 * 4);
+    IDL_CUDA(cudaMemcpyAsync(D.qbuf.ptr, pts, (size_t)n * 2 * 4, cudaMemcpyHostToDevice, D.C.stream));
+    return D.qbuf.as<int32_t>();
+}
+
+void check_handle(const idl_delaunay* d)
+{
+    if (!d) invalid("Delaunay handle must not be NULL");
+}
+
+}  // namespace
+}  // namespace idl
+
+using namespace idl;
+
+extern "C" {
+
+int idl_delaunay_create(int device, int width, int height, int64_t max_seeds, int border_padding, int mode,
+                        idl_delaunay** out)
+{
+    IDL_API_BEGIN
+    if (!out) invalid("out must not be NULL");
+    *out = nullptr;
+    if (width <= 0 || height <= 0 || max_seeds <= 0) invalid("dimensions and max_seeds must be positive");
+    if (max_seeds > MAX_SEEDS) invalid("max_seeds exceeds the 2097151 seeds this build can number");
+    if (mode != IDL_MODE_REFERENCE)
+        invalid("the incremental Delaunay supports voronoi_mode 'reference' only in this build");
+    int dev = device;
+    if (dev < 0) IDL_CUDA(cudaGetDevice(&dev));
+    DeviceGuard g(dev);
+    auto* d = new idl_delaunay();
+    try {
+        d->C.device = dev;
+        IDL_CUDA(cudaDeviceGetAttribute(&d->C.num_sms, cudaDevAttrMultiProcessorCount, dev));
+        ensure_scalars(d->C);
+        d->W = width;
+        d->H = height;
+        d->P = border_padding >= 0 ? border_padding : IDL_DEFAULT_BORDER_PADDING;
+        d->max_seeds = max_seeds;
+        d->mode = mode;
+        const int64_t Wd = (int64_t)width + 2 * d->P, Hd = (int64_t)height + 2 * d->P;
+        const int64_t pitch = (Wd + 31) / 32 * 32;
+        // The canvas-sized buffers first: a canvas no GPU can hold fails here,
+        // as a CUDA allocation error, before any size rule of this build.
+        IDL_CUDA(cudaMalloc(&d->planes, (size_t)pitch * Hd * 2 * sizeof(int32_t)));
+        IDL_CUDA(cudaMalloc(&d->tgrid, (size_t)Wd * Hd * sizeof(int32_t)));
+        IDL_CUDA(cudaMalloc(&d->pixmem, (size_t)width * height * 9));
+        IDL_CUDA(cudaMalloc(&d->seedmem, (size_t)max_seeds * 8 * sizeof(int32_t)));
+        if (Wd > MAX_CANVAS_SIDE || Hd > MAX_CANVAS_SIDE)
+            invalid("padded canvas side exceeds the 32767 pixels this build addresses");
+        d->Wd = (int)Wd;
+        d->Hd = (int)Hd;
+        d->pitch = (int)pitch;
+        int32_t* s = d->seedmem;
+        d->ix = s;
+        d->iy = s + max_seeds;
+        d->pos = reinterpret_cast<uint32_t*>(s + 2 * max_seeds);
+        d->rank = s + 3 * max_seeds;
+        d->inv = s + 4 * max_seeds;
+        d->sx = s + 5 * max_seeds;
+        d->sy = s + 6 * max_seeds;
+        d->values = reinterpret_cast<float*>(s + 7 * max_seeds);
+        d->pix_tid = static_cast<int32_t*>(d->pixmem);
+        d->pix_sid = d->pix_tid + (size_t)width * height;
+        d->pix_out = reinterpret_cast<uint8_t*>(d->pix_sid + (size_t)width * height);
+        const size_t plane = (size_t)pitch * Hd;
+        d->C.lab[0].borrow(d->planes, plane * 4);
+        d->C.lab[1].borrow(d->planes + plane, plane * 4);
+        IDL_CUDA(cudaMemset(d->planes, 0xFF, plane * 2 * sizeof(int32_t)));
+        IDL_CUDA(cudaMemset(d->tgrid, 0xFF, (size_t)Wd * Hd * sizeof(int32_t)));
+        IDL_CUDA(cudaMemset(d->values, 0, (size_t)max_seeds * sizeof(float)));
+        IDL_CUDA(cudaDeviceSynchronize());
+    } catch (...) {
+        delete d;
+        throw;
+    }
+    *out = d;
+    IDL_API_END
+}
+
+int idl_delaunay_destroy(idl_delaunay* d)
+{
+    IDL_API_BEGIN
+    if (!d) return IDL_OK;
+    DeviceGuard g(d->C.device);
+    cudaStreamSynchronize(d->C.stream);
+    delete d;
+    IDL_API_END
+}
+
+int idl_delaunay_set_stream(idl_delaunay* d, void* stream)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    d->C.stream = static_cast<cudaStream_t>(stream);
+    IDL_API_END
+}
+
+int idl_delaunay_insert(idl_delaunay* d, const int32_t* xy, int64_t k, const float* values, float* timings)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    if (timings)
+        for (int i = 0; i < IDL_T_COUNT; ++i) timings[i] = 0.f;
+    if (k < 0) invalid("seed count must not be negative");
+    if (k == 0) return IDL_OK;
+    if (!xy) invalid("seeds must not be NULL");
+    // validation before any change (delaunay.cu:190-212)
+    if (d->N + k > d->max_seeds) invalid("insert would exceed max_seeds capacity");
+    for (int64_t i = 0; i < k; ++i) {
+        const int32_t x = xy[2 * i], y = xy[2 * i + 1];
+        if (x < 0 || x >= d->W || y < 0 || y >= d->H) invalid("seed coordinate out of bounds");
+    }
+    {
+        std::unordered_set<uint64_t> batch;
+        batch.reserve((size_t)k * 2);
+        for (int64_t i = 0; i < k; ++i) {
+            const uint64_t key = pack_xy(xy[2 * i], xy[2 * i + 1]);
+            if (!batch.insert(key).second) invalid("duplicate seed positions within batch");
+            if (d->seen.count(key)) invalid("seed position already exists");
+        }
+    }
+    DeviceGuard g(d->C.device);
+    Context& C = d->C;
+    ++d->generation;
+    const int64_t n0 = d->N;
+    std::vector<int32_t> host((size_t)k * 3);
+    for (int64_t i = 0; i < k; ++i) {
+        const int32_t x = xy[2 * i], y = xy[2 * i + 1];
+        host[i] = x;
+        host[k + i] = y;
+        host[2 * k + i] = (int32_t)(uint32_t(x + d->P) | (uint32_t(y + d->P) << 16));
+        d->hx.push_back(x);
+        d->hy.push_back(y);
+        d->seen.insert(pack_xy(x, y));
+    }
+    IDL_CUDA(cudaMemcpyAsync(d->ix + n0, host.data(), (size_t)k * 4, cudaMemcpyHostToDevice, C.stream));
+    IDL_CUDA(cudaMemcpyAsync(d->iy + n0, host.data() + k, (size_t)k * 4, cudaMemcpyHostToDevice, C.stream));
+    IDL_CUDA(cudaMemcpyAsync(d->pos + n0, host.data() + 2 * k, (size_t)k * 4, cudaMemcpyHostToDevice, C.stream));
+    if (values) {
+        IDL_CUDA(cudaMemcpyAsync(d->values + n0, values, (size_t)k * 4, cudaMemcpyHostToDevice, C.stream));
+        d->hvals.insert(d->hvals.end(), values, values + k);
+        d->have_values = true;
+    }
+    d->N += k;
+    d->rank_dirty = d->topo_dirty = d->raster_dirty = d->edges_dirty = true;
+    d->pending = true;
+
+    Timer T(C, timings != nullptr);
+    k_put_seeds<<<blocks(k), 256, 0, C.stream>>>(d->planes, d->planes + (size_t)d->pitch * d->Hd, d->pitch,
+                                                 d->pos + n0, k, n0);
+    IDL_LAUNCH();
+    const int64_t passes = propagate(C, d->mode, d->canvas(), d->pos, d->pos + n0, k);
+    const float bfs = T.stop();
+    if (timings) {
+        timings[IDL_T_BFS_MS] = bfs;
+        timings[IDL_T_BFS_ITERS] = (float)passes;
+        ensure_topology(*d, timings);
+    }
+    IDL_API_END
+}
+
+int idl_delaunay_finalise(idl_delaunay* d, int32_t* grid_out, int64_t* n_tri_out, float* timings)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    if (timings)
+        for (int i = 0; i < IDL_T_COUNT; ++i) timings[i] = 0.f;
+    DeviceGuard g(d->C.device);
+    Context& C = d->C;
+    ensure_rank(*d);
+    ensure_raster(*d, timings);
+    if (d->pending) {
+        d->pending = false;
+        ++d->generation;
+    }
+    if (grid_out) {
+        const size_t bytes = (size_t)d->W * d->H * 3 * 4;
+        C.outgrid.ensure(bytes);
+        if (d->N == 0) {
+            IDL_CUDA(cudaMemsetAsync(C.outgrid.ptr, 0xFF, bytes, C.stream));
+        } else {
+            dim3 gr(blocks(d->W), d->H);
+            k_out3<<<gr, 256, 0, C.stream>>>(d->planes, d->pitch, d->P, d->W, d->H, d->pos, d->rank, d->tgrid, d->Wd,
+                                            C.outgrid.as<int32_t>());
+            IDL_LAUNCH();
+        }
+        IDL_CUDA(cudaMemcpyAsync(grid_out, C.outgrid.ptr, bytes, cudaMemcpyDeviceToHost, C.stream));
+    }
+    IDL_CUDA(cudaStreamSynchronize(C.stream));
+    if (n_tri_out) *n_tri_out = d->n_tri;
+    IDL_API_END
+}
+
+int idl_delaunay_finalise_device(idl_delaunay* d, int64_t* n_tri_out, const int32_t** tids,
+                                 const int32_t** sids, const uint8_t** mask, uint64_t* generation_out)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    DeviceGuard g(d->C.device);
+    Context& C = d->C;
+    ++d->generation;
+    ensure_rank(*d);
+    ensure_raster(*d, nullptr);
+    d->pending = false;
+    dim3 gr(blocks(d->W), d->H);
+    k_crop<<<gr, 256, 0, C.stream>>>(d->planes, d->pitch, d->P, d->W, d->H, d->rank, d->tgrid, d->Wd, d->pix_tid,
+                                     d->pix_sid, d->pix_out);
+    IDL_LAUNCH();
+    if (n_tri_out) *n_tri_out = d->n_tri;
+    if (tids) *tids = d->pix_tid;
+    if (sids) *sids = d->pix_sid;
+    if (mask) *mask = d->pix_out;
+    if (generation_out) *generation_out = d->generation;
+    IDL_API_END
+}
+
+int idl_delaunay_triangles(idl_delaunay* d, int ids, int32_t* out, int64_t capacity, int64_t* n_out)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    if (ids != 0 && ids != 1) invalid("ids must be 0 (batch) or 1 (insertion order)");
+    DeviceGuard g(d->C.device);
+    Context& C = d->C;
+    ensure_topology(*d, nullptr);
+    if (n_out) *n_out = d->n_tri;
+    if (!out || d->n_tri == 0) return IDL_OK;
+    const int cols = ids == 0 ? 5 : 3;
+    if (capacity < d->n_tri * cols) invalid("triangle buffer too small");
+    if (ids == 0) {
+        IDL_CUDA(cudaMemcpyAsync(out, C.tris.ptr, (size_t)d->n_tri * 5 * 4, cudaMemcpyDeviceToHost, C.stream));
+    } else {
+        d->stage.ensure((size_t)d->n_tri * 3 * 4);
+        k_tris_insertion<<<blocks(d->n_tri), 256, 0, C.stream>>>(C.tris.as<int32_t>(), d->n_tri, d->inv,
+                                                                 d->stage.as<int32_t>());
+        IDL_LAUNCH();
+        IDL_CUDA(cudaMemcpyAsync(out, d->stage.ptr, (size_t)d->n_tri * 3 * 4, cudaMemcpyDeviceToHost, C.stream));
+    }
+    IDL_CUDA(cudaStreamSynchronize(C.stream));
+    IDL_API_END
+}
+
+int idl_delaunay_edges(idl_delaunay* d, int32_t* out, int64_t capacity, int64_t* n_out)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    DeviceGuard g(d->C.device);
+    Context& C = d->C;
+    ensure_edges(*d);
+    if (n_out) *n_out = d->n_edges;
+    if (!out || d->n_edges == 0) return IDL_OK;
+    if (capacity < d->n_edges * 2) invalid("edge buffer too small");
+    d->stage.ensure((size_t)d->n_edges * 2 * 4);
+    k_edge_unpack<<<blocks(d->n_edges), 256, 0, C.stream>>>(d->edge_keys.as<unsigned long long>(), d->n_edges, d->N,
+                                                            d->stage.as<int32_t>());
+    IDL_LAUNCH();
+    IDL_CUDA(cudaMemcpyAsync(out, d->stage.ptr, (size_t)d->n_edges * 2 * 4, cudaMemcpyDeviceToHost, C.stream));
+    IDL_CUDA(cudaStreamSynchronize(C.stream));
+    IDL_API_END
+}
+
+int idl_delaunay_edge_scores(idl_delaunay* d, double min_length, float* out, int64_t capacity, int64_t* n_out)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    DeviceGuard g(d->C.device);
+    ensure_edges(*d);
+    if (n_out) *n_out = d->n_edges;
+    if (d->n_edges == 0) return IDL_OK;
+    if (!d->have_values)
+        throw Error(IDL_ERR_STATE, "edge_scores needs a value per seed; pass values to insert_deferred");
+    if (!out) return IDL_OK;
+    if (capacity < d->n_edges) invalid("score buffer too small");
+    compute_scores(*d, min_length);
+    IDL_CUDA(cudaMemcpyAsync(out, d->scores.ptr, (size_t)d->n_edges * 4, cudaMemcpyDeviceToHost, d->C.stream));
+    IDL_CUDA(cudaStreamSynchronize(d->C.stream));
+    IDL_API_END
+}
+
+int idl_delaunay_select_midpoints(idl_delaunay* d, double min_length, int count, float threshold, int32_t* out,
+                                  int64_t capacity, int64_t* n_out)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    if (n_out) *n_out = 0;
+    DeviceGuard g(d->C.device);
+    Context& C = d->C;
+    ensure_edges(*d);
+    if (d->n_edges == 0 || count <= 0) return IDL_OK;
+    if (!d->have_values)
+        throw Error(IDL_ERR_STATE, "select_midpoints needs a value per seed; pass values to insert_deferred");
+    const int64_t E = d->n_edges;
+    compute_scores(*d, min_length);
+    d->score_keys.ensure((size_t)E * 8);
+    d->score_sorted.ensure((size_t)E * 8);
+    k_score_keys<<<blocks(E), 256, 0, C.stream>>>(d->scores.as<float>(), E, threshold,
+                                                  d->score_keys.as<unsigned long long>());
+    IDL_LAUNCH();
+    size_t need = 0;
+    IDL_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, need, d->score_keys.as<unsigned long long>(),
+                                            d->score_sorted.as<unsigned long long>(), (int)E, 0, 64, C.stream));
+    d->sort_tmp.ensure(need);
+    size_t tb = d->sort_tmp.bytes;
+    IDL_CUDA(cub::DeviceRadixSort::SortKeys(d->sort_tmp.ptr, tb, d->score_keys.as<unsigned long long>(),
+                                            d->score_sorted.as<unsigned long long>(), (int)E, 0, 64, C.stream));
+    // the eligible edges sort first; take at most `count` of them
+    const int64_t look = std::min<int64_t>(count, E);
+    std::vector<unsigned long long> head((size_t)look);
+    IDL_CUDA(cudaMemcpyAsync(head.data(), d->score_sorted.ptr, (size_t)look * 8, cudaMemcpyDeviceToHost, C.stream));
+    IDL_CUDA(cudaStreamSynchronize(C.stream));
+    int take = 0;
+    while (take < look && (head[take] >> 32) != 0xFFFFFFFFull) ++take;
+    if (take == 0) return IDL_OK;
+    d->stage.ensure((size_t)take * 2 * 4);
+    k_take_edges<<<blocks(take), 256, 0, C.stream>>>(d->score_sorted.as<unsigned long long>(), take,
+                                                     d->edge_keys.as<unsigned long long>(), d->N,
+                                                     d->stage.as<int32_t>());
+    IDL_LAUNCH();
+    std::vector<int32_t> ab((size_t)take * 2);
+    IDL_CUDA(cudaMemcpyAsync(ab.data(), d->stage.ptr, ab.size() * 4, cudaMemcpyDeviceToHost, C.stream));
+    IDL_CUDA(cudaStreamSynchronize(C.stream));
+    // midpoints on the padded canvas, rounded half to even as lrint does
+    // (midpoints_from_sorted_kernel, delaunay_scalar_field.cu:129-160)
+    std::vector<std::pair<int64_t, int>> cand;
+    cand.reserve(take);
+    const int P = d->P;
+    for (int r = 0; r < take; ++r) {
+        const int32_t a = ab[2 * r], b = ab[2 * r + 1];
+        int mx = (int)std::lrint(0.5 * ((double)(d->hx[a] + P) + (double)(d->hx[b] + P)));
+        int my = (int)std::lrint(0.5 * ((double)(d->hy[a] + P) + (double)(d->hy[b] + P)));
+        mx = std::min(std::max(mx, P), d->Wd - 1 - P);
+        my = std::min(std::max(my, P), d->Hd - 1 - P);
+        if (d->seen.count(pack_xy(mx - P, my - P))) continue;
+        cand.emplace_back((int64_t)my * d->Wd + mx, r);
+    }
+    std::sort(cand.begin(), cand.end());
+    std::vector<int32_t> res;
+    for (size_t i = 0; i < cand.size(); ++i) {
+        if (i > 0 && cand[i].first == cand[i - 1].first) continue;
+        res.push_back((int32_t)(cand[i].first % d->Wd) - P);
+        res.push_back((int32_t)(cand[i].first / d->Wd) - P);
+    }
+    const int64_t n = (int64_t)res.size() / 2;
+    if (n_out) *n_out = n;
+    if (out) {
+        if (capacity < n * 2) invalid("midpoint buffer too small");
+        std::copy(res.begin(), res.end(), out);
+    }
+    IDL_API_END
+}
+
+int idl_delaunay_locate(idl_delaunay* d, const int32_t* pts, int64_t n, int32_t* out)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    if (n < 0) invalid("query count must not be negative");
+    if (n == 0) return IDL_OK;
+    if (!pts || !out) invalid("query and output buffers must not be NULL");
+    DeviceGuard g(d->C.device);
+    Context& C = d->C;
+    ensure_rank(*d);
+    ensure_raster(*d, nullptr);
+    const int32_t* q = upload_queries(*d, pts, n);
+    d->qout.ensure((size_t)n * 4);
+    k_locate<<<blocks(n), 256, 0, C.stream>>>(q, n, d->P, d->Wd, d->Hd, d->tgrid, d->qout.as<int32_t>());
+    IDL_LAUNCH();
+    IDL_CUDA(cudaMemcpyAsync(out, d->qout.ptr, (size_t)n * 4, cudaMemcpyDeviceToHost, C.stream));
+    IDL_CUDA(cudaStreamSynchronize(C.stream));
+    IDL_API_END
+}
+
+int idl_delaunay_in_circumsphere(idl_delaunay* d, const int32_t* pts, const double* t, int64_t n, uint8_t* mask,
+                                 int32_t* tids)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    if (n < 0) invalid("query count must not be negative");
+    if (n == 0) return IDL_OK;
+    if (!pts || !t || !mask || !tids) invalid("query and output buffers must not be NULL");
+    DeviceGuard g(d->C.device);
+    Context& C = d->C;
+    ensure_rank(*d);
+    ensure_raster(*d, nullptr);
+    const int32_t* q = upload_queries(*d, pts, n);
+    // one scratch block: t (8 B), tid (4 B), mask (1 B) per query
+    d->qout.ensure((size_t)n * 13);
+    double* dt = d->qout.as<double>();
+    int32_t* dtid = reinterpret_cast<int32_t*>(dt + n);
+    uint8_t* dm = reinterpret_cast<uint8_t*>(dtid + n);
+    IDL_CUDA(cudaMemcpyAsync(dt, t, (size_t)n * 8, cudaMemcpyHostToDevice, C.stream));
+    k_circumsphere<<<blocks(n), 256, 0, C.stream>>>(q, dt, n, d->P, d->Wd, d->Hd, d->tgrid, C.tris.as<int32_t>(),
+                                                    d->sx, d->sy, dm, dtid);
+    IDL_LAUNCH();
+    IDL_CUDA(cudaMemcpyAsync(tids, dtid, (size_t)n * 4, cudaMemcpyDeviceToHost, C.stream));
+    IDL_CUDA(cudaMemcpyAsync(mask, dm, (size_t)n, cudaMemcpyDeviceToHost, C.stream));
+    IDL_CUDA(cudaStreamSynchronize(C.stream));
+    IDL_API_END
+}
+
+int idl_delaunay_seeds(idl_delaunay* d, int32_t* xy_out, float* values_out, int64_t* n_values_out)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    if (xy_out)
+        for (int64_t i = 0; i < d->N; ++i) {
+            xy_out[2 * i] = d->hx[i];
+            xy_out[2 * i + 1] = d->hy[i];
+        }
+    if (values_out) std::copy(d->hvals.begin(), d->hvals.end(), values_out);
+    if (n_values_out) *n_values_out = (int64_t)d->hvals.size();
+    IDL_API_END
+}
+
+int idl_delaunay_sorted_rank(idl_delaunay* d, int32_t* out)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    if (d->N == 0) return IDL_OK;
+    if (!out) invalid("output must not be NULL");
+    DeviceGuard g(d->C.device);
+    ensure_rank(*d);
+    IDL_CUDA(cudaMemcpyAsync(out, d->rank, (size_t)d->N * 4, cudaMemcpyDeviceToHost, d->C.stream));
+    IDL_CUDA(cudaStreamSynchronize(d->C.stream));
+    IDL_API_END
+}
+
+int idl_delaunay_voronoi(idl_delaunay* d, int32_t* out)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    if (!out) invalid("output must not be NULL");
+    DeviceGuard g(d->C.device);
+    Context& C = d->C;
+    const size_t bytes = (size_t)d->W * d->H * 2 * 4;
+    C.outgrid.ensure(bytes);
+    if (d->N == 0) {
+        IDL_CUDA(cudaMemsetAsync(C.outgrid.ptr, 0xFF, bytes, C.stream));
+    } else {
+        ensure_rank(*d);
+        dim3 gr(blocks(d->W), d->H);
+        k_out2<<<gr, 256, 0, C.stream>>>(d->planes, d->pitch, d->P, d->W, d->H, d->pos, d->rank,
+                                        C.outgrid.as<int32_t>());
+        IDL_LAUNCH();
+    }
+    IDL_CUDA(cudaMemcpyAsync(out, C.outgrid.ptr, bytes, cudaMemcpyDeviceToHost, C.stream));
+    IDL_CUDA(cudaStreamSynchronize(C.stream));
+    IDL_API_END
+}
+
+int idl_delaunay_info(idl_delaunay* d, int64_t* info, int count)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    if (!info) invalid("output must not be NULL");
+    const int64_t v[IDL_DI_COUNT] = {d->N, d->W, d->H, d->P, d->pending ? 1 : 0, (int64_t)d->generation,
+                                     d->max_seeds, d->mode, d->have_values ? 1 : 0};
+    for (int i = 0; i < count && i < IDL_DI_COUNT; ++i) info[i] = v[i];
+    IDL_API_END
+}
+
+}  // extern "C"

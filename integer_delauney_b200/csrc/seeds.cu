@@ -193,8 +193,9 @@ __global__ void k_mark_xy(const int32_t* __restrict__ xs, const int32_t* __restr
 }
 
 __global__ void k_rank_xy(const int32_t* __restrict__ xs, const int32_t* __restrict__ ys, int64_t n, int H,
-                          const uint32_t* __restrict__ bitmap, const int32_t* __restrict__ word_rank,
-                          int32_t* __restrict__ rank, int32_t* __restrict__ xs_sorted, int32_t* __restrict__ ys_sorted)
+                          const uint32_t* __restrict__ bitmap, const int32_t* __restrict__ word_rank, int off,
+                          int32_t* __restrict__ rank, int32_t* __restrict__ inv, int32_t* __restrict__ xs_sorted,
+                          int32_t* __restrict__ ys_sorted)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -202,14 +203,15 @@ __global__ void k_rank_xy(const int32_t* __restrict__ xs, const int32_t* __restr
     const uint32_t below = bitmap[bit >> 5] & ((1u << (bit & 31)) - 1u);
     const int32_t r = word_rank[bit >> 5] + __popc(below);
     rank[i] = r;
-    xs_sorted[r] = xs[i];
-    ys_sorted[r] = ys[i];
+    inv[r] = (int32_t)i;
+    xs_sorted[r] = xs[i] + off;
+    ys_sorted[r] = ys[i] + off;
 }
 
 }  // namespace
 
-void rank_seeds_device(Context& C, int W, int H, const int32_t* xs, const int32_t* ys, int64_t n, int32_t* rank,
-                       int32_t* xs_sorted, int32_t* ys_sorted)
+void rank_seeds_device(Context& C, int W, int H, const int32_t* xs, const int32_t* ys, int64_t n, int off,
+                       int32_t* rank, int32_t* inv, int32_t* xs_sorted, int32_t* ys_sorted)
 {
     if (n <= 0) return;
     const int64_t nwords = ((int64_t)W * H + 31) / 32;
@@ -224,8 +226,8 @@ void rank_seeds_device(Context& C, int W, int H, const int32_t* xs, const int32_
                                                                   C.scan_b.as<int32_t>());
     IDL_LAUNCH();
     exclusive_scan(C, C.scan_b.as<int32_t>(), C.scan_c.as<int32_t>(), nwords);
-    k_rank_xy<<<gs, 256, 0, C.stream>>>(xs, ys, n, H, C.bitmap.as<uint32_t>(), C.scan_c.as<int32_t>(), rank,
-                                        xs_sorted, ys_sorted);
+    k_rank_xy<<<gs, 256, 0, C.stream>>>(xs, ys, n, H, C.bitmap.as<uint32_t>(), C.scan_c.as<int32_t>(), off, rank,
+                                        inv, xs_sorted, ys_sorted);
     IDL_LAUNCH();
 }
 

@@ -219,6 +219,65 @@ def triangulate(W: int, H: int, sorted_seeds, P: int = DEFAULT_BORDER_PADDING,
         cap = -nt
 
 
+def incremental(W: int, H: int, batches, P: int = DEFAULT_BORDER_PADDING):
+    """The reference's incremental Delaunay, restated on the CPU.
+
+    Seeds keep insertion-order ids; each batch is written into the padded
+    label grid and the Jacobi iteration continues from the previous fixed
+    point (src/cuda/delaunay.cu:184-268, src/cuda/delaunay_voronoi.cu:12-108).
+    Triangles are detected on the insertion-id grid (the block rule's
+    lowest-id tie-break sees insertion ids, triangle_detect.cuh:75-166) and
+    reported the batch way: vertex ids through sorted_rank
+    (src/cuda/delaunay_output.cu:39-84), triangle id = rank of the sorted
+    triple, pixel = highest id of the triangles containing it.
+
+    Returns dict(rank, tris (N_tri, 5) batch ids, tris_ins (N_tri, 3)
+    insertion ids, grid (H, W, 3), labels (padded, insertion ids), passes).
+    """
+    Wd, Hd = W + 2 * P, H + 2 * P
+    lab = np.full((Hd, Wd), -1, dtype=np.int32)
+    xs = np.zeros(0, dtype=np.int32)
+    ys = np.zeros(0, dtype=np.int32)
+    passes = []
+    for b in batches:
+        b = np.asarray(b, dtype=np.int32).reshape(-1, 2)
+        if len(b) == 0:
+            continue
+        n0 = len(xs)
+        xs = np.concatenate([xs, b[:, 0]])
+        ys = np.concatenate([ys, b[:, 1]])
+        lab[b[:, 1] + P, b[:, 0] + P] = np.arange(n0, n0 + len(b), dtype=np.int32)
+        lab, k = jacobi_from(Wd, Hd, xs + P, ys + P, lab)
+        passes.append(k)
+    n = len(xs)
+    order = np.lexsort((ys, xs))
+    rank = np.empty(n, dtype=np.int32)
+    rank[order] = np.arange(n, dtype=np.int32)
+    raw = detect(lab, xs + P, ys + P, P) if n >= 3 else np.zeros((0, 5), np.int32)
+    tris = raw.copy()
+    if len(raw):
+        tris[:, 2:5] = rank[raw[:, 2:5]]
+        key = np.sort(tris[:, 2:5], axis=1)
+        o = np.lexsort((key[:, 2], key[:, 1], key[:, 0]))
+        tris = tris[o]
+        raw = raw[o]
+    sx, sy = xs[order], ys[order]
+    tgrid = assign(W, H, sx, sy, tris) if n else np.full((H, W), -1, np.int32)
+    inner = lab[P:P + H, P:P + W]
+    grid = np.empty((H, W, 3), dtype=np.int32)
+    ok = inner >= 0
+    grid[:, :, 0] = np.where(ok, rank[np.maximum(inner, 0)], -1) if n else -1
+    yy, xx = np.mgrid[0:H, 0:W]
+    if n:
+        d = (xx - xs[np.maximum(inner, 0)]) ** 2 + (yy - ys[np.maximum(inner, 0)]) ** 2
+        grid[:, :, 1] = np.where(ok, d, -1)
+    else:
+        grid[:, :, 1] = -1
+    grid[:, :, 2] = tgrid
+    return {"rank": rank, "tris": tris, "tris_ins": np.ascontiguousarray(raw[:, 2:5]), "grid": grid,
+            "labels": lab, "passes": passes, "xs": xs, "ys": ys}
+
+
 # ---------------------------------------------------------------------------
 # The reference's own CUDA batch path (oracle/_ref/libref_cuda.so, built by
 # oracle/build_ref.sh).  Present only where it was built; needs a GPU to run.
