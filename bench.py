@@ -189,6 +189,55 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def incremental_case(cu, torch, rank):
+    """2048 x 2048, 50 000 uniform seeds, then 100 insert batches of 1 000
+    new seeds (30 % in a 256 x 256 hotspot).  Each batch is timed through the
+    public call a caller makes: insert() (propagate, topology, assignment and
+    the (H, W, 3) grid copied to host memory), wall clock per batch; then the
+    same batches through insert_deferred() and one finalise().  Triangles come
+    back as arrays (as_arrays=True): a 300 000-entry dict costs more host time
+    than the whole device update."""
+    from integer_delauney_b200.workloads import incremental
+    Wi = Hi = 2048
+    base, batches = incremental(Wi, Hi, 50_000, 100, 1_000, seed=rank)
+    cap = len(base) + sum(len(b) for b in batches)
+
+    def fresh():
+        d = cu.Delaunay(Wi, Hi, cap, PADDING)
+        d.insert_deferred(base)
+        d.finalise()
+        return d
+
+    d = fresh()
+    for b in batches[:3]:                 # warm-up on a throwaway object
+        d.insert(b, as_arrays=True)
+    d = fresh()
+    torch.cuda.synchronize()
+    lat = []
+    t_all = time.perf_counter()
+    for b in batches:
+        t0 = time.perf_counter()
+        m, g = d.insert(b, as_arrays=True)
+        lat.append(time.perf_counter() - t0)
+    t_all = time.perf_counter() - t_all
+    n_tri = len(m)
+    d2 = fresh()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for b in batches:
+        d2.insert_deferred(b)
+    d2.finalise(as_arrays=True)
+    t_def = time.perf_counter() - t0
+    lat_ms = sorted(x * 1e3 for x in lat)
+    return {"workload": f"Delaunay {Wi}x{Hi}, {len(base)} uniform seeds + {len(batches)} x {len(batches[0])} "
+                        f"(30% in a 256x256 hotspot), P={PADDING}, reference mode",
+            "insert_ms_mean": t_all * 1e3 / len(batches), "insert_ms_p50": lat_ms[len(lat_ms) // 2],
+            "insert_ms_p99": lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))],
+            "insert_mpix_s": Wi * Hi * len(batches) / t_all / 1e6,
+            "deferred_total_ms": t_def * 1e3, "triangles_final": n_tri,
+            "d2h_bytes_per_insert": Wi * Hi * 12}
+
+
 def run_ours(args, rank, world):
     import torch
 
@@ -292,6 +341,8 @@ def run_ours(args, rank, world):
     ms_e = reduce_max(e0.elapsed_time(e1), world)
     e2e = world * W * H * e_steps / (ms_e / 1e3) / 1e6
 
+    inc = incremental_case(cu, torch, rank)
+
     if rank != 0:
         return
     base = None
@@ -319,6 +370,7 @@ def run_ours(args, rank, world):
         "e2e": {"value": e2e, "unit": "Mpixel/s", "ms_per_step": ms_e / e_steps,
                 "h2d_bytes_per_step": int(seeds_u.nbytes),
                 "d2h_bytes_per_step": int(W * H * 12 + n_tri * 20)},
+        "incremental": inc,
         "gpu_launches": int(launches),
         "clocks": clocks,
         "cpu_baseline": base,

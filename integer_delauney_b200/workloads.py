@@ -7,6 +7,9 @@ benchmark configurations (no dataset is involved anywhere).
   batched_images(count, seed)     per-image (W, H, seeds) with sides
                                   log-uniform in 64..1024 and density
                                   uniform in 0.1%..2% of pixels
+  incremental(...)                a uniform base set and insert batches of
+                                  new distinct points, a fixed share of each
+                                  inside a hotspot square
 
 Points are returned in a shuffled (not sorted) order, as callers pass them.
 """
@@ -68,3 +71,39 @@ def batched_images(count: int = 512, seed: int = 0, side_lo: int = 64, side_hi: 
         n = max(3, int(math.ceil(dens * W * H)))
         out.append((W, H, uniform(W, H, n, seed=int(rng.integers(1 << 31)))))
     return out
+
+
+def incremental(W: int = 2048, H: int = 2048, base: int = 50_000, batches: int = 100, per_batch: int = 1_000,
+                hot_frac: float = 0.3, hot: int = 256, seed: int = 0):
+    """(base (base, 2), [batch (per_batch, 2), ...]) for the incremental
+    configuration: every point distinct from all earlier ones; in each batch
+    round(hot_frac * per_batch) points are uniform in a hot x hot square
+    placed by the seed, the rest uniform on the canvas."""
+    rng = np.random.default_rng(seed)
+    b0 = uniform(W, H, base, seed=seed)
+    taken = set((b0[:, 1].astype(np.int64) * W + b0[:, 0]).tolist())
+    hx = int(rng.integers(0, W - hot + 1))
+    hy = int(rng.integers(0, H - hot + 1))
+    out = []
+    n_hot = int(round(hot_frac * per_batch))
+    for _ in range(batches):
+        pts = []
+        for want, (x0, y0, w, h) in ((n_hot, (hx, hy, hot, hot)), (per_batch - n_hot, (0, 0, W, H))):
+            got = 0
+            while got < want:
+                k = (want - got) * 2 + 8
+                xs = rng.integers(x0, x0 + w, size=k)
+                ys = rng.integers(y0, y0 + h, size=k)
+                for x, y in zip(xs.tolist(), ys.tolist()):
+                    key = y * W + x
+                    if key in taken:
+                        continue
+                    taken.add(key)
+                    pts.append((x, y))
+                    got += 1
+                    if got == want:
+                        break
+        b = np.array(pts, dtype=np.int32)
+        rng.shuffle(b)
+        out.append(np.ascontiguousarray(b))
+    return b0, out

@@ -396,3 +396,18 @@ class TestQueries:
             assert not got.any()
         with pytest.raises(ValueError):
             mesh.in_circumsphere(q[:2], np.zeros(1))
+
+
+def test_incremental_config_prefix_bit_exact(cu):
+    """The incremental configuration at full size (2048 x 2048, 50 000 base
+    seeds, 1 000-seed batches with a hotspot), first three batches, checked
+    against the oracle after each batch."""
+    from integer_delauney_b200.workloads import incremental
+    base, batches = incremental(2048, 2048, 50_000, 3, 1_000, seed=0)
+    d = cu.Delaunay(2048, 2048, 60_000, 16)
+    d.insert_deferred(base)
+    done = [base]
+    for b in batches:
+        m, g = d.insert(b)
+        done.append(b)
+    assert_matches_oracle(d, m, g, oracle.incremental(2048, 2048, done, 16))
