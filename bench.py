@@ -238,6 +238,60 @@ def incremental_case(cu, torch, rank):
             "d2h_bytes_per_insert": Wi * Hi * 12}
 
 
+def batched_case(torch, lib, ctx, stream, rank):
+    """512 images, sides log-uniform in 64..1024, density 0.1..2 %: one
+    idl_triangulate_batch_device call against the plain per-image loop of
+    idl_triangulate_device (one call and one count read-back per image), both
+    on device-resident seeds and outputs, both timed with CUDA events."""
+    from integer_delauney_b200 import _capi
+    from integer_delauney_b200.workloads import batched_images
+    imgs = batched_images(512, seed=rank)
+    dims = np.array([(w, h) for w, h, _ in imgs], dtype=np.int32)
+    counts = np.array([len(sd) for _, _, sd in imgs], dtype=np.int64)
+    seeds = torch.from_numpy(np.concatenate([sd for _, _, sd in imgs])).cuda()
+    px = dims[:, 0].astype(np.int64) * dims[:, 1]
+    out = torch.empty(int(px.sum()) * 3, dtype=torch.int32, device="cuda")
+    tri_counts = np.zeros(len(imgs), dtype=np.int64)
+    s_off = np.concatenate([[0], np.cumsum(counts)])
+    p_off = np.concatenate([[0], np.cumsum(px)])
+    mode = _capi.mode_id(MODE)
+
+    def batch():
+        _capi.check(lib.idl_triangulate_batch_device(ctx.handle, len(imgs), dims.ctypes.data, counts.ctypes.data,
+                                                     seeds.data_ptr(), PADDING, mode, out.data_ptr(),
+                                                     tri_counts.ctypes.data))
+
+    n_tri = ctypes.c_int64(0)
+
+    def loop():
+        for i, (w, h, _) in enumerate(imgs):
+            _capi.check(lib.idl_triangulate_device(ctx.handle, w, h, seeds.data_ptr() + int(s_off[i]) * 8,
+                                                   int(counts[i]), PADDING, mode,
+                                                   out.data_ptr() + int(p_off[i]) * 12, ctypes.byref(n_tri)))
+
+    def timed(fn, reps):
+        fn()
+        fn()
+        torch.cuda.synchronize()
+        l0 = lib.idl_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, (lib.idl_launch_count() - l0) // reps
+
+    ms_b, launches_b = timed(batch, 5)
+    ms_l, launches_l = timed(loop, 2)
+    total = float(px.sum())
+    return {"workload": f"{len(imgs)} images, sides log-uniform 64..1024, density 0.1..2 %, "
+                        f"{int(counts.sum())} seeds, {int(total)} pixels, P={PADDING}, reference mode",
+            "batch_ms": ms_b, "batch_mpix_s": total / (ms_b / 1e3) / 1e6, "batch_launches": int(launches_b),
+            "loop_ms": ms_l, "loop_mpix_s": total / (ms_l / 1e3) / 1e6, "loop_launches": int(launches_l),
+            "speedup_vs_loop": ms_l / ms_b}
+
+
 def run_ours(args, rank, world):
     import torch
 
@@ -342,6 +396,7 @@ def run_ours(args, rank, world):
     e2e = world * W * H * e_steps / (ms_e / 1e3) / 1e6
 
     inc = incremental_case(cu, torch, rank)
+    bat = batched_case(torch, lib, ctx, stream, rank)
 
     if rank != 0:
         return
@@ -371,6 +426,7 @@ def run_ours(args, rank, world):
                 "h2d_bytes_per_step": int(seeds_u.nbytes),
                 "d2h_bytes_per_step": int(W * H * 12 + n_tri * 20)},
         "incremental": inc,
+        "batched": bat,
         "gpu_launches": int(launches),
         "clocks": clocks,
         "cpu_baseline": base,

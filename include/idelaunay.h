@@ -191,6 +191,36 @@ IDL_API int idl_triangles_device(idl_context* ctx, const int32_t** d_tris, const
 IDL_API int idl_voronoi_noalloc(int width, int height, const int32_t* d_seeds_xy, int64_t n_seeds, int mode,
                                 int32_t* d_grid_out, void* stream, int64_t* passes_out);
 
+/* ==== batched triangulation ==============================================
+ * No counterpart in the reference, which triangulates one image per call
+ * (src/cuda/bindings/triangulate.hpp:15-43).  n_images independent images of
+ * any sizes and seed counts run through the pipeline together: one
+ * propagation launch, one detection, one raster and one composition launch
+ * for the whole batch, and a fixed number of host synchronisations.  Each
+ * image's grid and triangles equal idl_triangulate on that image alone, bit
+ * for bit.  Limits: mode IDL_MODE_REFERENCE; at most 2097151 seeds in total;
+ * the padded canvases must shelf-pack into a 32767 x 32767 atlas (about
+ * 10^9 padded pixels), otherwise IDL_ERR_INVALID asks for a smaller batch.
+ *   dims         host n_images * 2 int32: (width, height) per image
+ *   seed_counts  host n_images int64: seeds per image (each >= 1)
+ *   seeds_xy     host (sum of seed_counts) * 2 int32, image after image
+ *   grids_out    host (NULL allowed): the images' (height, width, 3) int32
+ *                grids, concatenated in image order
+ *   tri_counts_out  host n_images int64 (NULL allowed)
+ * Validation errors name the image ("image k: ...").  The batch's triangles,
+ * image after image with image-local seed ids and triangle ids, are then
+ * available from idl_get_triangles (5 int32 each, as for one image). */
+IDL_API int idl_triangulate_batch(idl_context* ctx, int n_images, const int32_t* dims, const int64_t* seed_counts,
+                                  const int32_t* seeds_xy, int border_padding, int mode, int32_t* grids_out,
+                                  int64_t* tri_counts_out, float* timings_out);
+
+/* As idl_triangulate_batch with device seeds (d_seeds_xy) and device output
+ * (d_grids_out, concatenated grids); ordered on the context's stream, waits
+ * for it once for validation and once for the counts. */
+IDL_API int idl_triangulate_batch_device(idl_context* ctx, int n_images, const int32_t* dims,
+                                         const int64_t* seed_counts, const int32_t* d_seeds_xy, int border_padding,
+                                         int mode, int32_t* d_grids_out, int64_t* tri_counts_out);
+
 /* ==== incremental triangulation (stage (c)) ============================
  * An idl_delaunay holds one growing seed set on a padded canvas and keeps its
  * Voronoi diagram, triangles and pixel assignment on the device between

@@ -10,7 +10,7 @@ from __future__ import annotations
 
 import math
 
-_CUDA_EXPORTS = {"Voronoi", "GridTriangulation", "Delaunay", "triangulate"}
+_CUDA_EXPORTS = {"Voronoi", "GridTriangulation", "Delaunay", "triangulate", "triangulate_batch"}
 
 __all__ = list(_CUDA_EXPORTS) + ["DEFAULT_BORDER_PADDING", "max_boundary_spacing"]
 

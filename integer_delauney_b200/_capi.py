@@ -55,6 +55,9 @@ SIGNATURES = {
     "idl_triangulate_device": (_i32, [_vp, _i32, _i32, _vp, _i64, _i32, _i32, _vp, _pi64]),
     "idl_triangles_device": (_i32, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "idl_voronoi_noalloc": (_i32, [_i32, _i32, _vp, _i64, _i32, _vp, _vp, _pi64]),
+    # batched triangulation
+    "idl_triangulate_batch": (_i32, [_vp, _i32, _vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp]),
+    "idl_triangulate_batch_device": (_i32, [_vp, _i32, _vp, _vp, _vp, _i32, _i32, _vp, _vp]),
     # incremental triangulation
     "idl_delaunay_create": (_i32, [_i32, _i32, _i32, _i64, _i32, _i32, ctypes.POINTER(_vp)]),
     "idl_delaunay_destroy": (_i32, [_vp]),

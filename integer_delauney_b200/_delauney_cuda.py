@@ -159,6 +159,44 @@ def triangulate(width: int, height: int, seeds, border_padding: int = AUTO_BORDE
     return build_output(tris, grid, as_arrays)
 
 
+def triangulate_batch(images, border_padding: int = AUTO_BORDER_PADDING, as_arrays: bool = False, *,
+                      voronoi_mode="reference"):
+    """Triangulate many independent images in one pass of the pipeline.
+
+    ``images``: iterable of (width, height, seeds).  Returns a list with one
+    (triangle_map | verts, grid) per image, each equal to
+    ``triangulate(width, height, seeds, border_padding, as_arrays)``.  Not in
+    the reference API (which has one image per call); see
+    idl_triangulate_batch in include/idelaunay.h for the limits."""
+    imgs = [(int(w), int(h), parse_seeds(s)) for w, h, s in images]
+    n = len(imgs)
+    if n == 0:
+        return []
+    dims = np.array([(w, h) for w, h, _ in imgs], dtype=np.int32)
+    counts = np.array([len(s) for _, _, s in imgs], dtype=np.int64)
+    seeds = np.ascontiguousarray(np.concatenate([s for _, _, s in imgs]) if counts.sum() else
+                                 np.zeros((0, 2), np.int32), dtype=np.int32)
+    px = [w * h for w, h, _ in imgs]
+    grids = _host_buffer((max(sum(px), 0) * 3,))
+    tri_counts = np.zeros(n, dtype=np.int64)
+    lib = _capi.load()
+    ctx = _context()
+    with ctx.lock:
+        _bind(ctx)
+        check(lib.idl_triangulate_batch(ctx.handle, n, dims.ctypes.data, counts.ctypes.data,
+                                        seeds.ctypes.data if len(seeds) else None, int(border_padding),
+                                        mode_id(voronoi_mode), grids.ctypes.data, tri_counts.ctypes.data, None))
+        tris = _fetch_triangles(ctx, int(tri_counts.sum()))
+    out = []
+    p0 = t0 = 0
+    for (w, h, _), npx, nt in zip(imgs, px, tri_counts.tolist()):
+        g = grids[p0 * 3:(p0 + npx) * 3].reshape(h, w, 3)
+        out.append(build_output(tris[t0:t0 + nt], g, as_arrays))
+        p0 += npx
+        t0 += nt
+    return out
+
+
 class GridTriangulation:
     """Triangles from a Voronoi grid (src/cuda/bindings/py_grid_triangulation.hpp:10-110)."""
 

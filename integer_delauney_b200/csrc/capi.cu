@@ -23,7 +23,8 @@ size_t Context::workspace_bytes() const
 {
     const DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
                            &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &hkeys, &hvals, &ukeys, &uvals, &cnt,
-                           &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded, &scalars};
+                           &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded, &batch_img, &batch_seed_img,
+                           &batch_rows, &batch_sid, &batch_stats, &batch_bad, &scalars};
     size_t s = 0;
     for (const DevBuf* b : all) s += b->bytes;
     return s;
@@ -39,7 +40,8 @@ Context::~Context()
 {
     DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
                      &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &hkeys, &hvals, &ukeys, &uvals, &cnt,
-                     &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded, &scalars};
+                     &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded, &batch_img, &batch_seed_img,
+                           &batch_rows, &batch_sid, &batch_stats, &batch_bad, &scalars};
     for (DevBuf* b : all) b->release();
     if (host_sc && !host_sc_borrowed) cudaFreeHost(host_sc);
     for (auto& e : timing.ev)
@@ -269,7 +271,6 @@ void check_dims(int W, int H, int64_t n)
 
 using namespace idl;
 
-struct idl_context : public idl::Context {};
 
 extern "C" {
 

@@ -119,6 +119,14 @@ struct Context {
     DevBuf outgrid;       // H x W x 3 staging for host-pointer calls
     DevBuf padded;        // padded Voronoi grid for compute_debug
 
+    // batched triangulation (batch.cu)
+    DevBuf batch_img;       // per-image table
+    DevBuf batch_seed_img;  // image of each input seed
+    DevBuf batch_rows;      // image of each output row
+    DevBuf batch_sid;       // image of each sorted seed
+    DevBuf batch_stats;     // per-image triangle counts, longest sides, triangle offsets
+    DevBuf batch_bad;       // first out-of-bounds / duplicate seed index
+
     DevBuf scalars;       // one Scalars
     Scalars* host_sc = nullptr;  // pinned mirror
     bool host_sc_borrowed = false;  // host_sc points at static storage, not cudaMallocHost memory
@@ -215,3 +223,6 @@ void assign_pixels(Context& C, int W, int H, const int32_t* xs, const int32_t* y
 void ensure_scalars(Context& C);
 
 }  // namespace idl
+
+// The C ABI's opaque context handle is a Context.
+struct idl_context : public idl::Context {};

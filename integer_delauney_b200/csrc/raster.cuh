@@ -1,0 +1,91 @@
+// Device helpers of stage (d), shared by the single-image raster
+// (raster.cu) and the batched one (batch.cu).  The rules they implement are
+// documented at the top of raster.cu.
+#pragma once
+
+#include "context.cuh"
+
+namespace idl {
+
+__device__ __forceinline__ long long floor_div(long long p, long long q)   // q > 0
+{
+    return p >= 0 ? p / q : -((-p + q - 1) / q);
+}
+__device__ __forceinline__ long long ceil_div_ll(long long p, long long q) { return -floor_div(-p, q); }
+
+// Longest side of one triangle as triangulation.cu:357-362 computes it: float
+// dx, dy, dx*dx + dy*dy rounded per operation, sqrtf, truncation.
+__device__ __forceinline__ int tri_max_side(const int32_t* v, const int32_t* __restrict__ xs,
+                                            const int32_t* __restrict__ ys)
+{
+    const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2};
+    int best = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float dx = (float)(xs[v[pa[k]]] - xs[v[pb[k]]]);
+        const float dy = (float)(ys[v[pa[k]]] - ys[v[pb[k]]]);
+        const float s = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+        best = max(best, (int)__fsqrt_rn(s));
+    }
+    return best;
+}
+
+// Rasterise one triangle (vertex ids v, coordinates xs/ys) into a W x H grid
+// of triangle ids with atomicMax; the calling warp's 32 lanes share the rows.
+// wc: the degenerate-case seed window (max(20, max_side + 3)).
+__device__ __forceinline__ void raster_one(const int32_t* v, int32_t tid, const int32_t* __restrict__ xs,
+                                           const int32_t* __restrict__ ys, int W, int H, int wc,
+                                           int32_t* __restrict__ tgrid, int lane)
+{
+    const long long ax = xs[v[0]], ay = ys[v[0]], bx = xs[v[1]], by = ys[v[1]], cx = xs[v[2]], cy = ys[v[2]];
+    const long long area2 = (bx - ax) * (cy - ay) - (by - ay) * (cx - ax);
+    if (area2 == 0) {
+        // collinear: supporting line within the reference's seed window
+        if (lane != 0) return;
+        const long long lo_y = max(0ll, min(ay, min(by, cy)) - wc);
+        const long long hi_y = min((long long)H - 1, max(ay, max(by, cy)) + wc);
+        for (long long y = lo_y; y <= hi_y; ++y) {
+            long long x_lo, x_hi;
+            if (by == ay) {
+                if (y != ay) continue;
+                x_lo = 0; x_hi = W - 1;
+            } else {
+                const long long num = (bx - ax) * (y - ay);
+                const long long den = by - ay;
+                if (num % den != 0) continue;
+                x_lo = x_hi = ax + num / den;
+            }
+            for (long long x = max(0ll, x_lo); x <= min((long long)W - 1, x_hi); ++x) {
+                const bool near = (llabs(ax - x) <= wc && llabs(ay - y) <= wc) ||
+                                  (llabs(bx - x) <= wc && llabs(by - y) <= wc) ||
+                                  (llabs(cx - x) <= wc && llabs(cy - y) <= wc);
+                if (near) atomicMax(&tgrid[(size_t)y * W + x], tid);
+            }
+        }
+        return;
+    }
+    const long long sgn = area2 > 0 ? 1 : -1;
+    // d_i(x, y) = A_i * x + B_i * y + C_i for edges (a,b), (b,c), (c,a):
+    // cross(u - p, w - p) = (uy - wy) * px + (wx - ux) * py + (ux*wy - uy*wx)
+    const long long A[3] = {sgn * (ay - by), sgn * (by - cy), sgn * (cy - ay)};
+    const long long B[3] = {sgn * (bx - ax), sgn * (cx - bx), sgn * (ax - cx)};
+    const long long C0[3] = {sgn * (ax * by - ay * bx), sgn * (bx * cy - by * cx), sgn * (cx * ay - cy * ax)};
+    const long long y0 = max(0ll, min(ay, min(by, cy)));
+    const long long y1 = min((long long)H - 1, max(ay, max(by, cy)));
+    for (long long y = y0 + lane; y <= y1; y += 32) {
+        long long xl = 0, xr = W - 1;
+        bool empty = false;
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            const long long c = B[e] * y + C0[e];   // need A*x + c >= 0
+            if (A[e] > 0) xl = max(xl, ceil_div_ll(-c, A[e]));
+            else if (A[e] < 0) xr = min(xr, floor_div(c, -A[e]));
+            else if (c < 0) empty = true;
+        }
+        if (empty) continue;
+        int32_t* row = tgrid + (size_t)y * W;
+        for (long long x = xl; x <= xr; ++x) atomicMax(&row[x], tid);
+    }
+}
+
+}  // namespace idl

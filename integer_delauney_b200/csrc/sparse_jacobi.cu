@@ -107,9 +107,14 @@ __device__ __forceinline__ void best_of4(int32_t& b, int32_t n0, int32_t n1, int
     b = bl;
 }
 
+// Per-block staging of next-pass list entries.  Groups reserve slots with
+// atomicAdd on *n; a group whose slots would run past STAGE goes to the global
+// list instead and lowers *cut to its first slot, so that only the prefix
+// s_list[0, min(*n, *cut)) -- which every earlier group filled -- is flushed.
 struct Stage {
     int32_t* list;
     int* n;
+    int* cut;
 };
 
 // Advance `cnt` (<= GROUP, warp-uniform) micro-tiles by one Jacobi pass and
@@ -169,10 +174,11 @@ __device__ __forceinline__ void advance(const int (&ids)[GROUP], int cnt, const 
         if ((lane & 3) != 0) lf[k] = sl;
         if ((lane & 3) != 3) rt[k] = sr;
 
+        // cells below UNDEF are walls between packed images: never updated
         int32_t b0 = a0[k], b1 = a1[k];
-        if (in0[k] && (lf[k] != b0 || a1[k] != b0 || u0[k] != b0 || d0[k] != b0))
+        if (in0[k] && b0 >= UNDEF && (lf[k] != b0 || a1[k] != b0 || u0[k] != b0 || d0[k] != b0))
             best_of4(b0, lf[k], a1[k], u0[k], d0[k], gx[k], gy[k], pos);
-        if (in1[k] && (a0[k] != b1 || rt[k] != b1 || u1[k] != b1 || d1[k] != b1))
+        if (in1[k] && b1 >= UNDEF && (a0[k] != b1 || rt[k] != b1 || u1[k] != b1 || d1[k] != b1))
             best_of4(b1, a0[k], rt[k], u1[k], d1[k], gx[k] + 1, gy[k], pos);
         const size_t o = (size_t)gy[k] * pitch + gx[k];
         if (in1[k]) *reinterpret_cast<int2*>(nxt + o) = make_int2(b0, b1);
@@ -206,7 +212,10 @@ __device__ __forceinline__ void advance(const int (&ids)[GROUP], int cnt, const 
                     if (fresh) st.list[base + rank] = target;
                 } else {
                     int gbase = 0;
-                    if (lane == 0) gbase = atomicAdd(count_out, m);
+                    if (lane == 0) {
+                        atomicMin(st.cut, base);
+                        gbase = atomicAdd(count_out, m);
+                    }
                     gbase = __shfl_sync(FULL, gbase, 0);
                     if (fresh) lout[gbase + rank] = target;
                 }
@@ -223,7 +232,7 @@ k_sparse_jacobi(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, con
                 int mt_x, int mt_y, GridSync* gs)
 {
     __shared__ int32_t s_list[STAGE];
-    __shared__ int s_n, s_base, s_m;
+    __shared__ int s_n, s_cut, s_base, s_m;
     const int lane = threadIdx.x & 31;
     const int gwarp = blockIdx.x * SJ_WARPS + (threadIdx.x >> 5);
     const int nwarps = gridDim.x * SJ_WARPS;
@@ -232,7 +241,10 @@ k_sparse_jacobi(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, con
     for (; t < max_steps; ++t) {
         const int n = *reinterpret_cast<volatile int32_t*>(&counts[t]);
         if (n == 0) break;
-        if (threadIdx.x == 0) s_n = 0;
+        if (threadIdx.x == 0) {
+            s_n = 0;
+            s_cut = STAGE;
+        }
         __syncthreads();
         const int32_t* cur = (t & 1) ? plane1 : plane0;
         int32_t* nxt = (t & 1) ? plane0 : plane1;
@@ -246,11 +258,11 @@ k_sparse_jacobi(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, con
 #pragma unroll
             for (int k = 0; k < GROUP; ++k) ids[k] = k < cnt ? __ldcg(&lin[i0 + k]) : 0;
             advance(ids, cnt, cur, nxt, pitch, Wd, Hd, mt_x, mt_y, pos, bin, bout, lout, counts + t + 1,
-                    Stage{s_list, &s_n}, lane);
+                    Stage{s_list, &s_n, &s_cut}, lane);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            const int m = min(s_n, STAGE);
+            const int m = min(s_n, s_cut);
             s_m = m;
             s_base = m ? atomicAdd(&counts[t + 1], m) : 0;
         }

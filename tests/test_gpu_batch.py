@@ -207,3 +207,29 @@ def test_triangulate_vs_reference_cuda(W, H, n, seed, P):
     assert len(tris) == len(r_tris)
     np.testing.assert_array_equal(np.sort(tris[:, 2:5], axis=1), np.sort(r_tris[:, 2:5], axis=1))
     np.testing.assert_array_equal(grid, r_grid)
+
+
+def test_voronoi_large_canvas_matches_oracle():
+    """A canvas large enough that the propagation kernel's per-block staging
+    of next-pass work overflows into the global list in the early passes."""
+    W, H = 8192, 4096
+    seeds = random_seeds(W, H, 400_000, 12)
+    s = oracle.sort_seeds(seeds, W, H)
+    want, _ = oracle.voronoi("reference", W, H, s)
+    got = cu.Voronoi().compute(W, H, seeds)
+    np.testing.assert_array_equal(got, want)
+
+
+@ref
+@pytest.mark.parametrize("kind", ["uniform"])
+def test_triangulate_4096_200k_vs_reference_cuda(kind):
+    """The headline workload (4096 x 4096, 200 000 seeds, P = 16): grid bit
+    for bit and the same triangle set as the reference's own CUDA path."""
+    W = H = 4096
+    seeds = random_seeds(W, H, 200_000, 0) if kind == "uniform" else clustered_seeds(W, H, 200_000, 0)
+    s = oracle.sort_seeds(seeds, W, H)
+    r_tris, r_grid, _ = oracle.ref_triangulate(W, H, s, 16)
+    tm, grid = cu.triangulate(W, H, seeds, 16, as_arrays=True)
+    assert len(tm) == len(r_tris)
+    np.testing.assert_array_equal(np.sort(tm, axis=1), np.sort(r_tris[:, 2:5], axis=1))
+    np.testing.assert_array_equal(grid, r_grid)
