@@ -292,6 +292,151 @@ def batched_case(torch, lib, ctx, stream, rank):
             "speedup_vs_loop": ms_l / ms_b}
 
 
+def serving_case(torch, rank, seconds, slots=8):
+    """Serving: (1) a Poisson stream (1 000 req/s for `seconds`, 70 % new
+    triangulations of side log-uniform 128..4096 and density 0.05..1 %, 30 %
+    inserts of 100..5 000 seeds into a uniformly chosen resident diagram,
+    40 GB admission budget) replayed in real time against the server:
+    latency p50/p99 from arrival to result; (2) throughput with every request
+    of a fixed 2 000-request prefix submitted at once, server against the
+    plain serial loop over the same requests."""
+    from integer_delauney_b200.serving import Server, run_serial
+    from integer_delauney_b200.workloads import fresh_points, serving_trace, uniform
+    budget = 40 << 30
+    trace = serving_trace(1000.0, seconds, seed=rank)
+
+    def keys_of(W, pts):
+        return np.sort(pts[:, 1].astype(np.int64) * W + pts[:, 0])
+
+    # (1) real time; the new requests' seed sets are generated before the
+    # clock starts, the inserts' (which depend on the target) on the fly
+    pre = {i: uniform(prm[0], prm[1], prm[2], seed=prm[3]) for i, (t, kind, prm) in enumerate(trace)
+           if kind == "new"}
+    srv = Server(budget_bytes=budget, slots=slots, border_padding=PADDING)
+    info = {}          # diagram id -> (W, H, sorted keys)
+    futs = []
+    failed_submit = 0
+    late = 0.0
+    t0 = time.perf_counter() + 0.05
+    for i, (t, kind, prm) in enumerate(trace):
+        at = t0 + t
+        now = time.perf_counter()
+        if at > now:
+            time.sleep(at - now)
+        else:
+            late = max(late, now - at)
+        if kind == "new":
+            W, H, n, ps = prm
+            pts = pre.pop(i)
+            f = srv.submit_new(W, H, pts, arrival=at)
+            info[f.diagram_id] = (W, H, keys_of(W, pts))
+            futs.append(f)
+        else:
+            n, pick, ps = prm
+            res = [d for d in srv.resident() if d in info]
+            if not res:
+                failed_submit += 1
+                continue
+            did = res[int(pick * len(res))]
+            W, H, k = info[did]
+            pts = fresh_points(W, H, n, k, ps)
+            try:
+                futs.append(srv.submit_insert(did, pts, arrival=at))
+            except KeyError:
+                failed_submit += 1
+                continue
+            info[did] = (W, H, np.sort(np.concatenate([k, keys_of(W, pts)])))
+        if len(info) > 4096:
+            live = set(srv.resident())
+            for d in [d for d in info if d not in live]:
+                del info[d]
+    srv.drain()
+    t_end = time.perf_counter()
+    lat, n_new, n_ins, errors = [], 0, 0, 0
+    for f in futs:
+        e = f.exception()
+        if e is not None:
+            errors += 1
+            continue
+        r = f.result()
+        lat.append(r.latency * 1e3)
+        n_new += r.kind == "new"
+        n_ins += r.kind == "insert"
+    stats = dict(srv.stats)
+    peak = srv.memory_used()
+    srv.close()
+    lat.sort()
+
+    def pct(q):
+        return lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None
+
+    realtime = {"requests": len(trace), "completed": len(lat), "new": n_new, "inserts": n_ins,
+                "errors": errors, "not_submitted": failed_submit, "wall_s": t_end - t0,
+                "throughput_req_s": len(lat) / (t_end - t0), "p50_ms": pct(0.5), "p99_ms": pct(0.99),
+                "submit_lag_max_s": late,
+                "max_ms": lat[-1] if lat else None, "memory_bytes_end": peak, "objects": stats}
+
+    # (2) saturated: the same fixed requests through the server and the plain loop
+    reqs, meta = [], []
+    for t, kind, prm in trace[:2000]:
+        if kind == "new":
+            W, H, n, ps = prm
+            pts = uniform(W, H, n, seed=ps)
+            meta.append((W, H, keys_of(W, pts)))
+            reqs.append(("new", W, H, pts))
+        else:
+            n, pick, ps = prm
+            news = [i for i, r in enumerate(reqs) if r[0] == "new"][-100:]
+            if not news:
+                continue
+            j = news[int(pick * len(news))]
+            W, H, k = meta[j]
+            pts = fresh_points(W, H, n, k, ps)
+            meta[j] = (W, H, np.sort(np.concatenate([k, keys_of(W, pts)])))
+            meta.append(None)              # meta stays index-aligned with reqs
+            reqs.append(("insert", j, pts))
+    def saturate(n_slots):
+        torch.cuda.synchronize()
+        srv = Server(budget_bytes=budget, slots=n_slots, border_padding=PADDING)
+        t1 = time.perf_counter()
+        fut_of = {}
+        sfuts = []
+        for i, r in enumerate(reqs):
+            if r[0] == "new":
+                f = srv.submit_new(r[1], r[2], r[3])
+                fut_of[i] = f
+            else:
+                try:
+                    f = srv.submit_insert(fut_of[r[1]].diagram_id, r[2])
+                except KeyError:
+                    continue
+            sfuts.append(f)
+        srv.drain()
+        dt = time.perf_counter() - t1
+        ok = sum(1 for f in sfuts if f.exception() is None)
+        srv.close()
+        return dt, ok
+
+    t_srv, srv_ok = saturate(slots)
+    t_one, one_ok = saturate(1)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    out = run_serial(reqs, PADDING, budget)
+    torch.cuda.synchronize()
+    t_ser = time.perf_counter() - t1
+    ser_ok = sum(1 for o in out if o[1] >= 0)
+    saturated = {"requests": len(reqs), "slots": slots,
+                 "server_s": t_srv, "server_req_s": srv_ok / t_srv, "server_ok": srv_ok,
+                 "server_1slot_req_s": one_ok / t_one,
+                 "serial_s": t_ser, "serial_req_s": ser_ok / t_ser, "serial_ok": ser_ok,
+                 "speedup_vs_serial": (srv_ok / t_srv) / (ser_ok / t_ser),
+                 "speedup_vs_1slot": (srv_ok / t_srv) / (one_ok / t_one)}
+    return {"workload": f"Poisson 1000 req/s for {seconds:g} s: 70% new (side log-U 128..4096, density "
+                        f"0.05..1%), 30% inserts of 100..5000 seeds into resident diagrams; 40 GB budget; "
+                        f"P={PADDING}, reference mode; results stay on the device",
+            "realtime": realtime, "saturated": saturated}
+
+
 def run_ours(args, rank, world):
     import torch
 
@@ -397,6 +542,7 @@ def run_ours(args, rank, world):
 
     inc = incremental_case(cu, torch, rank)
     bat = batched_case(torch, lib, ctx, stream, rank)
+    srv = serving_case(torch, rank, args.serve_seconds) if args.serve_seconds > 0 else None
 
     if rank != 0:
         return
@@ -427,6 +573,7 @@ def run_ours(args, rank, world):
                 "d2h_bytes_per_step": int(W * H * 12 + n_tri * 20)},
         "incremental": inc,
         "batched": bat,
+        "serving": srv,
         "gpu_launches": int(launches),
         "clocks": clocks,
         "cpu_baseline": base,
@@ -442,6 +589,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--ref-rows", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=10.0,
+                    help="length of the real-time serving trace (0 skips the serving measurement)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 

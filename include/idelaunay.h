@@ -258,7 +258,8 @@ typedef struct idl_delaunay idl_delaunay;
 #define IDL_DI_MAX_SEEDS 6
 #define IDL_DI_MODE 7
 #define IDL_DI_HAS_VALUES 8
-#define IDL_DI_COUNT 9
+#define IDL_DI_DEVICE_BYTES 9 /* device memory the object holds, workspace included */
+#define IDL_DI_COUNT 10
 
 /* Delaunay::Delaunay (src/cuda/delaunay.cu:24-112).  Allocates every canvas-
  * sized buffer up front; border_padding < 0 selects IDL_DEFAULT_BORDER_PADDING.
@@ -268,8 +269,22 @@ typedef struct idl_delaunay idl_delaunay;
 IDL_API int idl_delaunay_create(int device, int width, int height, int64_t max_seeds, int border_padding, int mode,
                                 idl_delaunay** out);
 IDL_API int idl_delaunay_destroy(idl_delaunay* d);
+/* Empty the object and lay its existing allocations out for another canvas
+ * (no allocation, no free).  No counterpart in the reference, whose objects
+ * are sized once at construction: this lets a server recycle resident
+ * diagrams.  IDL_ERR_INVALID if the canvas, padding or seed capacity needs
+ * more memory than the object was created with. */
+IDL_API int idl_delaunay_reset(idl_delaunay* d, int width, int height, int64_t max_seeds, int border_padding);
 /* Order the object's work on `stream` (a cudaStream_t; NULL = legacy default). */
 IDL_API int idl_delaunay_set_stream(idl_delaunay* d, void* stream);
+
+/* Take scratch memory (hash table, work lists, triangle rows, ...) from the
+ * context `ws` instead of the object's own, or go back to its own with NULL.
+ * No counterpart in the reference.  Many resident objects can then share the
+ * scratch of a few contexts -- one per stream a server runs -- so an object
+ * holds only its persistent state.  Objects sharing a context must not run
+ * at the same time.  ws must be on the object's device. */
+IDL_API int idl_delaunay_set_workspace(idl_delaunay* d, idl_context* ws);
 
 /* Delaunay::insert_deferred (src/cuda/delaunay.cu:276-323 with apply_batch_,
  * :184-268): validate and append k seeds (host int32 x, y pairs), write them

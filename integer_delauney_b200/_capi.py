@@ -61,6 +61,8 @@ SIGNATURES = {
     # incremental triangulation
     "idl_delaunay_create": (_i32, [_i32, _i32, _i32, _i64, _i32, _i32, ctypes.POINTER(_vp)]),
     "idl_delaunay_destroy": (_i32, [_vp]),
+    "idl_delaunay_reset": (_i32, [_vp, _i32, _i32, _i64, _i32]),
+    "idl_delaunay_set_workspace": (_i32, [_vp, _vp]),
     "idl_delaunay_set_stream": (_i32, [_vp, _vp]),
     "idl_delaunay_insert": (_i32, [_vp, _vp, _i64, _vp, _vp]),
     "idl_delaunay_finalise": (_i32, [_vp, _vp, _pi64, _vp]),
@@ -80,7 +82,7 @@ SIGNATURES = {
 
 # idl_delaunay_info slots
 (DI_SEED_COUNT, DI_WIDTH, DI_HEIGHT, DI_BORDER_PADDING, DI_HAS_PENDING, DI_GENERATION, DI_MAX_SEEDS, DI_MODE,
- DI_HAS_VALUES, DI_COUNT) = range(10)
+ DI_HAS_VALUES, DI_DEVICE_BYTES, DI_COUNT) = range(11)
 
 _lib = None
 _lib_lock = threading.Lock()

@@ -490,6 +490,24 @@ class Delaunay:
         self._call("idl_delaunay_voronoi", out.ctypes.data)
         return out
 
+    # -- additions (no counterpart in the reference) ------------------------
+    def reset(self, width: int, height: int, max_seeds: int, border_padding: int = AUTO_BORDER_PADDING) -> None:
+        """Empty the object and reuse its device memory for another canvas
+        (ValueError if it does not fit).  Outstanding device views go stale."""
+        self._call("idl_delaunay_reset", int(width), int(height), int(max_seeds), int(border_padding))
+
+    def use_workspace(self, context) -> None:
+        """Take scratch memory from ``context`` (an ``_capi.Context`` on the
+        same device) instead of the object's own; None goes back to its own.
+        Objects sharing a context must not run at the same time."""
+        self._workspace = context            # keeps the context alive while in use
+        self._call("idl_delaunay_set_workspace", context.handle if context is not None else None)
+
+    @property
+    def device_bytes(self) -> int:
+        """Device memory held by the object, workspace included."""
+        return int(self._info()[_capi.DI_DEVICE_BYTES])
+
     @property
     def seed_count(self) -> int:
         return int(self._info()[_capi.DI_SEED_COUNT])

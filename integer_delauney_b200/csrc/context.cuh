@@ -131,6 +131,7 @@ struct Context {
     Scalars* host_sc = nullptr;  // pinned mirror
     bool host_sc_borrowed = false;  // host_sc points at static storage, not cudaMallocHost memory
 
+    const void* owner = nullptr; // object whose intermediates the buffers hold (shared workspaces)
     int64_t last_n_tri = 0;      // triangles of the last triangulation (host copy)
     bool have_result = false;
 

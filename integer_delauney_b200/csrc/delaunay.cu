@@ -30,13 +30,17 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <unordered_set>
 #include <vector>
 
 namespace idl {
 
 struct DelaunayState {
-    Context C;
+    Context own;                  // scratch of this object unless a shared workspace is set
+    Context* ws = nullptr;        // shared workspace context (idl_delaunay_set_workspace)
+    cudaStream_t stream = nullptr;
+    int device = 0;
     int W = 0, H = 0, P = 0, Wd = 0, Hd = 0, pitch = 0;
     int64_t max_seeds = 0;
     int mode = IDL_MODE_REFERENCE;
@@ -47,7 +51,10 @@ struct DelaunayState {
     bool have_values = false;
     int64_t n_tri = 0, n_edges = 0;
 
-    // device memory owned by this object (allocated in create)
+    // device memory owned by this object (allocated in create; reset re-lays
+    // the same allocations out for another canvas that fits)
+    size_t planes_bytes = 0, tgrid_bytes = 0, pix_bytes = 0;
+    int64_t seed_cap = 0;
     int32_t* planes = nullptr;
     int32_t* tgrid = nullptr;
     int32_t* seedmem = nullptr;
@@ -68,19 +75,45 @@ struct DelaunayState {
 
     Canvas canvas() const { return Canvas{Wd, Hd, pitch}; }
 
+    // The context whose scratch (and stream) this object's work uses, bound to
+    // this object: its label planes point at ours, and if another object used
+    // it last, the triangle rows it holds are not ours, so topology is redone
+    // when next needed (the raster, ranks and seeds live in our own memory).
+    Context& ctx()
+    {
+        Context& c = ws ? *ws : own;
+        if (!ws && !own.scalars.ptr) ensure_scalars(own);
+        c.stream = stream;
+        const size_t plane = (size_t)pitch * Hd;
+        c.lab[0].borrow(planes, plane * 4);
+        c.lab[1].borrow(planes + plane, plane * 4);
+        if (c.owner != this) {
+            c.owner = this;
+            topo_dirty = true;
+        }
+        return c;
+    }
+
+    // Device memory of the object comes from the stream-ordered allocator:
+    // freeing it never waits for the whole device, which matters when many
+    // objects on many streams come and go (a server recycling diagrams).
     void free_owned() noexcept
     {
-        if (planes) cudaFree(planes);
-        if (tgrid) cudaFree(tgrid);
-        if (seedmem) cudaFree(seedmem);
-        if (pixmem) cudaFree(pixmem);
+        if (planes) cudaFreeAsync(planes, stream);
+        if (tgrid) cudaFreeAsync(tgrid, stream);
+        if (seedmem) cudaFreeAsync(seedmem, stream);
+        if (pixmem) cudaFreeAsync(pixmem, stream);
         planes = tgrid = seedmem = nullptr;
         pixmem = nullptr;
         DevBuf* all[] = {&stage, &edge_keys, &edge_tmp, &sort_tmp, &num_sel, &scores, &score_keys, &score_sorted,
                          &qbuf, &qout};
         for (DevBuf* b : all) b->release();
     }
-    ~DelaunayState() { free_owned(); }
+    ~DelaunayState()
+    {
+        if (ws && ws->owner == this) ws->owner = nullptr;
+        free_owned();
+    }
 };
 
 }  // namespace idl
@@ -338,7 +371,7 @@ struct Timer {
 void ensure_rank(DelaunayState& D)
 {
     if (!D.rank_dirty) return;
-    rank_seeds_device(D.C, D.W, D.H, D.ix, D.iy, D.N, D.P, D.rank, D.inv, D.sx, D.sy);
+    rank_seeds_device(D.ctx(), D.W, D.H, D.ix, D.iy, D.N, D.P, D.rank, D.inv, D.sx, D.sy);
     D.rank_dirty = false;
 }
 
@@ -346,7 +379,7 @@ void ensure_topology(DelaunayState& D, float* timings)
 {
     if (!D.topo_dirty) return;
     ensure_rank(D);
-    Context& C = D.C;
+    Context& C = D.ctx();
     if (D.N < 3) {
         D.n_tri = 0;
     } else {
@@ -381,10 +414,11 @@ void ensure_topology(DelaunayState& D, float* timings)
 // (the batch rule of triangulation.cu:101-137 over the whole triangle set).
 void ensure_raster(DelaunayState& D, float* timings)
 {
-    ensure_topology(D, timings);
     if (!D.raster_dirty) return;
-    Timer T(D.C, timings != nullptr);
-    assign_pixels(D.C, D.Wd, D.Hd, D.sx, D.sy, D.tgrid, D.n_tri);
+    ensure_topology(D, timings);
+    Context& C = D.ctx();
+    Timer T(C, timings != nullptr);
+    assign_pixels(C, D.Wd, D.Hd, D.sx, D.sy, D.tgrid, D.n_tri);
     const float ms = T.stop();
     if (timings) timings[IDL_T_ASSIGN_MS] += ms;
     D.raster_dirty = false;
@@ -394,7 +428,7 @@ void ensure_edges(DelaunayState& D)
 {
     ensure_topology(D, nullptr);
     if (!D.edges_dirty) return;
-    Context& C = D.C;
+    Context& C = D.ctx();
     D.n_edges = 0;
     if (D.n_tri > 0) {
         const int64_t m = D.n_tri * 3;
@@ -428,7 +462,7 @@ void ensure_edges(DelaunayState& D)
 void compute_scores(DelaunayState& D, double min_length)
 {
     D.scores.ensure((size_t)std::max<int64_t>(1, D.n_edges) * 4);
-    k_edge_scores<<<blocks(D.n_edges), 256, 0, D.C.stream>>>(D.edge_keys.as<unsigned long long>(), D.n_edges, D.N,
+    k_edge_scores<<<blocks(D.n_edges), 256, 0, D.ctx().stream>>>(D.edge_keys.as<unsigned long long>(), D.n_edges, D.N,
                                                              D.ix, D.iy, D.values, min_length * min_length,
                                                              D.scores.as<float>());
     IDL_LAUNCH();
@@ -437,8 +471,66 @@ void compute_scores(DelaunayState& D, double min_length)
 const int32_t* upload_queries(DelaunayState& D, const int32_t* pts, int64_t n)
 {
     D.qbuf.ensure((size_t)n * 2 * 4);
-    IDL_CUDA(cudaMemcpyAsync(D.qbuf.ptr, pts, (size_t)n * 2 * 4, cudaMemcpyHostToDevice, D.C.stream));
+    IDL_CUDA(cudaMemcpyAsync(D.qbuf.ptr, pts, (size_t)n * 2 * 4, cudaMemcpyHostToDevice, D.ctx().stream));
     return D.qbuf.as<int32_t>();
+}
+
+// Objects allocate from the device's default stream-ordered pool; keep what
+// they free in the pool (no release threshold) so the next object reuses it
+// without a trip to the driver.  This changes only this process's pool.
+void keep_pool_memory(int dev)
+{
+    static std::once_flag once[64];
+    std::call_once(once[dev & 63], [dev] {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            uint64_t keep = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    });
+}
+
+// Lay the object's allocations out for a width x height canvas with padding P
+// and room for max_seeds seeds, and reset it to the empty state.  The caller
+// has checked that everything fits.
+void layout(DelaunayState& d, int width, int height, int64_t max_seeds, int P)
+{
+    d.W = width;
+    d.H = height;
+    d.P = P;
+    d.Wd = width + 2 * P;
+    d.Hd = height + 2 * P;
+    d.pitch = (d.Wd + 31) / 32 * 32;
+    d.max_seeds = max_seeds;
+    int32_t* s = d.seedmem;
+    const int64_t cap = d.seed_cap;
+    d.ix = s;
+    d.iy = s + cap;
+    d.pos = reinterpret_cast<uint32_t*>(s + 2 * cap);
+    d.rank = s + 3 * cap;
+    d.inv = s + 4 * cap;
+    d.sx = s + 5 * cap;
+    d.sy = s + 6 * cap;
+    d.values = reinterpret_cast<float*>(s + 7 * cap);
+    d.pix_tid = static_cast<int32_t*>(d.pixmem);
+    d.pix_sid = d.pix_tid + (size_t)width * height;
+    d.pix_out = reinterpret_cast<uint8_t*>(d.pix_sid + (size_t)width * height);
+    const size_t plane = (size_t)d.pitch * d.Hd;
+    d.N = 0;
+    d.pending = false;
+    d.rank_dirty = d.topo_dirty = d.raster_dirty = false;
+    d.edges_dirty = true;
+    d.have_values = false;
+    d.n_tri = d.n_edges = 0;
+    d.hx.clear();
+    d.hy.clear();
+    d.hvals.clear();
+    d.seen.clear();
+    IDL_CUDA(cudaMemsetAsync(d.planes, 0xFF, plane * 2 * sizeof(int32_t), d.stream));
+    IDL_CUDA(cudaMemsetAsync(d.tgrid, 0xFF, (size_t)d.Wd * d.Hd * sizeof(int32_t), d.stream));
+    IDL_CUDA(cudaMemsetAsync(d.values, 0, (size_t)max_seeds * sizeof(float), d.stream));
+    IDL_CUDA(cudaStreamSynchronize(d.stream));
 }
 
 void check_handle(const idl_delaunay* d)
@@ -468,45 +560,28 @@ int idl_delaunay_create(int device, int width, int height, int64_t max_seeds, in
     DeviceGuard g(dev);
     auto* d = new idl_delaunay();
     try {
-        d->C.device = dev;
-        IDL_CUDA(cudaDeviceGetAttribute(&d->C.num_sms, cudaDevAttrMultiProcessorCount, dev));
-        ensure_scalars(d->C);
-        d->W = width;
-        d->H = height;
-        d->P = border_padding >= 0 ? border_padding : IDL_DEFAULT_BORDER_PADDING;
-        d->max_seeds = max_seeds;
-        d->mode = mode;
-        const int64_t Wd = (int64_t)width + 2 * d->P, Hd = (int64_t)height + 2 * d->P;
+        d->device = dev;
+        d->own.device = dev;
+        IDL_CUDA(cudaDeviceGetAttribute(&d->own.num_sms, cudaDevAttrMultiProcessorCount, dev));
+        keep_pool_memory(dev);
+        const int P = border_padding >= 0 ? border_padding : IDL_DEFAULT_BORDER_PADDING;
+        const int64_t Wd = (int64_t)width + 2 * P, Hd = (int64_t)height + 2 * P;
         const int64_t pitch = (Wd + 31) / 32 * 32;
         // The canvas-sized buffers first: a canvas no GPU can hold fails here,
         // as a CUDA allocation error, before any size rule of this build.
-        IDL_CUDA(cudaMalloc(&d->planes, (size_t)pitch * Hd * 2 * sizeof(int32_t)));
-        IDL_CUDA(cudaMalloc(&d->tgrid, (size_t)Wd * Hd * sizeof(int32_t)));
-        IDL_CUDA(cudaMalloc(&d->pixmem, (size_t)width * height * 9));
-        IDL_CUDA(cudaMalloc(&d->seedmem, (size_t)max_seeds * 8 * sizeof(int32_t)));
+        d->planes_bytes = (size_t)pitch * Hd * 2 * sizeof(int32_t);
+        d->tgrid_bytes = (size_t)Wd * Hd * sizeof(int32_t);
+        d->pix_bytes = (size_t)width * height * 9;
+        d->seed_cap = max_seeds;
+        IDL_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d->planes), d->planes_bytes, d->stream));
+        IDL_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d->tgrid), d->tgrid_bytes, d->stream));
+        IDL_CUDA(cudaMallocAsync(&d->pixmem, d->pix_bytes, d->stream));
+        IDL_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d->seedmem), (size_t)max_seeds * 8 * sizeof(int32_t),
+                                 d->stream));
         if (Wd > MAX_CANVAS_SIDE || Hd > MAX_CANVAS_SIDE)
             invalid("padded canvas side exceeds the 32767 pixels this build addresses");
-        d->Wd = (int)Wd;
-        d->Hd = (int)Hd;
-        d->pitch = (int)pitch;
-        int32_t* s = d->seedmem;
-        d->ix = s;
-        d->iy = s + max_seeds;
-        d->pos = reinterpret_cast<uint32_t*>(s + 2 * max_seeds);
-        d->rank = s + 3 * max_seeds;
-        d->inv = s + 4 * max_seeds;
-        d->sx = s + 5 * max_seeds;
-        d->sy = s + 6 * max_seeds;
-        d->values = reinterpret_cast<float*>(s + 7 * max_seeds);
-        d->pix_tid = static_cast<int32_t*>(d->pixmem);
-        d->pix_sid = d->pix_tid + (size_t)width * height;
-        d->pix_out = reinterpret_cast<uint8_t*>(d->pix_sid + (size_t)width * height);
-        const size_t plane = (size_t)pitch * Hd;
-        d->C.lab[0].borrow(d->planes, plane * 4);
-        d->C.lab[1].borrow(d->planes + plane, plane * 4);
-        IDL_CUDA(cudaMemset(d->planes, 0xFF, plane * 2 * sizeof(int32_t)));
-        IDL_CUDA(cudaMemset(d->tgrid, 0xFF, (size_t)Wd * Hd * sizeof(int32_t)));
-        IDL_CUDA(cudaMemset(d->values, 0, (size_t)max_seeds * sizeof(float)));
+        d->mode = mode;
+        layout(*d, width, height, max_seeds, P);
         IDL_CUDA(cudaDeviceSynchronize());
     } catch (...) {
         delete d;
@@ -516,12 +591,29 @@ int idl_delaunay_create(int device, int width, int height, int64_t max_seeds, in
     IDL_API_END
 }
 
+int idl_delaunay_reset(idl_delaunay* d, int width, int height, int64_t max_seeds, int border_padding)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    if (width <= 0 || height <= 0 || max_seeds <= 0) invalid("dimensions and max_seeds must be positive");
+    const int P = border_padding >= 0 ? border_padding : IDL_DEFAULT_BORDER_PADDING;
+    const int64_t Wd = (int64_t)width + 2 * P, Hd = (int64_t)height + 2 * P;
+    const int64_t pitch = (Wd + 31) / 32 * 32;
+    if ((size_t)pitch * Hd * 8 > d->planes_bytes || (size_t)Wd * Hd * 4 > d->tgrid_bytes ||
+        (size_t)width * height * 9 > d->pix_bytes || max_seeds > d->seed_cap)
+        invalid("reset: the new canvas or seed capacity does not fit this object's allocations");
+    DeviceGuard g(d->device);
+    ++d->generation;
+    layout(*d, width, height, max_seeds, P);
+    IDL_API_END
+}
+
 int idl_delaunay_destroy(idl_delaunay* d)
 {
     IDL_API_BEGIN
     if (!d) return IDL_OK;
-    DeviceGuard g(d->C.device);
-    cudaStreamSynchronize(d->C.stream);
+    DeviceGuard g(d->device);
+    cudaStreamSynchronize(d->stream);
     delete d;
     IDL_API_END
 }
@@ -530,7 +622,16 @@ int idl_delaunay_set_stream(idl_delaunay* d, void* stream)
 {
     IDL_API_BEGIN
     check_handle(d);
-    d->C.stream = static_cast<cudaStream_t>(stream);
+    d->stream = static_cast<cudaStream_t>(stream);
+    IDL_API_END
+}
+
+int idl_delaunay_set_workspace(idl_delaunay* d, idl_context* ws)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    if (ws && ws->device != d->device) invalid("the workspace context belongs to another device");
+    d->ws = ws;
     IDL_API_END
 }
 
@@ -558,8 +659,8 @@ int idl_delaunay_insert(idl_delaunay* d, const int32_t* xy, int64_t k, const flo
             if (d->seen.count(key)) invalid("seed position already exists");
         }
     }
-    DeviceGuard g(d->C.device);
-    Context& C = d->C;
+    DeviceGuard g(d->device);
+    Context& C = d->ctx();
     ++d->generation;
     const int64_t n0 = d->N;
     std::vector<int32_t> host((size_t)k * 3);
@@ -604,8 +705,8 @@ int idl_delaunay_finalise(idl_delaunay* d, int32_t* grid_out, int64_t* n_tri_out
     check_handle(d);
     if (timings)
         for (int i = 0; i < IDL_T_COUNT; ++i) timings[i] = 0.f;
-    DeviceGuard g(d->C.device);
-    Context& C = d->C;
+    DeviceGuard g(d->device);
+    Context& C = d->ctx();
     ensure_rank(*d);
     ensure_raster(*d, timings);
     if (d->pending) {
@@ -635,8 +736,8 @@ int idl_delaunay_finalise_device(idl_delaunay* d, int64_t* n_tri_out, const int3
 {
     IDL_API_BEGIN
     check_handle(d);
-    DeviceGuard g(d->C.device);
-    Context& C = d->C;
+    DeviceGuard g(d->device);
+    Context& C = d->ctx();
     ++d->generation;
     ensure_rank(*d);
     ensure_raster(*d, nullptr);
@@ -658,8 +759,8 @@ int idl_delaunay_triangles(idl_delaunay* d, int ids, int32_t* out, int64_t capac
     IDL_API_BEGIN
     check_handle(d);
     if (ids != 0 && ids != 1) invalid("ids must be 0 (batch) or 1 (insertion order)");
-    DeviceGuard g(d->C.device);
-    Context& C = d->C;
+    DeviceGuard g(d->device);
+    Context& C = d->ctx();
     ensure_topology(*d, nullptr);
     if (n_out) *n_out = d->n_tri;
     if (!out || d->n_tri == 0) return IDL_OK;
@@ -682,8 +783,8 @@ int idl_delaunay_edges(idl_delaunay* d, int32_t* out, int64_t capacity, int64_t*
 {
     IDL_API_BEGIN
     check_handle(d);
-    DeviceGuard g(d->C.device);
-    Context& C = d->C;
+    DeviceGuard g(d->device);
+    Context& C = d->ctx();
     ensure_edges(*d);
     if (n_out) *n_out = d->n_edges;
     if (!out || d->n_edges == 0) return IDL_OK;
@@ -701,7 +802,7 @@ int idl_delaunay_edge_scores(idl_delaunay* d, double min_length, float* out, int
 {
     IDL_API_BEGIN
     check_handle(d);
-    DeviceGuard g(d->C.device);
+    DeviceGuard g(d->device);
     ensure_edges(*d);
     if (n_out) *n_out = d->n_edges;
     if (d->n_edges == 0) return IDL_OK;
@@ -710,8 +811,8 @@ int idl_delaunay_edge_scores(idl_delaunay* d, double min_length, float* out, int
     if (!out) return IDL_OK;
     if (capacity < d->n_edges) invalid("score buffer too small");
     compute_scores(*d, min_length);
-    IDL_CUDA(cudaMemcpyAsync(out, d->scores.ptr, (size_t)d->n_edges * 4, cudaMemcpyDeviceToHost, d->C.stream));
-    IDL_CUDA(cudaStreamSynchronize(d->C.stream));
+    IDL_CUDA(cudaMemcpyAsync(out, d->scores.ptr, (size_t)d->n_edges * 4, cudaMemcpyDeviceToHost, d->stream));
+    IDL_CUDA(cudaStreamSynchronize(d->stream));
     IDL_API_END
 }
 
@@ -721,8 +822,8 @@ int idl_delaunay_select_midpoints(idl_delaunay* d, double min_length, int count,
     IDL_API_BEGIN
     check_handle(d);
     if (n_out) *n_out = 0;
-    DeviceGuard g(d->C.device);
-    Context& C = d->C;
+    DeviceGuard g(d->device);
+    Context& C = d->ctx();
     ensure_edges(*d);
     if (d->n_edges == 0 || count <= 0) return IDL_OK;
     if (!d->have_values)
@@ -794,8 +895,8 @@ int idl_delaunay_locate(idl_delaunay* d, const int32_t* pts, int64_t n, int32_t*
     if (n < 0) invalid("query count must not be negative");
     if (n == 0) return IDL_OK;
     if (!pts || !out) invalid("query and output buffers must not be NULL");
-    DeviceGuard g(d->C.device);
-    Context& C = d->C;
+    DeviceGuard g(d->device);
+    Context& C = d->ctx();
     ensure_rank(*d);
     ensure_raster(*d, nullptr);
     const int32_t* q = upload_queries(*d, pts, n);
@@ -815,10 +916,11 @@ int idl_delaunay_in_circumsphere(idl_delaunay* d, const int32_t* pts, const doub
     if (n < 0) invalid("query count must not be negative");
     if (n == 0) return IDL_OK;
     if (!pts || !t || !mask || !tids) invalid("query and output buffers must not be NULL");
-    DeviceGuard g(d->C.device);
-    Context& C = d->C;
+    DeviceGuard g(d->device);
+    Context& C = d->ctx();
     ensure_rank(*d);
     ensure_raster(*d, nullptr);
+    ensure_topology(*d, nullptr);
     const int32_t* q = upload_queries(*d, pts, n);
     // one scratch block: t (8 B), tid (4 B), mask (1 B) per query
     d->qout.ensure((size_t)n * 13);
@@ -855,10 +957,10 @@ int idl_delaunay_sorted_rank(idl_delaunay* d, int32_t* out)
     check_handle(d);
     if (d->N == 0) return IDL_OK;
     if (!out) invalid("output must not be NULL");
-    DeviceGuard g(d->C.device);
+    DeviceGuard g(d->device);
     ensure_rank(*d);
-    IDL_CUDA(cudaMemcpyAsync(out, d->rank, (size_t)d->N * 4, cudaMemcpyDeviceToHost, d->C.stream));
-    IDL_CUDA(cudaStreamSynchronize(d->C.stream));
+    IDL_CUDA(cudaMemcpyAsync(out, d->rank, (size_t)d->N * 4, cudaMemcpyDeviceToHost, d->stream));
+    IDL_CUDA(cudaStreamSynchronize(d->stream));
     IDL_API_END
 }
 
@@ -867,8 +969,8 @@ int idl_delaunay_voronoi(idl_delaunay* d, int32_t* out)
     IDL_API_BEGIN
     check_handle(d);
     if (!out) invalid("output must not be NULL");
-    DeviceGuard g(d->C.device);
-    Context& C = d->C;
+    DeviceGuard g(d->device);
+    Context& C = d->ctx();
     const size_t bytes = (size_t)d->W * d->H * 2 * 4;
     C.outgrid.ensure(bytes);
     if (d->N == 0) {
@@ -890,8 +992,14 @@ int idl_delaunay_info(idl_delaunay* d, int64_t* info, int count)
     IDL_API_BEGIN
     check_handle(d);
     if (!info) invalid("output must not be NULL");
+    const int64_t device_bytes = (int64_t)(d->planes_bytes + d->tgrid_bytes + d->pix_bytes +
+                                           (size_t)d->seed_cap * 32 + d->own.workspace_bytes()) +
+                                 (int64_t)(d->stage.bytes + d->edge_keys.bytes + d->edge_tmp.bytes +
+                                           d->sort_tmp.bytes + d->num_sel.bytes + d->scores.bytes +
+                                           d->score_keys.bytes + d->score_sorted.bytes + d->qbuf.bytes +
+                                           d->qout.bytes);
     const int64_t v[IDL_DI_COUNT] = {d->N, d->W, d->H, d->P, d->pending ? 1 : 0, (int64_t)d->generation,
-                                     d->max_seeds, d->mode, d->have_values ? 1 : 0};
+                                     d->max_seeds, d->mode, d->have_values ? 1 : 0, device_bytes};
     for (int i = 0; i < count && i < IDL_DI_COUNT; ++i) info[i] = v[i];
     IDL_API_END
 }

@@ -30,6 +30,7 @@
 #include "stencil.cuh"
 
 #include <cuda/atomic>
+#include <mutex>
 #include <vector>
 
 namespace idl {
@@ -353,12 +354,20 @@ int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos, cons
     GridSync* gs = C.gsync.as<GridSync>();
     int pitch = cv.pitch, Wd = cv.Wd, Hd = cv.Hd, ms = max_steps, mx = mt_x, my = mt_y;
     void* args[] = {&p0, &p1, &pitch, &Wd, &Hd, (void*)&pos, &b0, &b1, &l0, &l1, &counts, &ms, &mx, &my, &gs};
-    IDL_CUDA(cudaLaunchCooperativeKernel((const void*)k_sparse_jacobi, dim3(grid), dim3(SJ_THREADS), args, 0,
-                                         C.stream));
-    count_launch();
     GridSync h{};
-    IDL_CUDA(cudaMemcpyAsync(&h, gs, sizeof(GridSync), cudaMemcpyDeviceToHost, C.stream));
-    IDL_CUDA(cudaStreamSynchronize(C.stream));
+    {
+        // One persistent grid per device at a time: the kernel fills every SM,
+        // so two contexts' launches on different streams could not run side by
+        // side anyway, and holding the device lock from launch to completion
+        // keeps each grid's co-residency independent of the other streams.
+        static std::mutex device_locks[64];
+        std::lock_guard<std::mutex> lock(device_locks[C.device & 63]);
+        IDL_CUDA(cudaLaunchCooperativeKernel((const void*)k_sparse_jacobi, dim3(grid), dim3(SJ_THREADS), args, 0,
+                                             C.stream));
+        count_launch();
+        IDL_CUDA(cudaMemcpyAsync(&h, gs, sizeof(GridSync), cudaMemcpyDeviceToHost, C.stream));
+        IDL_CUDA(cudaStreamSynchronize(C.stream));
+    }
     if (h.error) throw Error(IDL_ERR_INTERNAL, "Voronoi propagation: grid barrier timed out");
     const int64_t passes = h.passes;
     if (passes >= max_steps) throw Error(IDL_ERR_INTERNAL, "Voronoi propagation did not converge");

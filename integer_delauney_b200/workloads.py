@@ -10,6 +10,9 @@ benchmark configurations (no dataset is involved anywhere).
   incremental(...)                a uniform base set and insert batches of
                                   new distinct points, a fixed share of each
                                   inside a hotspot square
+  serving_trace(...)              Poisson arrivals of new triangulations and
+                                  insert batches, and fresh_points() for the
+                                  inserts' seeds
 
 Points are returned in a shuffled (not sorted) order, as callers pass them.
 """
@@ -107,3 +110,47 @@ def incremental(W: int = 2048, H: int = 2048, base: int = 50_000, batches: int =
         rng.shuffle(b)
         out.append(np.ascontiguousarray(b))
     return b0, out
+
+
+def serving_trace(rate: float = 1000.0, seconds: float = 60.0, frac_new: float = 0.7, side=(128, 4096),
+                  density=(0.0005, 0.01), insert=(100, 5000), seed: int = 0):
+    """Poisson request stream for the serving configuration: a list of
+    (arrival_s, kind, params) with kind "new" -> (width, height, n_seeds,
+    point_seed) and kind "insert" -> (n_seeds, pick, point_seed), pick in
+    [0, 1) choosing the target among the diagrams resident at that time.
+    Sides are log-uniform in `side`, density uniform in `density`, insert
+    sizes uniform integers in `insert`."""
+    rng = np.random.default_rng(seed)
+    out = []
+    t = 0.0
+    lo, hi = math.log(side[0]), math.log(side[1])
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= seconds:
+            break
+        if rng.random() < frac_new:
+            W = int(round(math.exp(rng.uniform(lo, hi))))
+            H = int(round(math.exp(rng.uniform(lo, hi))))
+            n = max(3, int(math.ceil(rng.uniform(*density) * W * H)))
+            out.append((t, "new", (W, H, n, int(rng.integers(1 << 31)))))
+        else:
+            out.append((t, "insert", (int(rng.integers(insert[0], insert[1] + 1)), float(rng.random()),
+                                      int(rng.integers(1 << 31)))))
+    return out
+
+
+def fresh_points(W: int, H: int, n: int, taken_keys: np.ndarray, seed: int) -> np.ndarray:
+    """n distinct uniform points of a W x H canvas whose keys y * W + x are
+    not in the sorted int64 array `taken_keys` (fewer if the canvas is full)."""
+    rng = np.random.default_rng(seed)
+    free = W * H - len(taken_keys)
+    n = min(n, max(free, 0))
+    got = np.zeros(0, dtype=np.int64)
+    while len(got) < n:
+        k = rng.integers(0, W * H, size=(n - len(got)) * 2 + 16, dtype=np.int64)
+        k = k[~np.isin(k, taken_keys, assume_unique=False)]
+        got = np.concatenate([got, k])
+        _, first = np.unique(got, return_index=True)
+        got = got[np.sort(first)]
+    got = got[:n]
+    return np.ascontiguousarray(np.stack([got % W, got // W], axis=1).astype(np.int32))

@@ -1,0 +1,105 @@
+"""Serving: every request's result is the same when it runs alone as when it
+runs in the mix on the server (many slots, overlapping streams, admission by
+memory budget, recycled objects), bit for bit."""
+import numpy as np
+import pytest
+
+from integer_delauney_b200.workloads import fresh_points, uniform
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def cu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from integer_delauney_b200 import _delauney_cuda
+    return _delauney_cuda
+
+
+def _requests(seed=0, n_new=14):
+    rng = np.random.default_rng(seed)
+    news, inserts = [], []
+    for i in range(n_new):
+        W, H = int(rng.integers(40, 700)), int(rng.integers(40, 700))
+        n = int(max(3, rng.uniform(0.001, 0.02) * W * H))
+        pts = uniform(W, H, n, seed=1000 + i)
+        news.append((W, H, pts))
+        keys = np.sort(pts[:, 1].astype(np.int64) * W + pts[:, 0])
+        for j in range(int(rng.integers(0, 3))):
+            add = fresh_points(W, H, int(rng.integers(10, 400)), keys, seed=5000 + 10 * i + j)
+            keys = np.sort(np.concatenate([keys, add[:, 1].astype(np.int64) * W + add[:, 0]]))
+            inserts.append((i, add))
+    return news, inserts
+
+
+def _alone(cu, news, inserts, P=16):
+    """Each diagram on its own, one request at a time."""
+    out_new, out_ins = [], []
+    objs = []
+    for W, H, pts in news:
+        d = cu.Delaunay(W, H, len(pts) + 2000, P)
+        order = np.lexsort((pts[:, 1], pts[:, 0]))
+        d.insert_deferred(np.ascontiguousarray(pts[order]))
+        out_new.append(d.finalise(as_arrays=True))
+        objs.append(d)
+    for i, add in inserts:
+        objs[i].insert_deferred(add)
+        out_ins.append(objs[i].finalise(as_arrays=True))
+    return out_new, out_ins
+
+
+def _mixed(news, inserts, budget=40 << 30, slots=4):
+    from integer_delauney_b200.serving import Server
+    with Server(budget_bytes=budget, slots=slots, border_padding=16) as srv:
+        fn = [srv.submit_new(W, H, pts, fetch=True) for W, H, pts in news]
+        fi = [srv.submit_insert(fn[i].diagram_id, add, fetch=True) for i, add in inserts]
+        srv.drain()
+        stats = dict(srv.stats)
+        return [f.result() for f in fn], [f.result() for f in fi], stats
+
+
+def _same(a, b):
+    np.testing.assert_array_equal(a[0], b.verts)
+    np.testing.assert_array_equal(np.asarray(a[1]), b.grid)
+
+
+def test_alone_equals_mixed(cu):
+    news, inserts = _requests(0)
+    a_new, a_ins = _alone(cu, news, inserts)
+    m_new, m_ins, _ = _mixed(news, inserts)
+    for a, m in zip(a_new, m_new):
+        _same(a, m)
+    for a, m in zip(a_ins, m_ins):
+        _same(a, m)
+
+
+def test_new_requests_equal_the_batch_pipeline(cu):
+    news, _ = _requests(1, n_new=6)
+    m_new, _, _ = _mixed(news, [])
+    for (W, H, pts), r in zip(news, m_new):
+        v, g = cu.triangulate(W, H, pts, 16, as_arrays=True)
+        np.testing.assert_array_equal(v, r.verts)
+        np.testing.assert_array_equal(g, r.grid)
+
+
+def test_small_budget_recycles_objects_and_keeps_results(cu):
+    from integer_delauney_b200.serving import SEED_HEADROOM, estimate_bytes, slot_reserve
+    news = [(200, 180, uniform(200, 180, 300, seed=i)) for i in range(12)]
+    budget = 3 * estimate_bytes(256, 256, 300 + SEED_HEADROOM, 16, workspace=False) + 2 * slot_reserve(16)
+    a_new, _ = _alone(cu, news, [])
+    m_new, _, stats = _mixed(news, [], budget=budget, slots=2)
+    for a, m in zip(a_new, m_new):
+        _same(a, m)
+    assert stats.get("evicted", 0) > 0 and stats.get("reused_objects", 0) > 0
+
+
+def test_over_budget_and_unknown_diagram(cu):
+    from integer_delauney_b200.serving import Server
+    with Server(budget_bytes=1 << 20, slots=1) as srv:
+        f = srv.submit_new(512, 512, uniform(512, 512, 100, seed=1))
+        with pytest.raises(MemoryError):
+            f.result(timeout=60)
+        with pytest.raises(KeyError):
+            srv.submit_insert(12345, [(1, 1)])
