@@ -221,6 +221,14 @@ IDL_API int idl_triangulate_batch_device(idl_context* ctx, int n_images, const i
                                          const int64_t* seed_counts, const int32_t* d_seeds_xy, int border_padding,
                                          int mode, int32_t* d_grids_out, int64_t* tri_counts_out);
 
+/* Stage (a) only for a batch, as idl_triangulate_batch lays it out: the
+ * converged labels of every image stay in the context for idl_delaunay_adopt
+ * (until the context's next triangulation or batch call).  No counterpart in
+ * the reference; a server uses it to propagate many new diagrams in one
+ * launch.  Arguments as idl_triangulate_batch. */
+IDL_API int idl_voronoi_batch(idl_context* ctx, int n_images, const int32_t* dims, const int64_t* seed_counts,
+                              const int32_t* seeds_xy, int border_padding, int mode);
+
 /* ==== incremental triangulation (stage (c)) ============================
  * An idl_delaunay holds one growing seed set on a padded canvas and keeps its
  * Voronoi diagram, triangles and pixel assignment on the device between
@@ -296,6 +304,21 @@ IDL_API int idl_delaunay_set_workspace(idl_delaunay* d, idl_context* ws);
  * IDL_ERR_INVALID with the reference's messages. */
 IDL_API int idl_delaunay_insert(idl_delaunay* d, const int32_t* seeds_xy, int64_t k, const float* values,
                                 float* timings_out);
+
+/* As idl_delaunay_insert; with order = 1 the batch's seeds (and values) take
+ * their ids in (x asc, y asc) order instead of the order given, which into an
+ * empty object reproduces the batch pipeline's numbering (and so its result,
+ * bit for bit) without a host-side sort.  No counterpart in the reference. */
+IDL_API int idl_delaunay_insert_ordered(idl_delaunay* d, const int32_t* seeds_xy, int64_t k, const float* values,
+                                        int order, float* timings_out);
+
+/* Make an empty object (fresh or reset, same width, height and padding) hold
+ * image `image` of the last idl_voronoi_batch on `src`: its converged labels
+ * and its seeds, numbered in (x, y) order -- the state idl_delaunay_insert_
+ * ordered(order = 1) of the same seeds would reach, bit for bit, without a
+ * propagation of its own.  No counterpart in the reference.  Waits for the
+ * copy; src may then run its next batch. */
+IDL_API int idl_delaunay_adopt(idl_delaunay* d, idl_context* src, int image);
 
 /* Delaunay::finalise (src/cuda/delaunay.cu:325-347): assign pixels for the
  * pending changes and write the (height, width, 3) int32 grid (batch seed id,

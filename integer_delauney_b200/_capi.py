@@ -58,13 +58,16 @@ SIGNATURES = {
     # batched triangulation
     "idl_triangulate_batch": (_i32, [_vp, _i32, _vp, _vp, _vp, _i32, _i32, _vp, _vp, _vp]),
     "idl_triangulate_batch_device": (_i32, [_vp, _i32, _vp, _vp, _vp, _i32, _i32, _vp, _vp]),
+    "idl_voronoi_batch": (_i32, [_vp, _i32, _vp, _vp, _vp, _i32, _i32]),
     # incremental triangulation
     "idl_delaunay_create": (_i32, [_i32, _i32, _i32, _i64, _i32, _i32, ctypes.POINTER(_vp)]),
     "idl_delaunay_destroy": (_i32, [_vp]),
     "idl_delaunay_reset": (_i32, [_vp, _i32, _i32, _i64, _i32]),
     "idl_delaunay_set_workspace": (_i32, [_vp, _vp]),
+    "idl_delaunay_adopt": (_i32, [_vp, _vp, _i32]),
     "idl_delaunay_set_stream": (_i32, [_vp, _vp]),
     "idl_delaunay_insert": (_i32, [_vp, _vp, _i64, _vp, _vp]),
+    "idl_delaunay_insert_ordered": (_i32, [_vp, _vp, _i64, _vp, _i32, _vp]),
     "idl_delaunay_finalise": (_i32, [_vp, _vp, _pi64, _vp]),
     "idl_delaunay_finalise_device": (_i32, [_vp, _pi64, ctypes.POINTER(_vp), ctypes.POINTER(_vp),
                                             ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_uint64)]),

@@ -350,7 +350,9 @@ class Delaunay:
             self._call("idl_delaunay_triangles", ids, out.ctypes.data, out.size, ctypes.byref(n))
         return out
 
-    def _insert(self, seeds, values, timings: bool):
+    def _insert(self, seeds, values, timings: bool, order: str = "given"):
+        if order not in ("given", "xy"):
+            raise ValueError("order must be 'given' or 'xy'")
         s = parse_seeds(seeds)
         v = None
         if values is not None:
@@ -358,8 +360,8 @@ class Delaunay:
             if len(v) != len(s):
                 raise ValueError("values must have one entry per seed in the batch")
         t = (ctypes.c_float * _capi.T_COUNT)() if timings else None
-        self._call("idl_delaunay_insert", s.ctypes.data if len(s) else None, len(s),
-                   v.ctypes.data if (v is not None and len(v)) else None,
+        self._call("idl_delaunay_insert_ordered", s.ctypes.data if len(s) else None, len(s),
+                   v.ctypes.data if (v is not None and len(v)) else None, 1 if order == "xy" else 0,
                    ctypes.cast(t, ctypes.c_void_p) if t is not None else None)
         return t
 
@@ -389,9 +391,13 @@ class Delaunay:
         d["dedup_ms"] += float(t1[_capi.T_DEDUP_MS])
         return m, g, d
 
-    def insert_deferred(self, seeds, values=None) -> None:
-        """Append a batch (and optionally its scalar values) without assigning pixels."""
-        self._insert(seeds, values, False)
+    def insert_deferred(self, seeds, values=None, *, order: str = "given") -> None:
+        """Append a batch (and optionally its scalar values) without assigning pixels.
+
+        ``order="xy"`` (an addition) numbers this batch's seeds in (x, y)
+        order instead of the order given; into an empty object that yields
+        the batch pipeline's result exactly."""
+        self._insert(seeds, values, False, order)
 
     def insert_deferred_timed(self, seeds) -> dict:
         return _timings_dict(self._insert(seeds, None, True))
@@ -417,6 +423,17 @@ class Delaunay:
         return (verts, DeviceArrayView(self, p_t.value or 0, count, "<i4", gen.value),
                 DeviceArrayView(self, p_s.value or 0, count, "<i4", gen.value),
                 DeviceArrayView(self, p_m.value or 0, count, "|u1", gen.value))
+
+    def _adopt(self, context, image: int) -> None:
+        """Take image `image` of the last idl_voronoi_batch on `context` as
+        this (empty) object's state (see idl_delaunay_adopt)."""
+        self._call("idl_delaunay_adopt", context.handle, int(image))
+
+    def _finalise_device_count(self) -> int:
+        """finalise_device() without the triangle copy: the count only."""
+        n = ctypes.c_int64(0)
+        self._call("idl_delaunay_finalise_device", ctypes.byref(n), None, None, None, None)
+        return int(n.value)
 
     def get_triangles(self) -> np.ndarray:
         """(N_tri, 3) vertex ids in INSERTION order, rows in triangle-id order."""

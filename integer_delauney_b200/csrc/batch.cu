@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <memory>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -271,9 +272,17 @@ Plan make_plan(int n_images, const int32_t* dims, const int64_t* counts, int P)
 
 // The pipeline; seeds already in C.seeds_in.  Leaves per-image grids in
 // d_out (or C.outgrid) and image-local triangle rows in C.tris.
+// What idl_delaunay_adopt needs of the last labels-only batch on a context.
+struct LabelsOnly {
+    std::vector<BImg> imgs;
+    int P = 0, pitch = 0;
+    int64_t n_seeds = 0;
+};
+
 void run_batch(Context& C, const Plan& pl, int P, int n_images, int32_t* d_out, int64_t* tri_counts,
-               float* timings)
+               float* timings, bool labels_only = false)
 {
+    C.batch_plan.reset();
     const int64_t n = pl.n_seeds;
     C.batch_img.ensure(pl.imgs.size() * sizeof(BImg));
     C.batch_seed_img.ensure((size_t)n * 4);
@@ -349,6 +358,15 @@ void run_batch(Context& C, const Plan& pl, int P, int n_images, int32_t* d_out, 
     mark(1);
     propagate(C, IDL_MODE_REFERENCE, cv, C.pos.as<uint32_t>());
     mark(2);
+    if (labels_only) {
+        auto lo = std::make_shared<LabelsOnly>();
+        lo->imgs = pl.imgs;
+        lo->P = P;
+        lo->pitch = cv.pitch;
+        lo->n_seeds = n;
+        C.batch_plan = lo;
+        return;
+    }
     detect_triangles(C, cv, C.lab[0].as<int32_t>(), C.pos.as<uint32_t>(), n, 0, timings ? ev[3] : nullptr);
 
     // per-image counts, offsets and windows; raster; compose
@@ -402,11 +420,49 @@ void run_batch(Context& C, const Plan& pl, int P, int n_images, int32_t* d_out, 
 }
 
 }  // namespace
+
+bool batch_image(const Context& C, int k, BatchImage& out)
+{
+    const auto* lo = static_cast<const LabelsOnly*>(C.batch_plan.get());
+    if (!lo || k < 0 || k >= (int)lo->imgs.size()) return false;
+    const BImg& m = lo->imgs[k];
+    out.W = m.W;
+    out.H = m.H;
+    out.ox = m.ox;
+    out.oy = m.oy;
+    out.P = lo->P;
+    out.pitch = lo->pitch;
+    out.seed_off = m.seed_off;
+    out.n = (k + 1 < (int)lo->imgs.size() ? lo->imgs[k + 1].seed_off : lo->n_seeds) - m.seed_off;
+    return true;
+}
+
 }  // namespace idl
 
 using namespace idl;
 
 extern "C" {
+
+int idl_voronoi_batch(idl_context* ctx, int n_images, const int32_t* dims, const int64_t* seed_counts,
+                      const int32_t* seeds_xy, int border_padding, int mode)
+{
+    IDL_API_BEGIN
+    if (!ctx) invalid("context must not be NULL");
+    if (!dims || !seed_counts) invalid("dims and seed_counts must not be NULL");
+    if (mode != IDL_MODE_REFERENCE) invalid("batched propagation supports voronoi_mode 'reference' only");
+    const int P = border_padding == IDL_AUTO_BORDER_PADDING ? IDL_DEFAULT_BORDER_PADDING
+                                                            : std::max(0, border_padding);
+    const Plan pl = make_plan(n_images, dims, seed_counts, P);
+    if (!seeds_xy) invalid("seeds must not be NULL");
+    DeviceGuard g(ctx->device);
+    Context& C = *ctx;
+    C.have_result = false;
+    C.batch_plan.reset();
+    C.seeds_in.ensure((size_t)pl.n_seeds * 8);
+    IDL_CUDA(cudaMemcpyAsync(C.seeds_in.ptr, seeds_xy, (size_t)pl.n_seeds * 8, cudaMemcpyHostToDevice, C.stream));
+    run_batch(C, pl, P, n_images, nullptr, nullptr, nullptr, true);
+    IDL_API_END
+}
 
 int idl_triangulate_batch(idl_context* ctx, int n_images, const int32_t* dims, const int64_t* seed_counts,
                           const int32_t* seeds_xy, int border_padding, int mode, int32_t* grids_out,

@@ -10,6 +10,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <memory>
 #include <string>
 
 #include "common.cuh"
@@ -132,6 +133,7 @@ struct Context {
     bool host_sc_borrowed = false;  // host_sc points at static storage, not cudaMallocHost memory
 
     const void* owner = nullptr; // object whose intermediates the buffers hold (shared workspaces)
+    std::shared_ptr<void> batch_plan;  // layout of the last labels-only batch (batch.cu)
     int64_t last_n_tri = 0;      // triangles of the last triangulation (host copy)
     bool have_result = false;
 
@@ -222,6 +224,16 @@ void assign_pixels(Context& C, int W, int H, const int32_t* xs, const int32_t* y
                    int64_t max_tri);
 
 void ensure_scalars(Context& C);
+
+// One image of the last labels-only batch on a context (idl_voronoi_batch):
+// its padded canvas sits at (ox, oy) of the atlas label planes C.lab[0/1]
+// (row pitch `pitch`), its seeds are C.xs/C.ys[seed_off, seed_off + n) in
+// (x, y) order with atlas labels seed_off + local id (batch.cu).
+struct BatchImage {
+    int W, H, ox, oy, P, pitch;
+    int64_t seed_off, n;
+};
+bool batch_image(const Context& C, int k, BatchImage& out);
 
 }  // namespace idl
 

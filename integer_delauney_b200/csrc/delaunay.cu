@@ -66,12 +66,11 @@ struct DelaunayState {
     uint8_t* pix_out = nullptr;
 
     // grow-only scratch
-    DevBuf stage, edge_keys, edge_tmp, sort_tmp, num_sel, scores, score_keys, score_sorted, qbuf, qout;
+    DevBuf stage, edge_keys, edge_tmp, sort_tmp, num_sel, scores, score_keys, score_sorted, qbuf, qout, batch, verr;
 
     // host mirrors (insertion order, image coordinates)
     std::vector<int32_t> hx, hy;
     std::vector<float> hvals;
-    std::unordered_set<uint64_t> seen;
 
     Canvas canvas() const { return Canvas{Wd, Hd, pitch}; }
 
@@ -79,11 +78,21 @@ struct DelaunayState {
     // this object: its label planes point at ours, and if another object used
     // it last, the triangle rows it holds are not ours, so topology is redone
     // when next needed (the raster, ranks and seeds live in our own memory).
+    //
+    // The binding of the planes is undone when the entry point returns
+    // (unbind), so a context lent as a workspace keeps its own label buffers
+    // for its other users.
     Context& ctx()
     {
         Context& c = ws ? *ws : own;
         if (!ws && !own.scalars.ptr) ensure_scalars(own);
         c.stream = stream;
+        if (bound != &c) {
+            unbind();
+            saved[0] = c.lab[0];
+            saved[1] = c.lab[1];
+            bound = &c;
+        }
         const size_t plane = (size_t)pitch * Hd;
         c.lab[0].borrow(planes, plane * 4);
         c.lab[1].borrow(planes + plane, plane * 4);
@@ -93,6 +102,16 @@ struct DelaunayState {
         }
         return c;
     }
+
+    void unbind() noexcept
+    {
+        if (!bound) return;
+        bound->lab[0] = saved[0];
+        bound->lab[1] = saved[1];
+        bound = nullptr;
+    }
+    Context* bound = nullptr;     // context whose label buffers currently point at our planes
+    DevBuf saved[2];              // its own label buffers meanwhile
 
     // Device memory of the object comes from the stream-ordered allocator:
     // freeing it never waits for the whole device, which matters when many
@@ -106,11 +125,12 @@ struct DelaunayState {
         planes = tgrid = seedmem = nullptr;
         pixmem = nullptr;
         DevBuf* all[] = {&stage, &edge_keys, &edge_tmp, &sort_tmp, &num_sel, &scores, &score_keys, &score_sorted,
-                         &qbuf, &qout};
+                         &qbuf, &qout, &batch, &verr};
         for (DevBuf* b : all) b->release();
     }
     ~DelaunayState()
     {
+        unbind();
         if (ws && ws->owner == this) ws->owner = nullptr;
         free_owned();
     }
@@ -122,8 +142,6 @@ struct idl_delaunay : idl::DelaunayState {};
 
 namespace idl {
 namespace {
-
-inline uint64_t pack_xy(int32_t x, int32_t y) { return ((uint64_t)(uint32_t)x << 32) | (uint32_t)y; }
 
 // ---- kernels ------------------------------------------------------------
 
@@ -138,6 +156,86 @@ __global__ void k_put_seeds(int32_t* __restrict__ a, int32_t* __restrict__ b, in
     const size_t o = (size_t)pos_y(p) * pitch + pos_x(p);
     a[o] = (int32_t)(first_id + i);
     b[o] = (int32_t)(first_id + i);
+}
+
+// ---- batch validation (before any change), on the raster as scratch ----
+// Out-of-bounds seeds are recorded and skipped; each in-bounds seed's cell
+// is reset to "no seed yet".
+__global__ void k_v_bounds(const int32_t* __restrict__ xy, int64_t k, int W, int H, int P, int Wd,
+                           int32_t* __restrict__ mark, unsigned long long* __restrict__ err)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k) return;
+    const int32_t x = xy[2 * i], y = xy[2 * i + 1];
+    if (x < 0 || y < 0 || x >= W || y >= H) {
+        atomicMin(&err[0], (unsigned long long)i);
+        return;
+    }
+    mark[(size_t)(y + P) * Wd + x + P] = 0x7FFFFFFF;
+}
+
+// Each cell remembers the first batch index that names it.
+__global__ void k_v_first(const int32_t* __restrict__ xy, int64_t k, int W, int H, int P, int Wd,
+                          int32_t* __restrict__ mark)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k) return;
+    const int32_t x = xy[2 * i], y = xy[2 * i + 1];
+    if (x < 0 || y < 0 || x >= W || y >= H) return;
+    atomicMin(&mark[(size_t)(y + P) * Wd + x + P], (int32_t)i);
+}
+
+// err[1]: first index repeating an earlier one of the batch; err[2]: first
+// index at a position the diagram already has a seed on.
+__global__ void k_v_check(const int32_t* __restrict__ xy, int64_t k, int W, int H, int P, int Wd, int pitch,
+                          const int32_t* __restrict__ mark, const int32_t* __restrict__ plane,
+                          const uint32_t* __restrict__ pos, int64_t n_old, unsigned long long* __restrict__ err)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k) return;
+    const int32_t x = xy[2 * i], y = xy[2 * i + 1];
+    if (x < 0 || y < 0 || x >= W || y >= H) return;
+    if (mark[(size_t)(y + P) * Wd + x + P] != (int32_t)i) atomicMin(&err[1], (unsigned long long)i);
+    const int32_t l = plane[(size_t)(y + P) * pitch + x + P];
+    if (l >= 0 && l < n_old && pos[l] == pack_pos(x + P, y + P)) atomicMin(&err[2], (unsigned long long)i);
+}
+
+// One block per row of an image's padded canvas: the atlas labels of that
+// image, as local ids, into both of the object's planes.
+__global__ void k_adopt(const int32_t* __restrict__ atlas, int apitch, int ox, int oy, long long seed_off, int Wd,
+                        int32_t* __restrict__ a, int32_t* __restrict__ b, int pitch)
+{
+    const int r = blockIdx.x;
+    const int32_t* src = atlas + (size_t)(oy + r) * apitch + ox;
+    const size_t o = (size_t)r * pitch;
+    for (int c = threadIdx.x; c < Wd; c += blockDim.x) {
+        const int32_t l = src[c];
+        const int32_t v = l >= 0 ? (int32_t)(l - seed_off) : UNDEF;
+        a[o + c] = v;
+        b[o + c] = v;
+    }
+}
+
+__global__ void k_split(const int32_t* __restrict__ xy, int64_t k, int32_t* __restrict__ x, int32_t* __restrict__ y)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k) return;
+    x[i] = xy[2 * i];
+    y[i] = xy[2 * i + 1];
+}
+
+__global__ void k_pack_pos(const int32_t* __restrict__ x, const int32_t* __restrict__ y, int64_t k, int P,
+                           uint32_t* __restrict__ pos)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < k) pos[i] = pack_pos(x[i] + P, y[i] + P);
+}
+
+__global__ void k_permute(const float* __restrict__ in, const int32_t* __restrict__ rank, int64_t k,
+                          float* __restrict__ out)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < k) out[rank[i]] = in[i];
 }
 
 __device__ __forceinline__ void cell_out(const int32_t* __restrict__ lab, int pitch, int P, int x, int y,
@@ -265,17 +363,29 @@ __global__ void k_score_keys(const float* __restrict__ scores, int64_t n, float 
     keys[i] = ((unsigned long long)hi << 32) | (uint32_t)i;
 }
 
-// Endpoints (insertion ids) of the first `take` edges in sorted key order.
-__global__ void k_take_edges(const unsigned long long* __restrict__ sorted, int take,
-                             const unsigned long long* __restrict__ edge_keys, int64_t n_seeds,
-                             int32_t* __restrict__ out)
+// Midpoints of the first `take` edges in sorted key order, on the padded
+// canvas, rounded half to even (lrint) and clamped to the image
+// (midpoints_from_sorted_kernel, delaunay_scalar_field.cu:129-160): the padded
+// pixel index, or -1 where the pixel already holds a seed (its cell's label
+// is a seed at that very position).
+__global__ void k_midpoints(const unsigned long long* __restrict__ sorted, int take,
+                            const unsigned long long* __restrict__ edge_keys, int64_t n_seeds,
+                            const int32_t* __restrict__ x, const int32_t* __restrict__ y, int P, int Wd, int Hd,
+                            int pitch, const int32_t* __restrict__ plane, const uint32_t* __restrict__ pos,
+                            long long* __restrict__ out)
 {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= take) return;
     const uint32_t e = (uint32_t)(sorted[r] & 0xFFFFFFFFull);
     const unsigned long long k = edge_keys[e];
-    out[r * 2] = (int32_t)(k / (unsigned long long)n_seeds);
-    out[r * 2 + 1] = (int32_t)(k % (unsigned long long)n_seeds);
+    const int32_t a = (int32_t)(k / (unsigned long long)n_seeds), b = (int32_t)(k % (unsigned long long)n_seeds);
+    int mx = (int)lrint(0.5 * ((double)(x[a] + P) + (double)(x[b] + P)));
+    int my = (int)lrint(0.5 * ((double)(y[a] + P) + (double)(y[b] + P)));
+    mx = min(max(mx, P), Wd - 1 - P);
+    my = min(max(my, P), Hd - 1 - P);
+    const int32_t l = plane[(size_t)my * pitch + mx];
+    const bool seeded = l >= 0 && pos[l] == pack_pos(mx, my);
+    out[r] = seeded ? -1ll : (long long)my * Wd + mx;
 }
 
 // Containing triangle of each query (image coordinates), read from the
@@ -526,7 +636,6 @@ void layout(DelaunayState& d, int width, int height, int64_t max_seeds, int P)
     d.hx.clear();
     d.hy.clear();
     d.hvals.clear();
-    d.seen.clear();
     IDL_CUDA(cudaMemsetAsync(d.planes, 0xFF, plane * 2 * sizeof(int32_t), d.stream));
     IDL_CUDA(cudaMemsetAsync(d.tgrid, 0xFF, (size_t)d.Wd * d.Hd * sizeof(int32_t), d.stream));
     IDL_CUDA(cudaMemsetAsync(d.values, 0, (size_t)max_seeds * sizeof(float), d.stream));
@@ -537,6 +646,11 @@ void check_handle(const idl_delaunay* d)
 {
     if (!d) invalid("Delaunay handle must not be NULL");
 }
+
+struct Unbinder {
+    DelaunayState* d;
+    ~Unbinder() { d->unbind(); }
+};
 
 }  // namespace
 }  // namespace idl
@@ -595,6 +709,7 @@ int idl_delaunay_reset(idl_delaunay* d, int width, int height, int64_t max_seeds
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     if (width <= 0 || height <= 0 || max_seeds <= 0) invalid("dimensions and max_seeds must be positive");
     const int P = border_padding >= 0 ? border_padding : IDL_DEFAULT_BORDER_PADDING;
     const int64_t Wd = (int64_t)width + 2 * P, Hd = (int64_t)height + 2 * P;
@@ -622,6 +737,7 @@ int idl_delaunay_set_stream(idl_delaunay* d, void* stream)
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     d->stream = static_cast<cudaStream_t>(stream);
     IDL_API_END
 }
@@ -630,6 +746,7 @@ int idl_delaunay_set_workspace(idl_delaunay* d, idl_context* ws)
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     if (ws && ws->device != d->device) invalid("the workspace context belongs to another device");
     d->ws = ws;
     IDL_API_END
@@ -637,48 +754,93 @@ int idl_delaunay_set_workspace(idl_delaunay* d, idl_context* ws)
 
 int idl_delaunay_insert(idl_delaunay* d, const int32_t* xy, int64_t k, const float* values, float* timings)
 {
+    return idl_delaunay_insert_ordered(d, xy, k, values, 0, timings);
+}
+
+int idl_delaunay_insert_ordered(idl_delaunay* d, const int32_t* xy, int64_t k, const float* values, int order,
+                                float* timings)
+{
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     if (timings)
         for (int i = 0; i < IDL_T_COUNT; ++i) timings[i] = 0.f;
+    if (order != 0 && order != 1) invalid("order must be 0 (as given) or 1 (x, y)");
     if (k < 0) invalid("seed count must not be negative");
     if (k == 0) return IDL_OK;
     if (!xy) invalid("seeds must not be NULL");
     // validation before any change (delaunay.cu:190-212)
     if (d->N + k > d->max_seeds) invalid("insert would exceed max_seeds capacity");
-    for (int64_t i = 0; i < k; ++i) {
-        const int32_t x = xy[2 * i], y = xy[2 * i + 1];
-        if (x < 0 || x >= d->W || y < 0 || y >= d->H) invalid("seed coordinate out of bounds");
-    }
-    {
-        std::unordered_set<uint64_t> batch;
-        batch.reserve((size_t)k * 2);
-        for (int64_t i = 0; i < k; ++i) {
-            const uint64_t key = pack_xy(xy[2 * i], xy[2 * i + 1]);
-            if (!batch.insert(key).second) invalid("duplicate seed positions within batch");
-            if (d->seen.count(key)) invalid("seed position already exists");
-        }
-    }
     DeviceGuard g(d->device);
     Context& C = d->ctx();
-    ++d->generation;
     const int64_t n0 = d->N;
-    std::vector<int32_t> host((size_t)k * 3);
-    for (int64_t i = 0; i < k; ++i) {
-        const int32_t x = xy[2 * i], y = xy[2 * i + 1];
-        host[i] = x;
-        host[k + i] = y;
-        host[2 * k + i] = (int32_t)(uint32_t(x + d->P) | (uint32_t(y + d->P) << 16));
-        d->hx.push_back(x);
-        d->hy.push_back(y);
-        d->seen.insert(pack_xy(x, y));
+
+    // upload, then validate on the device: bounds, repeats within the batch,
+    // positions already seeded (a seed's own cell always holds its label)
+    d->batch.ensure((size_t)k * 6 * 4);
+    int32_t* b_xy = d->batch.as<int32_t>();
+    int32_t* b_tx = b_xy + 2 * k;
+    int32_t* b_ty = b_xy + 3 * k;
+    int32_t* b_rank = b_xy + 4 * k;
+    int32_t* b_inv = b_xy + 5 * k;
+    d->verr.ensure(3 * sizeof(unsigned long long));
+    unsigned long long* err = d->verr.as<unsigned long long>();
+    IDL_CUDA(cudaMemcpyAsync(b_xy, xy, (size_t)k * 8, cudaMemcpyHostToDevice, C.stream));
+    IDL_CUDA(cudaMemsetAsync(err, 0xFF, 3 * sizeof(unsigned long long), C.stream));
+    const unsigned gk = blocks(k);
+    k_v_bounds<<<gk, 256, 0, C.stream>>>(b_xy, k, d->W, d->H, d->P, d->Wd, d->tgrid, err);
+    IDL_LAUNCH();
+    k_v_first<<<gk, 256, 0, C.stream>>>(b_xy, k, d->W, d->H, d->P, d->Wd, d->tgrid);
+    IDL_LAUNCH();
+    k_v_check<<<gk, 256, 0, C.stream>>>(b_xy, k, d->W, d->H, d->P, d->Wd, d->pitch, d->tgrid, d->planes, d->pos,
+                                        n0, err);
+    IDL_LAUNCH();
+    unsigned long long he[3];
+    IDL_CUDA(cudaMemcpyAsync(he, err, sizeof(he), cudaMemcpyDeviceToHost, C.stream));
+    IDL_CUDA(cudaStreamSynchronize(C.stream));
+    d->raster_dirty = true;   // the raster served as scratch; it is rebuilt when next read
+    if (he[0] != ~0ull) invalid("seed coordinate out of bounds");
+    if (he[1] != ~0ull || he[2] != ~0ull)
+        invalid(he[1] <= he[2] ? "duplicate seed positions within batch" : "seed position already exists");
+
+    ++d->generation;
+    // coordinates in insertion order, or (order 1) this batch in (x, y) order
+    if (order == 0) {
+        k_split<<<gk, 256, 0, C.stream>>>(b_xy, k, d->ix + n0, d->iy + n0);
+        IDL_LAUNCH();
+    } else {
+        k_split<<<gk, 256, 0, C.stream>>>(b_xy, k, b_tx, b_ty);
+        IDL_LAUNCH();
+        rank_seeds_device(C, d->W, d->H, b_tx, b_ty, k, 0, b_rank, b_inv, d->ix + n0, d->iy + n0);
     }
-    IDL_CUDA(cudaMemcpyAsync(d->ix + n0, host.data(), (size_t)k * 4, cudaMemcpyHostToDevice, C.stream));
-    IDL_CUDA(cudaMemcpyAsync(d->iy + n0, host.data() + k, (size_t)k * 4, cudaMemcpyHostToDevice, C.stream));
-    IDL_CUDA(cudaMemcpyAsync(d->pos + n0, host.data() + 2 * k, (size_t)k * 4, cudaMemcpyHostToDevice, C.stream));
+    k_pack_pos<<<gk, 256, 0, C.stream>>>(d->ix + n0, d->iy + n0, k, d->P, d->pos + n0);
+    IDL_LAUNCH();
+    const size_t hn = d->hx.size();
+    d->hx.resize(hn + k);
+    d->hy.resize(hn + k);
+    if (order == 0) {
+        for (int64_t i = 0; i < k; ++i) {
+            d->hx[hn + i] = xy[2 * i];
+            d->hy[hn + i] = xy[2 * i + 1];
+        }
+    } else {
+        IDL_CUDA(cudaMemcpyAsync(d->hx.data() + hn, d->ix + n0, (size_t)k * 4, cudaMemcpyDeviceToHost, C.stream));
+        IDL_CUDA(cudaMemcpyAsync(d->hy.data() + hn, d->iy + n0, (size_t)k * 4, cudaMemcpyDeviceToHost, C.stream));
+    }
     if (values) {
-        IDL_CUDA(cudaMemcpyAsync(d->values + n0, values, (size_t)k * 4, cudaMemcpyHostToDevice, C.stream));
-        d->hvals.insert(d->hvals.end(), values, values + k);
+        const size_t vn = d->hvals.size();
+        d->hvals.resize(vn + k);
+        if (order == 0) {
+            IDL_CUDA(cudaMemcpyAsync(d->values + n0, values, (size_t)k * 4, cudaMemcpyHostToDevice, C.stream));
+            std::copy(values, values + k, d->hvals.begin() + vn);
+        } else {
+            float* b_val = reinterpret_cast<float*>(b_tx);   // free again after the rank
+            IDL_CUDA(cudaMemcpyAsync(b_val, values, (size_t)k * 4, cudaMemcpyHostToDevice, C.stream));
+            k_permute<<<gk, 256, 0, C.stream>>>(b_val, b_rank, k, d->values + n0);
+            IDL_LAUNCH();
+            IDL_CUDA(cudaMemcpyAsync(d->hvals.data() + vn, d->values + n0, (size_t)k * 4, cudaMemcpyDeviceToHost,
+                                     C.stream));
+        }
         d->have_values = true;
     }
     d->N += k;
@@ -686,8 +848,8 @@ int idl_delaunay_insert(idl_delaunay* d, const int32_t* xy, int64_t k, const flo
     d->pending = true;
 
     Timer T(C, timings != nullptr);
-    k_put_seeds<<<blocks(k), 256, 0, C.stream>>>(d->planes, d->planes + (size_t)d->pitch * d->Hd, d->pitch,
-                                                 d->pos + n0, k, n0);
+    k_put_seeds<<<gk, 256, 0, C.stream>>>(d->planes, d->planes + (size_t)d->pitch * d->Hd, d->pitch, d->pos + n0,
+                                          k, n0);
     IDL_LAUNCH();
     const int64_t passes = propagate(C, d->mode, d->canvas(), d->pos, d->pos + n0, k);
     const float bfs = T.stop();
@@ -699,10 +861,49 @@ int idl_delaunay_insert(idl_delaunay* d, const int32_t* xy, int64_t k, const flo
     IDL_API_END
 }
 
+int idl_delaunay_adopt(idl_delaunay* d, idl_context* src, int image)
+{
+    IDL_API_BEGIN
+    check_handle(d);
+    const Unbinder unbind_on_exit{d};
+    if (!src) invalid("context must not be NULL");
+    BatchImage bi;
+    if (!batch_image(*src, image, bi)) invalid("the context holds no labels-only batch with that image");
+    if (src->device != d->device) invalid("the batch was computed on another device");
+    if (bi.W != d->W || bi.H != d->H || bi.P != d->P)
+        invalid("the batch image's size or border padding differs from the object's");
+    if (d->N != 0) invalid("adopt needs an empty object (reset it first)");
+    if (bi.n > d->max_seeds) invalid("insert would exceed max_seeds capacity");
+    DeviceGuard g(d->device);
+    Context& C = d->ctx();
+    const int32_t* atlas = src->lab[0].as<int32_t>();
+    k_adopt<<<dim3((unsigned)d->Hd), 256, 0, C.stream>>>(atlas, bi.pitch, bi.ox, bi.oy, bi.seed_off, d->Wd,
+                                                        d->planes, d->planes + (size_t)d->pitch * d->Hd, d->pitch);
+    IDL_LAUNCH();
+    const int64_t n = bi.n;
+    IDL_CUDA(cudaMemcpyAsync(d->ix, src->xs.as<int32_t>() + bi.seed_off, (size_t)n * 4, cudaMemcpyDeviceToDevice,
+                             C.stream));
+    IDL_CUDA(cudaMemcpyAsync(d->iy, src->ys.as<int32_t>() + bi.seed_off, (size_t)n * 4, cudaMemcpyDeviceToDevice,
+                             C.stream));
+    k_pack_pos<<<blocks(n), 256, 0, C.stream>>>(d->ix, d->iy, n, d->P, d->pos);
+    IDL_LAUNCH();
+    d->hx.resize(n);
+    d->hy.resize(n);
+    IDL_CUDA(cudaMemcpyAsync(d->hx.data(), d->ix, (size_t)n * 4, cudaMemcpyDeviceToHost, C.stream));
+    IDL_CUDA(cudaMemcpyAsync(d->hy.data(), d->iy, (size_t)n * 4, cudaMemcpyDeviceToHost, C.stream));
+    IDL_CUDA(cudaStreamSynchronize(C.stream));
+    ++d->generation;
+    d->N = n;
+    d->rank_dirty = d->topo_dirty = d->raster_dirty = d->edges_dirty = true;
+    d->pending = true;
+    IDL_API_END
+}
+
 int idl_delaunay_finalise(idl_delaunay* d, int32_t* grid_out, int64_t* n_tri_out, float* timings)
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     if (timings)
         for (int i = 0; i < IDL_T_COUNT; ++i) timings[i] = 0.f;
     DeviceGuard g(d->device);
@@ -736,6 +937,7 @@ int idl_delaunay_finalise_device(idl_delaunay* d, int64_t* n_tri_out, const int3
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     DeviceGuard g(d->device);
     Context& C = d->ctx();
     ++d->generation;
@@ -758,6 +960,7 @@ int idl_delaunay_triangles(idl_delaunay* d, int ids, int32_t* out, int64_t capac
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     if (ids != 0 && ids != 1) invalid("ids must be 0 (batch) or 1 (insertion order)");
     DeviceGuard g(d->device);
     Context& C = d->ctx();
@@ -783,6 +986,7 @@ int idl_delaunay_edges(idl_delaunay* d, int32_t* out, int64_t capacity, int64_t*
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     DeviceGuard g(d->device);
     Context& C = d->ctx();
     ensure_edges(*d);
@@ -802,6 +1006,7 @@ int idl_delaunay_edge_scores(idl_delaunay* d, double min_length, float* out, int
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     DeviceGuard g(d->device);
     ensure_edges(*d);
     if (n_out) *n_out = d->n_edges;
@@ -821,6 +1026,7 @@ int idl_delaunay_select_midpoints(idl_delaunay* d, double min_length, int count,
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     if (n_out) *n_out = 0;
     DeviceGuard g(d->device);
     Context& C = d->ctx();
@@ -850,28 +1056,21 @@ int idl_delaunay_select_midpoints(idl_delaunay* d, double min_length, int count,
     int take = 0;
     while (take < look && (head[take] >> 32) != 0xFFFFFFFFull) ++take;
     if (take == 0) return IDL_OK;
-    d->stage.ensure((size_t)take * 2 * 4);
-    k_take_edges<<<blocks(take), 256, 0, C.stream>>>(d->score_sorted.as<unsigned long long>(), take,
-                                                     d->edge_keys.as<unsigned long long>(), d->N,
-                                                     d->stage.as<int32_t>());
+    d->stage.ensure((size_t)take * 8);
+    k_midpoints<<<blocks(take), 256, 0, C.stream>>>(d->score_sorted.as<unsigned long long>(), take,
+                                                    d->edge_keys.as<unsigned long long>(), d->N, d->ix, d->iy, d->P,
+                                                    d->Wd, d->Hd, d->pitch, d->planes, d->pos,
+                                                    d->stage.as<long long>());
     IDL_LAUNCH();
-    std::vector<int32_t> ab((size_t)take * 2);
-    IDL_CUDA(cudaMemcpyAsync(ab.data(), d->stage.ptr, ab.size() * 4, cudaMemcpyDeviceToHost, C.stream));
+    std::vector<long long> pix((size_t)take);
+    IDL_CUDA(cudaMemcpyAsync(pix.data(), d->stage.ptr, pix.size() * 8, cudaMemcpyDeviceToHost, C.stream));
     IDL_CUDA(cudaStreamSynchronize(C.stream));
-    // midpoints on the padded canvas, rounded half to even as lrint does
-    // (midpoints_from_sorted_kernel, delaunay_scalar_field.cu:129-160)
+    // collisions keep the best-ranked edge; results ascend by padded pixel
     std::vector<std::pair<int64_t, int>> cand;
     cand.reserve(take);
     const int P = d->P;
-    for (int r = 0; r < take; ++r) {
-        const int32_t a = ab[2 * r], b = ab[2 * r + 1];
-        int mx = (int)std::lrint(0.5 * ((double)(d->hx[a] + P) + (double)(d->hx[b] + P)));
-        int my = (int)std::lrint(0.5 * ((double)(d->hy[a] + P) + (double)(d->hy[b] + P)));
-        mx = std::min(std::max(mx, P), d->Wd - 1 - P);
-        my = std::min(std::max(my, P), d->Hd - 1 - P);
-        if (d->seen.count(pack_xy(mx - P, my - P))) continue;
-        cand.emplace_back((int64_t)my * d->Wd + mx, r);
-    }
+    for (int r = 0; r < take; ++r)
+        if (pix[r] >= 0) cand.emplace_back(pix[r], r);
     std::sort(cand.begin(), cand.end());
     std::vector<int32_t> res;
     for (size_t i = 0; i < cand.size(); ++i) {
@@ -892,6 +1091,7 @@ int idl_delaunay_locate(idl_delaunay* d, const int32_t* pts, int64_t n, int32_t*
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     if (n < 0) invalid("query count must not be negative");
     if (n == 0) return IDL_OK;
     if (!pts || !out) invalid("query and output buffers must not be NULL");
@@ -913,6 +1113,7 @@ int idl_delaunay_in_circumsphere(idl_delaunay* d, const int32_t* pts, const doub
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     if (n < 0) invalid("query count must not be negative");
     if (n == 0) return IDL_OK;
     if (!pts || !t || !mask || !tids) invalid("query and output buffers must not be NULL");
@@ -941,6 +1142,7 @@ int idl_delaunay_seeds(idl_delaunay* d, int32_t* xy_out, float* values_out, int6
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     if (xy_out)
         for (int64_t i = 0; i < d->N; ++i) {
             xy_out[2 * i] = d->hx[i];
@@ -955,6 +1157,7 @@ int idl_delaunay_sorted_rank(idl_delaunay* d, int32_t* out)
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     if (d->N == 0) return IDL_OK;
     if (!out) invalid("output must not be NULL");
     DeviceGuard g(d->device);
@@ -968,6 +1171,7 @@ int idl_delaunay_voronoi(idl_delaunay* d, int32_t* out)
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     if (!out) invalid("output must not be NULL");
     DeviceGuard g(d->device);
     Context& C = d->ctx();
@@ -991,6 +1195,7 @@ int idl_delaunay_info(idl_delaunay* d, int64_t* info, int count)
 {
     IDL_API_BEGIN
     check_handle(d);
+    const Unbinder unbind_on_exit{d};
     if (!info) invalid("output must not be NULL");
     const int64_t device_bytes = (int64_t)(d->planes_bytes + d->tgrid_bytes + d->pix_bytes +
                                            (size_t)d->seed_cap * 32 + d->own.workspace_bytes()) +

@@ -44,6 +44,7 @@ from . import _capi
 
 SIZE_CLASS = 128            # object canvases are rounded up to multiples of this
 SEED_HEADROOM = 50_000      # seed capacity beyond the initial set, for inserts
+GROUP_MAX = 32              # new diagrams propagated together in one launch, at most
 
 
 @dataclass
@@ -101,6 +102,20 @@ def _class_dims(width: int, height: int):
     return r(width), r(height)
 
 
+def _capacity(width: int, height: int, max_seeds: int, padding: int) -> tuple:
+    """The four allocations of a Delaunay object created for this canvas:
+    label planes, padded raster, pixel outputs (bytes) and seed slots."""
+    Wd, Hd = width + 2 * padding, height + 2 * padding
+    return ((Wd + 31) // 32 * 32 * Hd * 8, Wd * Hd * 4, width * height * 9, max_seeds)
+
+
+def _fits(cap: tuple, width: int, height: int, max_seeds: int, padding: int) -> bool:
+    """Whether an object with allocations `cap` can be reset to this canvas
+    (the rule of idl_delaunay_reset: areas, not sides, must fit)."""
+    need = _capacity(width, height, max_seeds, padding)
+    return all(n <= c for n, c in zip(need, cap))
+
+
 def estimate_bytes(width: int, height: int, max_seeds: int, padding: int, workspace: bool = True) -> int:
     """Device footprint of a diagram: label planes, padded raster, pixel
     outputs and seed arrays, plus (``workspace``) the scratch a triangulation
@@ -143,7 +158,8 @@ class Server:
         self._queue: collections.deque[_Request] = collections.deque()
         self._diagrams: dict[int, _Diagram] = {}
         self._pool: list[_Pooled] = []
-        self._used = max(1, int(slots)) * slot_reserve(self.padding)
+        # each slot: a workspace for diagrams and one for its grouped propagations
+        self._used = 2 * max(1, int(slots)) * slot_reserve(self.padding)
         self._ids = itertools.count()
         self._dids = itertools.count()
         self._closed = False
@@ -169,7 +185,7 @@ class Server:
         with self._cv:
             if self._closed:
                 raise RuntimeError("server is closed")
-            self._diagrams[did] = _Diagram(did, pins=1, cap=(int(width), int(height), cap))
+            self._diagrams[did] = _Diagram(did, pins=1)
             self._queue.append(req)
             self._cv.notify()
         return fut
@@ -226,14 +242,12 @@ class Server:
 
     # -- scheduling (called with the lock held) ----------------------------
     def _take_pooled(self, req: _Request) -> Optional[_Pooled]:
-        """Smallest pooled object whose class covers the request, if it is
-        not more than twice the request's own footprint."""
-        Wc, Hc = _class_dims(req.width, req.height)
+        """Smallest pooled object the request fits in, if it is not more than
+        twice the request's own footprint."""
         cap = len(req.seeds) + SEED_HEADROOM
         best = None
         for i, p in enumerate(self._pool):
-            pw, ph, pc = p.cap
-            if pw >= Wc and ph >= Hc and pc >= cap and p.bytes <= 2 * req.need and \
+            if p.bytes <= 2 * req.need and _fits(p.cap, req.width, req.height, cap, self.padding) and \
                     (best is None or p.bytes < self._pool[best].bytes):
                 best = i
         return self._pool.pop(best) if best is not None else None
@@ -288,16 +302,59 @@ class Server:
                         self._used += req.need          # charged now, corrected after creation
                     del self._queue[i]
                     d.busy = True
-                    return req, pooled
+                    return "new", [(req, pooled)] + self._group_more(req, to_free)
                 if d.busy or d.obj is None:
                     continue                            # busy, or its creation has not run yet
                 del self._queue[i]
                 d.busy = True
-                return req, None
+                return "insert", [(req, None)]
             else:
                 if self._closed and not self._queue:
                     return None
+                if self._queue and not any(d.busy for d in self._diagrams.values()):
+                    # nothing in flight can free memory any more: a new
+                    # diagram that does not fit now never will
+                    for i, req in enumerate(self._queue):
+                        if req.kind == "new":
+                            del self._queue[i]
+                            del self._diagrams[req.diagram_id]
+                            req.future.set_exception(MemoryError(
+                                f"request needs {req.need} bytes; the budget of {self.budget} bytes has "
+                                f"{self.budget - self._used} left with nothing to evict"))
+                            break
+                    else:
+                        self._cv.wait(0.1)
+                    continue
                 self._cv.wait()
+
+    def _group_more(self, first: _Request, to_free: list) -> list:
+        """Further queued new diagrams to propagate in the same launch as
+        `first`, while they fit the group limits and the memory budget."""
+        out = []
+        area = (first.width + 2 * self.padding + 1) * (first.height + 2 * self.padding + 1)
+        seeds = len(first.seeds)
+        limit_area = (MAX_SIDE + 2 * self.padding + 1) ** 2
+        i = 0
+        while i < len(self._queue) and len(out) + 1 < GROUP_MAX:
+            req = self._queue[i]
+            if req.kind != "new" or req.need > self.budget:
+                i += 1
+                continue
+            a = (req.width + 2 * self.padding + 1) * (req.height + 2 * self.padding + 1)
+            if area + a > limit_area or seeds + len(req.seeds) > MAX_REQUEST_SEEDS:
+                i += 1
+                continue
+            ok, pooled = self._place(req, to_free)
+            if not ok:
+                break
+            if pooled is None:
+                self._used += req.need
+            del self._queue[i]
+            self._diagrams[req.diagram_id].busy = True
+            out.append((req, pooled))
+            area += a
+            seeds += len(req.seeds)
+        return out
 
     # -- execution ------------------------------------------------------------
     def _worker(self):
@@ -305,6 +362,8 @@ class Server:
         torch.cuda.set_device(self.device)
         stream = torch.cuda.Stream(self.device)
         workspace = _capi.Context(self.device)   # scratch shared by every diagram this slot runs
+        batch = _capi.Context(self.device)       # atlas of the new diagrams this slot propagates together
+        lib = _capi.load()
         while True:
             to_free: list = []
             with self._cv:
@@ -312,29 +371,50 @@ class Server:
             to_free.clear()                             # objects are freed outside the lock
             if got is None:
                 return
-            req, pooled = got
-            start = time.perf_counter()
-            try:
-                with torch.cuda.stream(stream):
-                    res = self._run(req, pooled, start, workspace)
-                req.future.set_result(res)
-            except BaseException as e:   # noqa: BLE001 - delivered to the caller
-                with self._cv:
-                    dd = self._diagrams.get(req.diagram_id)
-                    if req.kind == "new" and dd is not None and dd.obj is None:
-                        self._used -= pooled.bytes if pooled is not None else req.need
-                        del self._diagrams[req.diagram_id]
-                req.future.set_exception(e)
-            finally:
-                with self._cv:
-                    d = self._diagrams.get(req.diagram_id)
-                    if d is not None:
-                        d.busy = False
-                        d.pins -= 1
-                        d.last_used = time.perf_counter()
-                    self._cv.notify_all()
+            kind, items = got
+            with torch.cuda.stream(stream):
+                src = None
+                if kind == "new":
+                    # one propagation launch for the whole group; a request
+                    # the batch rejects fails alone on the per-diagram path
+                    start = time.perf_counter()
+                    batch.set_stream(stream.cuda_stream)
+                    reqs = [r for r, _ in items]
+                    dims = np.array([(r.width, r.height) for r in reqs], dtype=np.int32)
+                    counts = np.array([len(r.seeds) for r in reqs], dtype=np.int64)
+                    seeds = np.ascontiguousarray(np.concatenate([r.seeds for r in reqs]), dtype=np.int32)
+                    st = lib.idl_voronoi_batch(batch.handle, len(reqs), dims.ctypes.data, counts.ctypes.data,
+                                               seeds.ctypes.data, self.padding, _capi.MODE_REFERENCE)
+                    src = batch if st == _capi.IDL_OK else None
+                    with self._cv:
+                        self.stats["groups"] += 1
+                        self.stats["grouped_requests"] += len(reqs)
+                else:
+                    start = time.perf_counter()
+                for k, (req, pooled) in enumerate(items):
+                    self._execute(req, pooled, start, workspace, (src, k) if src is not None else None)
 
-    def _run(self, req: _Request, pooled: Optional[_Pooled], start: float, workspace) -> Result:
+    def _execute(self, req: _Request, pooled: Optional[_Pooled], start: float, workspace, adopt) -> None:
+        try:
+            res = self._run(req, pooled, start, workspace, adopt)
+            req.future.set_result(res)
+        except BaseException as e:   # noqa: BLE001 - delivered to the caller
+            with self._cv:
+                dd = self._diagrams.get(req.diagram_id)
+                if req.kind == "new" and dd is not None and dd.obj is None:
+                    self._used -= pooled.bytes if pooled is not None else req.need
+                    del self._diagrams[req.diagram_id]
+            req.future.set_exception(e)
+        finally:
+            with self._cv:
+                d = self._diagrams.get(req.diagram_id)
+                if d is not None:
+                    d.busy = False
+                    d.pins -= 1
+                    d.last_used = time.perf_counter()
+                self._cv.notify_all()
+
+    def _run(self, req: _Request, pooled: Optional[_Pooled], start: float, workspace, adopt=None) -> Result:
         cu = self._cu
         d = self._diagrams[req.diagram_id]
         if req.kind == "new":
@@ -346,14 +426,16 @@ class Server:
             else:
                 Wc, Hc = _class_dims(req.width, req.height)
                 obj = cu.Delaunay(Wc, Hc, cap, self.padding)
+                alloc_cap = _capacity(Wc, Hc, cap, self.padding)
                 charged = req.need
                 self.stats["new_objects"] += 1
             obj.use_workspace(workspace)
             obj.reset(req.width, req.height, cap, self.padding)
-            s = req.seeds
-            order = np.lexsort((s[:, 1], s[:, 0]))
-            obj.insert_deferred(np.ascontiguousarray(s[order]))
-            seeds_after = len(s)
+            if adopt is not None:
+                obj._adopt(*adopt)
+            else:
+                obj.insert_deferred(req.seeds, order="xy")
+            seeds_after = len(req.seeds)
         else:
             obj = d.obj
             obj.use_workspace(workspace)
@@ -365,15 +447,13 @@ class Server:
             grid = np.array(grid, copy=True)
             n_tri = len(verts)
         else:
-            verts_dev = obj.finalise_device()[0]
-            n_tri = len(verts_dev)
+            n_tri = obj._finalise_device_count()
         if req.kind == "new":
             actual = max(obj.device_bytes, charged)
             with self._cv:
                 d.obj = obj
                 d.bytes = actual
-                d.cap = (_class_dims(req.width, req.height)[0], _class_dims(req.width, req.height)[1],
-                         cap)
+                d.cap = pooled.cap if pooled is not None else alloc_cap
                 self._used += actual - charged
         done = time.perf_counter()
         return Result(req.rid, req.kind, req.diagram_id, seeds_after, n_tri, req.arrival, start, done,
@@ -415,12 +495,10 @@ def run_serial(requests, border_padding: int = _capi.AUTO_BORDER_PADDING, budget
                 used -= b
                 del o
             obj = cu.Delaunay(w, h, cap, P)
-            order = np.lexsort((s[:, 1], s[:, 0]))
-            obj.insert_deferred(np.ascontiguousarray(s[order]))
-            verts = obj.finalise_device()[0]
+            obj.insert_deferred(s, order="xy")
             live[i] = (obj, need)
             used += need
-            out.append((len(s), len(verts)))
+            out.append((len(s), obj._finalise_device_count()))
         else:
             _, j, s = r
             if j not in live:
@@ -429,6 +507,5 @@ def run_serial(requests, border_padding: int = _capi.AUTO_BORDER_PADDING, budget
             obj = live[j][0]
             live.move_to_end(j)
             obj.insert_deferred(s)
-            verts = obj.finalise_device()[0]
-            out.append((obj.seed_count, len(verts)))
+            out.append((obj.seed_count, obj._finalise_device_count()))
     return out

@@ -411,3 +411,42 @@ def test_incremental_config_prefix_bit_exact(cu):
         m, g = d.insert(b)
         done.append(b)
     assert_matches_oracle(d, m, g, oracle.incremental(2048, 2048, done, 16))
+
+
+def test_ordered_insert_equals_batch_pipeline(cu):
+    """order='xy' numbers the batch by (x, y): into an empty object that is
+    the batch pipeline's numbering, so its result, bit for bit; the values
+    follow their seeds."""
+    W, H = 230, 170
+    s = uniform(W, H, 900, seed=21)
+    vals = np.arange(len(s), dtype=np.float32)
+    d = cu.Delaunay(W, H, 2000, 16)
+    d.insert_deferred(s, vals, order="xy")
+    v, g = d.finalise(as_arrays=True)
+    v1, g1 = cu.triangulate(W, H, s, 16, as_arrays=True)
+    np.testing.assert_array_equal(v, v1)
+    np.testing.assert_array_equal(g, g1)
+    order = np.lexsort((s[:, 1], s[:, 0]))
+    np.testing.assert_array_equal(d.get_seeds(), s[order])
+    np.testing.assert_array_equal(d.get_values(), vals[order])
+    np.testing.assert_array_equal(d.sorted_rank, np.arange(len(s)))
+
+
+def test_rejected_insert_changes_nothing(cu):
+    W, H = 120, 90
+    s = uniform(W, H, 200, seed=22)
+    d = cu.Delaunay(W, H, 400, 16)
+    d.insert_deferred(s[:150])
+    m0, g0 = d.finalise(as_arrays=True)
+    bad = np.concatenate([s[150:160], s[10:11]])           # repeats an existing seed
+    with pytest.raises(ValueError, match="already exists"):
+        d.insert(bad)
+    with pytest.raises(ValueError, match="within batch"):
+        d.insert(np.concatenate([s[150:160], s[155:156]]))
+    with pytest.raises(ValueError, match="out of bounds"):
+        d.insert(np.concatenate([s[150:160], [[W, 0]]]))
+    assert d.seed_count == 150
+    m1, g1 = d.finalise(as_arrays=True)
+    np.testing.assert_array_equal(m0, m1)
+    np.testing.assert_array_equal(g0, g1)
+    np.testing.assert_array_equal(d.locate(s[:50]), g0[s[:50, 1], s[:50, 0], 2])

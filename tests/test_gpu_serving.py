@@ -87,7 +87,8 @@ def test_new_requests_equal_the_batch_pipeline(cu):
 def test_small_budget_recycles_objects_and_keeps_results(cu):
     from integer_delauney_b200.serving import SEED_HEADROOM, estimate_bytes, slot_reserve
     news = [(200, 180, uniform(200, 180, 300, seed=i)) for i in range(12)]
-    budget = 3 * estimate_bytes(256, 256, 300 + SEED_HEADROOM, 16, workspace=False) + 2 * slot_reserve(16)
+    # two slots reserve two workspaces each; room for three diagrams besides
+    budget = 3 * estimate_bytes(256, 256, 300 + SEED_HEADROOM, 16, workspace=False) + 4 * slot_reserve(16)
     a_new, _ = _alone(cu, news, [])
     m_new, _, stats = _mixed(news, [], budget=budget, slots=2)
     for a, m in zip(a_new, m_new):
@@ -103,3 +104,37 @@ def test_over_budget_and_unknown_diagram(cu):
             f.result(timeout=60)
         with pytest.raises(KeyError):
             srv.submit_insert(12345, [(1, 1)])
+
+
+def test_adopt_from_a_batch_equals_ordered_insert(cu):
+    """idl_voronoi_batch + idl_delaunay_adopt (one propagation launch for
+    several new diagrams) leaves each object exactly as an ordered insert of
+    its seeds would; the object then takes inserts as usual."""
+    from integer_delauney_b200 import _capi
+    news, inserts = _requests(3, n_new=6)
+    ctx = _capi.Context(0)
+    lib = _capi.load()
+    dims = np.array([(W, H) for W, H, _ in news], dtype=np.int32)
+    counts = np.array([len(p) for _, _, p in news], dtype=np.int64)
+    seeds = np.ascontiguousarray(np.concatenate([p for _, _, p in news]), dtype=np.int32)
+    _capi.check(lib.idl_voronoi_batch(ctx.handle, len(news), dims.ctypes.data, counts.ctypes.data,
+                                      seeds.ctypes.data, 16, 0))
+    for k, (W, H, pts) in enumerate(news):
+        a = cu.Delaunay(W, H, len(pts) + 500, 16)
+        a._adopt(ctx, k)
+        b = cu.Delaunay(W, H, len(pts) + 500, 16)
+        b.insert_deferred(pts, order="xy")
+        for x, y in ((a, b),):
+            np.testing.assert_array_equal(x.get_voronoi_grid(), y.get_voronoi_grid())
+            np.testing.assert_array_equal(x.get_seeds(), y.get_seeds())
+        va, ga = a.finalise(as_arrays=True)
+        vb, gb = b.finalise(as_arrays=True)
+        np.testing.assert_array_equal(va, vb)
+        np.testing.assert_array_equal(ga, gb)
+        for i, add in inserts:
+            if i == k:
+                a.insert_deferred(add)
+                b.insert_deferred(add)
+        np.testing.assert_array_equal(a.finalise(as_arrays=True)[1], b.finalise(as_arrays=True)[1])
+    with pytest.raises(ValueError):
+        cu.Delaunay(7, 7, 10, 16)._adopt(ctx, 0)          # size differs from the batch image
