@@ -31,6 +31,7 @@ submitted, and no kernel reads another diagram's memory.
 from __future__ import annotations
 
 import collections
+import ctypes
 import itertools
 import threading
 import time
@@ -88,6 +89,7 @@ class _Diagram:
     pins: int = 0
     last_used: float = 0.0
     cap: tuple = ()
+    n_seeds: int = 0
 
 
 @dataclass
@@ -151,6 +153,7 @@ class Server:
         from . import _delauney_cuda as cu
         self._torch = torch
         self._cu = cu
+        self._lib = _capi.load()
         self.device = torch.cuda.current_device() if device is None else int(device)
         self.budget = int(budget_bytes)
         self.padding = cu.resolve_padding(border_padding)
@@ -392,11 +395,13 @@ class Server:
                 else:
                     start = time.perf_counter()
                 for k, (req, pooled) in enumerate(items):
-                    self._execute(req, pooled, start, workspace, (src, k) if src is not None else None)
+                    self._execute(req, pooled, start, workspace, (src, k) if src is not None else None,
+                                  stream.cuda_stream)
 
-    def _execute(self, req: _Request, pooled: Optional[_Pooled], start: float, workspace, adopt) -> None:
+    def _execute(self, req: _Request, pooled: Optional[_Pooled], start: float, workspace, adopt,
+                 stream_handle: int) -> None:
         try:
-            res = self._run(req, pooled, start, workspace, adopt)
+            res = self._run(req, pooled, start, workspace, adopt, stream_handle)
             req.future.set_result(res)
         except BaseException as e:   # noqa: BLE001 - delivered to the caller
             with self._cv:
@@ -414,8 +419,11 @@ class Server:
                     d.last_used = time.perf_counter()
                 self._cv.notify_all()
 
-    def _run(self, req: _Request, pooled: Optional[_Pooled], start: float, workspace, adopt=None) -> Result:
-        cu = self._cu
+    def _run(self, req: _Request, pooled: Optional[_Pooled], start: float, workspace, adopt=None,
+             stream_handle: int = 0) -> Result:
+        """One request on this slot's stream.  The calls go to the C ABI
+        directly (one per step), so a request costs the interpreter little."""
+        cu, lib, ck = self._cu, self._lib, _capi.check
         d = self._diagrams[req.diagram_id]
         if req.kind == "new":
             cap = len(req.seeds) + SEED_HEADROOM
@@ -429,25 +437,32 @@ class Server:
                 alloc_cap = _capacity(Wc, Hc, cap, self.padding)
                 charged = req.need
                 self.stats["new_objects"] += 1
-            obj.use_workspace(workspace)
-            obj.reset(req.width, req.height, cap, self.padding)
-            if adopt is not None:
-                obj._adopt(*adopt)
-            else:
-                obj.insert_deferred(req.seeds, order="xy")
-            seeds_after = len(req.seeds)
         else:
             obj = d.obj
-            obj.use_workspace(workspace)
-            obj.insert_deferred(req.seeds)
-            seeds_after = obj.seed_count
+        h = obj._h
+        ck(lib.idl_delaunay_set_stream(h, stream_handle or None))
+        ck(lib.idl_delaunay_set_workspace(h, workspace.handle))
+        obj._workspace = workspace
+        s = req.seeds
+        if req.kind == "new":
+            ck(lib.idl_delaunay_reset(h, req.width, req.height, cap, self.padding))
+            if adopt is not None:
+                ck(lib.idl_delaunay_adopt(h, adopt[0].handle, adopt[1]))
+            else:
+                ck(lib.idl_delaunay_insert_ordered(h, s.ctypes.data if len(s) else None, len(s), None, 1, None))
+            seeds_after = len(s)
+        else:
+            ck(lib.idl_delaunay_insert_ordered(h, s.ctypes.data if len(s) else None, len(s), None, 0, None))
+            seeds_after = d.n_seeds + len(s)
         verts = grid = None
         if req.fetch:
             verts, grid = obj.finalise(as_arrays=True)
             grid = np.array(grid, copy=True)
             n_tri = len(verts)
         else:
-            n_tri = obj._finalise_device_count()
+            n = ctypes.c_int64(0)
+            ck(lib.idl_delaunay_finalise_device(h, ctypes.byref(n), None, None, None, None))
+            n_tri = int(n.value)
         if req.kind == "new":
             actual = max(obj.device_bytes, charged)
             with self._cv:
@@ -455,6 +470,7 @@ class Server:
                 d.bytes = actual
                 d.cap = pooled.cap if pooled is not None else alloc_cap
                 self._used += actual - charged
+        d.n_seeds = seeds_after
         done = time.perf_counter()
         return Result(req.rid, req.kind, req.diagram_id, seeds_after, n_tri, req.arrival, start, done,
                       verts, grid)

@@ -142,13 +142,16 @@ def serving_trace(rate: float = 1000.0, seconds: float = 60.0, frac_new: float =
 def fresh_points(W: int, H: int, n: int, taken_keys: np.ndarray, seed: int) -> np.ndarray:
     """n distinct uniform points of a W x H canvas whose keys y * W + x are
     not in the sorted int64 array `taken_keys` (fewer if the canvas is full)."""
+    taken_keys = np.asarray(taken_keys, dtype=np.int64)
     rng = np.random.default_rng(seed)
     free = W * H - len(taken_keys)
     n = min(n, max(free, 0))
     got = np.zeros(0, dtype=np.int64)
     while len(got) < n:
         k = rng.integers(0, W * H, size=(n - len(got)) * 2 + 16, dtype=np.int64)
-        k = k[~np.isin(k, taken_keys, assume_unique=False)]
+        if len(taken_keys):
+            at = np.minimum(np.searchsorted(taken_keys, k), len(taken_keys) - 1)
+            k = k[taken_keys[at] != k]
         got = np.concatenate([got, k])
         _, first = np.unique(got, return_index=True)
         got = got[np.sort(first)]
