@@ -161,7 +161,6 @@ __device__ __forceinline__ void hash_insert(unsigned long long key, unsigned lon
         const unsigned long long prev = atomicCAS(&keys[slot], EMPTY_KEY, key);
         if (prev == EMPTY_KEY || prev == key) {
             atomicMin(&vals[slot], val);
-            if (prev == EMPTY_KEY) atomicAdd(reinterpret_cast<unsigned long long*>(&sc->n_inserted), 1ull);
             return;
         }
         slot = (slot + 1) & mask;
@@ -267,18 +266,25 @@ __global__ void k_rank(const unsigned long long* __restrict__ ukeys, const unsig
 void detect_triangles(Context& C, const Canvas& cv, const int32_t* labels, const uint32_t* pos, int64_t n,
                       int shift, cudaEvent_t mid, const int32_t* rank)
 {
-    // Unique triangles of a planar triangulation number under 2n; keep the
-    // table at most half full, and grow and redo on the rare overflow.
+    // Unique triangles of a planar triangulation number under 2n; the table
+    // starts at four times that, and on the rare probe overflow it grows and
+    // the detection is redone.  The occupied slots are counted while they are
+    // compacted (one atomic per warp), not while they are inserted, where a
+    // single counter would serialise every new key.
     int64_t cap = std::max<int64_t>(next_pow2(8 * n + 1024), C.hash_cap);
+    C.cnt.ensure((size_t)(n + 1) * 4);
+    C.off.ensure((size_t)(n + 2) * 4);
+    C.fill.ensure((size_t)(n + 1) * 4);
     for (int attempt = 0;; ++attempt) {
         C.hkeys.ensure((size_t)cap * 8);
         C.hvals.ensure((size_t)cap * 8);
-        C.ukeys.ensure((size_t)cap / 2 * 8 + 8);
-        C.uvals.ensure((size_t)cap / 2 * 8 + 8);
+        C.ukeys.ensure((size_t)cap * 8);
+        C.uvals.ensure((size_t)cap * 8);
         IDL_CUDA(cudaMemsetAsync(C.hkeys.ptr, 0xFF, (size_t)cap * 8, C.stream));
         IDL_CUDA(cudaMemsetAsync(C.hvals.ptr, 0xFF, (size_t)cap * 8, C.stream));
-        IDL_CUDA(cudaMemsetAsync(&C.sc()->n_inserted, 0, sizeof(int64_t), C.stream));
         IDL_CUDA(cudaMemsetAsync(&C.sc()->overflow, 0, sizeof(int32_t), C.stream));
+        IDL_CUDA(cudaMemsetAsync(&C.sc()->n_triangles, 0, sizeof(int64_t), C.stream));
+        IDL_CUDA(cudaMemsetAsync(C.cnt.ptr, 0, (size_t)(n + 1) * 4, C.stream));
 
         dim3 blk(32, 8);
         dim3 grd(ceil_div(std::max(cv.Wd - 1, 1), 32), ceil_div(std::max(cv.Hd - 1, 1), 8));
@@ -287,28 +293,23 @@ void detect_triangles(Context& C, const Canvas& cv, const int32_t* labels, const
         IDL_LAUNCH();
         if (mid) IDL_CUDA(cudaEventRecord(mid, C.stream));
         C.mark(PM_DETECT);
+        const int g1 = (int)std::min<int64_t>(ceil_div(cap, 256), C.num_sms * 16);
+        k_enumerate<<<g1, 256, 0, C.stream>>>(C.hkeys.as<unsigned long long>(), C.hvals.as<unsigned long long>(),
+                                              cap, C.ukeys.as<unsigned long long>(),
+                                              C.uvals.as<unsigned long long>(), C.cnt.as<int32_t>(), C.sc());
+        IDL_LAUNCH();
         C.fetch_scalars();
-        if (!C.host_sc->overflow && C.host_sc->n_inserted <= cap / 2) break;
+        if (!C.host_sc->overflow) break;
         if (attempt >= 6) throw Error(IDL_ERR_INTERNAL, "triangle hash table overflow");
         cap *= 4;
     }
+    const int64_t nu = C.host_sc->n_triangles;
+    if (nu > cap / 2) cap *= 4;          // keep the next run's table at most half full
     C.hash_cap = cap;
-    const int64_t nu = C.host_sc->n_inserted;
 
-    C.cnt.ensure((size_t)(n + 1) * 4);
-    C.off.ensure((size_t)(n + 2) * 4);
-    C.fill.ensure((size_t)(n + 1) * 4);
     C.grp.ensure((size_t)std::max<int64_t>(nu, 1) * 4);
     C.tris.ensure((size_t)std::max<int64_t>(nu, 1) * 5 * 4);
-    IDL_CUDA(cudaMemsetAsync(C.cnt.ptr, 0, (size_t)(n + 1) * 4, C.stream));
     IDL_CUDA(cudaMemsetAsync(C.fill.ptr, 0, (size_t)(n + 1) * 4, C.stream));
-    IDL_CUDA(cudaMemsetAsync(&C.sc()->n_triangles, 0, sizeof(int64_t), C.stream));
-
-    const int g1 = (int)std::min<int64_t>(ceil_div(cap, 256), C.num_sms * 16);
-    k_enumerate<<<g1, 256, 0, C.stream>>>(C.hkeys.as<unsigned long long>(), C.hvals.as<unsigned long long>(), cap,
-                                          C.ukeys.as<unsigned long long>(), C.uvals.as<unsigned long long>(),
-                                          C.cnt.as<int32_t>(), C.sc());
-    IDL_LAUNCH();
     exclusive_scan(C, C.cnt.as<int32_t>(), C.off.as<int32_t>(), n);
     const int g2 = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(nu, 256), C.num_sms * 16));
     k_group<<<g2, 256, 0, C.stream>>>(C.ukeys.as<unsigned long long>(), C.sc(), C.off.as<int32_t>(),
