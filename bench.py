@@ -499,6 +499,11 @@ def run_ours(args, rank, world):
         return ms, profs, clk.summary(), launches
 
     seeds_u = uniform(W, H, N_SEEDS, seed=rank)
+    # propagation schedule for this input class, picked by timing the
+    # candidates (untimed; every schedule gives the same result)
+    from integer_delauney_b200 import autotune
+    schedule = autotune.tune(W, H, seeds_u, PADDING, context=ctx)
+    ctx.set_stream(stream.cuda_stream)
     # headline: K plain steps; the per-stage events are recorded in a second
     # timed run, since profiling reads counters back between stages
     ms, _, clocks, launches = time_device(seeds_u, args.steps, args.warmup, profile=False)
@@ -510,10 +515,9 @@ def run_ours(args, rank, world):
     stage = {k: statistics.mean(p[k] for p in profs) for k in keys}
     p0 = profs[-1]
     hbm, peak_kind = _peaks()
-    inner_px = p0["tile_w"] * p0["tile_h"]
-    # propagation: 8 B per canvas pixel per HBM round trip (read + write a
-    # 4-byte label), over the tiles the rounds actually processed
-    prop_bytes = 8.0 * inner_px * statistics.mean(p["tiles"] for p in profs)
+    # propagation: 8 B per cell update (4-byte label in, label out), counted
+    # by the library over the tiles the schedule actually processed
+    prop_bytes = statistics.mean(p["prop_bytes"] for p in profs)
     prop_gbs = prop_bytes / (stage["propagate_ms"] / 1e3) / 1e9
     canvas = p0["canvas_px"]
     detect_gbs = 4.0 * canvas / (stage["detect_ms"] / 1e3) / 1e9
@@ -573,7 +577,8 @@ def run_ours(args, rank, world):
                    "global_batch": world, "parallelism": f"replicas x{world}",
                    "l2": "working set > L2 (label planes 2 x 68 MB, output 201 MB); no flush"},
         "stages_ms": {k[:-3]: round(v, 4) for k, v in stage.items()},
-        "propagation": {"passes": p0["passes"], "rounds": p0["rounds"], "tiles": p0["tiles"],
+        "propagation": {"schedule_dense_rounds": schedule, "passes": p0["passes"], "rounds": p0["rounds"],
+                        "tiles": p0["tiles"],
                         "tile": [p0["tile_w"], p0["tile_h"]], "steps_per_round": p0["steps_per_round"]},
         "roofline": {"bound": "hbm", "kernel": dom_kernel[:-3], "achieved": achieved, "peak": hbm,
                      "unit": "GB/s", "frac": achieved / hbm, "peak_kind": peak_kind,

@@ -94,6 +94,14 @@ IDL_API int idl_context_synchronize(idl_context* ctx);
 /* Bytes of device workspace currently held by the context. */
 IDL_API int idl_context_workspace_bytes(idl_context* ctx, int64_t* bytes_out);
 
+/* Propagation schedule from scratch (reference semantics): the first
+ * `dense_rounds` rounds of 8 passes run as tile rounds (one HBM round trip per
+ * 8 passes over every tile that can change), the rest in the persistent
+ * sparse kernel; 0 = sparse kernel only, < 0 = tile rounds to convergence.
+ * Results do not depend on it, only the time does.  Default 1.  No
+ * counterpart in the reference (its schedule is one full pass per launch). */
+IDL_API int idl_context_set_schedule(idl_context* ctx, int dense_rounds);
+
 /* Record per-stage CUDA events on the context's stream for every following
  * triangulation call (off by default; the reference's PhaseTimer,
  * src/cuda/phase_timer.cuh:17-62, plays the same role). */
@@ -115,7 +123,8 @@ IDL_API int idl_context_set_profiling(idl_context* ctx, int enable);
 #define IDL_PROF_CANVAS_PX 12   /* detection canvas pixels */
 #define IDL_PROF_IMAGE_PX 13    /* output pixels */
 #define IDL_PROF_TRIANGLES 14
-#define IDL_PROF_COUNT 15
+#define IDL_PROF_PROP_BYTES 15  /* algorithmic HBM bytes of stage (a): 8 per cell update */
+#define IDL_PROF_COUNT 16
 IDL_API int idl_context_last_profile(idl_context* ctx, double* out, int n);
 
 /* ---- stage (a): Voronoi().compute ----------------------------------- */

@@ -46,6 +46,7 @@ SIGNATURES = {
     "idl_context_destroy": (_i32, [_vp]),
     "idl_context_set_stream": (_i32, [_vp, _vp]),
     "idl_context_synchronize": (_i32, [_vp]),
+    "idl_context_set_schedule": (_i32, [_vp, _i32]),
     "idl_context_workspace_bytes": (_i32, [_vp, _pi64]),
     "idl_context_set_profiling": (_i32, [_vp, _i32]),
     "idl_context_last_profile": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _i32]),
@@ -163,12 +164,16 @@ class Context:
     def synchronize(self) -> None:
         check(self._lib.idl_context_synchronize(self.handle))
 
+    def set_schedule(self, dense_rounds: int) -> None:
+        """Propagation schedule from scratch (idl_context_set_schedule)."""
+        check(self._lib.idl_context_set_schedule(self.handle, int(dense_rounds)))
+
     def set_profiling(self, enable: bool) -> None:
         check(self._lib.idl_context_set_profiling(self.handle, 1 if enable else 0))
 
     PROFILE_KEYS = ("seeds_ms", "propagate_ms", "detect_ms", "dedup_ms", "assign_ms", "compose_ms", "rounds",
                     "tiles", "passes", "tile_w", "tile_h", "steps_per_round", "canvas_px", "image_px",
-                    "n_triangles")
+                    "n_triangles", "prop_bytes")
 
     def last_profile(self) -> dict:
         buf = (ctypes.c_double * len(self.PROFILE_KEYS))()

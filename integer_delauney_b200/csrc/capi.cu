@@ -22,7 +22,7 @@ void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 size_t Context::workspace_bytes() const
 {
     const DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
-                           &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &hkeys, &hvals, &ukeys, &uvals, &cnt,
+                           &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &big_tiles, &hkeys, &hvals, &ukeys, &uvals, &cnt,
                            &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded, &batch_img, &batch_seed_img,
                            &batch_rows, &batch_sid, &batch_stats, &batch_bad, &scalars};
     size_t s = 0;
@@ -39,7 +39,7 @@ void Context::fetch_scalars()
 Context::~Context()
 {
     DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
-                     &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &hkeys, &hvals, &ukeys, &uvals, &cnt,
+                     &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &big_tiles, &hkeys, &hvals, &ukeys, &uvals, &cnt,
                      &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded, &batch_img, &batch_seed_img,
                            &batch_rows, &batch_sid, &batch_stats, &batch_bad, &scalars};
     for (DevBuf* b : all) b->release();
@@ -185,6 +185,7 @@ int64_t run_triangulate(Context& C, int W, int H, int64_t n, const int32_t* vgri
     C.prof.valid = false;
     for (bool& r : C.prof.recorded) r = false;
     C.prof.rounds = C.prof.tiles = C.prof.passes = 0;
+    C.prof.prop_bytes = 0;
     C.mark(PM_START);
     sort_seeds_device(C, W, H, n, P);
     C.mark(PM_SEEDS);
@@ -319,6 +320,14 @@ int idl_context_set_stream(idl_context* ctx, void* stream)
     IDL_API_END
 }
 
+int idl_context_set_schedule(idl_context* ctx, int dense_rounds)
+{
+    IDL_API_BEGIN
+    if (!ctx) invalid("context must not be NULL");
+    ctx->dense_rounds = dense_rounds;
+    IDL_API_END
+}
+
 int idl_context_synchronize(idl_context* ctx)
 {
     IDL_API_BEGIN
@@ -372,6 +381,7 @@ int idl_context_last_profile(idl_context* ctx, double* out, int n)
     v[IDL_PROF_CANVAS_PX] = (double)P.canvas_px;
     v[IDL_PROF_IMAGE_PX] = (double)P.image_px;
     v[IDL_PROF_TRIANGLES] = (double)P.n_triangles;
+    v[IDL_PROF_PROP_BYTES] = P.prop_bytes;
     for (int i = 0; i < n && i < IDL_PROF_COUNT; ++i) out[i] = v[i];
     IDL_API_END
 }

@@ -80,6 +80,7 @@ struct Profile {
     int64_t rounds = 0;           // propagation rounds launched with work
     int64_t tiles = 0;            // tiles processed over all rounds
     int64_t passes = 0;           // propagation passes (reference semantics)
+    double prop_bytes = 0;        // algorithmic HBM bytes of the propagation (8 B per cell update)
     int64_t canvas_px = 0;        // detection canvas pixels
     int64_t image_px = 0;         // output pixels
     int64_t n_triangles = 0;
@@ -105,7 +106,9 @@ struct Context {
     DevBuf counts;        // per-round list lengths
     DevBuf gsync;         // grid barrier state of the persistent propagation kernel
     DevBuf bits;          // work-list dedup bitmaps of the persistent propagation kernel
+    DevBuf big_tiles;     // tile rounds' last work list, handed to the persistent kernel
     int32_t stamp_epoch = 0;
+    int dense_rounds = 1;  // propagation schedule from scratch (propagate.cu; idl_context_set_schedule)
 
     // topology
     DevBuf hkeys, hvals;  // hash table of triangle keys -> first witness
@@ -203,6 +206,17 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, c
 // micro-tiles around them start active; otherwise every micro-tile does.
 int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos = nullptr,
                          int64_t n_new = 0);
+
+// As propagate_sparse from scratch, with the first work list built from a
+// device list of n_big tiles of big_w x big_h cells (big_tiles_x per row;
+// both multiples of the micro-tile side): all their micro-tiles.  Plane 0
+// holds the starting state, and every micro-tile outside the list must hold
+// the same state in both planes.
+int64_t propagate_sparse_from_tiles(Context& C, const Canvas& cv, const uint32_t* pos, const int32_t* big_list,
+                                    int n_big, int big_tiles_x, int big_w, int big_h);
+int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
+                              int64_t n_new, const int32_t* big_list, int n_big, int big_tiles_x, int sub_x,
+                              int sub_y);
 
 // Reserve a range of per-item stamp values for `steps` steps (propagate.cu).
 int32_t claim_stamps(Context& C, int n_items, int64_t steps);

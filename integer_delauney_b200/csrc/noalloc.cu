@@ -90,6 +90,7 @@ Context& noalloc_context(int dev)
     };
     Context& C = s.ctx;
     C.device = dev;
+    C.dense_rounds = 0;   // the persistent kernel alone: its buffers are the ones carved below
     IDL_CUDA(cudaDeviceGetAttribute(&C.num_sms, cudaDevAttrMultiProcessorCount, dev));
     take(C.xs, NA_SEEDS);
     take(C.ys, NA_SEEDS);

@@ -162,7 +162,7 @@ k_round(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pitch, i
                         const int32_t b0 = r + 1 < ROWS ? L[r + 1][0] : dn0;
                         const int32_t b1 = r + 1 < ROWS ? L[r + 1][1] : dn1;
                         const int gy = gyb + r;
-                        if (((dirty >> (2 * r)) & 1u) && o0 != OUTSIDE) {
+                        if (((dirty >> (2 * r)) & 1u) && o0 >= UNDEF) {
                             int32_t bl = o0, bd = D[r][0];
                             relax(bl, bd, left, gx, gy, pos);
                             relax(bl, bd, o1, gx, gy, pos);
@@ -174,7 +174,7 @@ k_round(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pitch, i
                                 new_chg |= 1u << (2 * r);
                             }
                         }
-                        if (((dirty >> (2 * r + 1)) & 1u) && o1 != OUTSIDE) {
+                        if (((dirty >> (2 * r + 1)) & 1u) && o1 >= UNDEF) {
                             int32_t bl = o1, bd = D[r][1];
                             relax(bl, bd, o0, gx + 1, gy, pos);
                             relax(bl, bd, right, gx + 1, gy, pos);
@@ -200,8 +200,8 @@ k_round(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pitch, i
                     int32_t left = __shfl_up_sync(FULL, o1, 1);
                     if (lane == 0) left = OUTSIDE;
                     const int gy = gyb + r;
-                    if (o0 != OUTSIDE) relax(L[r][0], D[r][0], left, gx, gy, pos);
-                    if (o1 != OUTSIDE) relax(L[r][1], D[r][1], o0, gx + 1, gy, pos);
+                    if (o0 >= UNDEF) relax(L[r][0], D[r][0], left, gx, gy, pos);
+                    if (o1 >= UNDEF) relax(L[r][1], D[r][1], o0, gx + 1, gy, pos);
                     new_chg |= (uint32_t(L[r][0] != o0) << (2 * r)) | (uint32_t(L[r][1] != o1) << (2 * r + 1));
                 }
 #pragma unroll
@@ -210,8 +210,8 @@ k_round(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pitch, i
                     int32_t right = __shfl_down_sync(FULL, o0, 1);
                     if (lane == 31) right = OUTSIDE;
                     const int gy = gyb + r;
-                    if (o0 != OUTSIDE) relax(L[r][0], D[r][0], o1, gx, gy, pos);
-                    if (o1 != OUTSIDE) relax(L[r][1], D[r][1], right, gx + 1, gy, pos);
+                    if (o0 >= UNDEF) relax(L[r][0], D[r][0], o1, gx, gy, pos);
+                    if (o1 >= UNDEF) relax(L[r][1], D[r][1], right, gx + 1, gy, pos);
                     new_chg |= (uint32_t(L[r][0] != o0) << (2 * r)) | (uint32_t(L[r][1] != o1) << (2 * r + 1));
                 }
                 par ^= 1;
@@ -225,8 +225,8 @@ k_round(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pitch, i
                         const int32_t o0 = L[r][0], o1 = L[r][1];
                         const int32_t n0 = r > 0 ? L[r - 1][0] : up0, n1 = r > 0 ? L[r - 1][1] : up1;
                         const int gy = gyb + r;
-                        if (o0 != OUTSIDE) relax(L[r][0], D[r][0], n0, gx, gy, pos);
-                        if (o1 != OUTSIDE) relax(L[r][1], D[r][1], n1, gx + 1, gy, pos);
+                        if (o0 >= UNDEF) relax(L[r][0], D[r][0], n0, gx, gy, pos);
+                        if (o1 >= UNDEF) relax(L[r][1], D[r][1], n1, gx + 1, gy, pos);
                         new_chg |= (uint32_t(L[r][0] != o0) << (2 * r)) | (uint32_t(L[r][1] != o1) << (2 * r + 1));
                     }
                 }
@@ -241,8 +241,8 @@ k_round(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pitch, i
                         const int32_t o0 = L[r][0], o1 = L[r][1];
                         const int32_t n0 = r + 1 < ROWS ? L[r + 1][0] : dn0, n1 = r + 1 < ROWS ? L[r + 1][1] : dn1;
                         const int gy = gyb + r;
-                        if (o0 != OUTSIDE) relax(L[r][0], D[r][0], n0, gx, gy, pos);
-                        if (o1 != OUTSIDE) relax(L[r][1], D[r][1], n1, gx + 1, gy, pos);
+                        if (o0 >= UNDEF) relax(L[r][0], D[r][0], n0, gx, gy, pos);
+                        if (o1 >= UNDEF) relax(L[r][1], D[r][1], n1, gx + 1, gy, pos);
                         new_chg |= (uint32_t(L[r][0] != o0) << (2 * r)) | (uint32_t(L[r][1] != o1) << (2 * r + 1));
                     }
                 }
@@ -336,7 +336,18 @@ int32_t claim_stamps(Context& C, int n_items, int64_t steps)
 int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
                   int64_t n_new)
 {
-    if (mode == IDL_MODE_REFERENCE) return propagate_sparse(C, cv, pos, seed_pos, n_new);
+    C.prof.tiles = C.prof.rounds = C.prof.passes = 0;
+    C.prof.prop_bytes = 0.0;
+    // Reference semantics.  A continued propagation (seed_pos) is local from
+    // its first pass: the sparse kernel alone.  From scratch, the first
+    // passes change most of the canvas, which the tile rounds (KSTEPS passes
+    // per HBM round trip, no per-pass bookkeeping) do best; once the changes
+    // thin out, the sparse kernel takes over the tail, whose single passes
+    // touch few cells.  C.dense_rounds sets the switch (0: sparse only,
+    // < 0: tile rounds to convergence).
+    const bool hybrid = mode == IDL_MODE_REFERENCE && !seed_pos && C.dense_rounds != 0;
+    if (mode == IDL_MODE_REFERENCE && !hybrid) return propagate_sparse(C, cv, pos, seed_pos, n_new);
+    const int64_t round_limit = hybrid && C.dense_rounds > 0 ? C.dense_rounds : -1;
     const int tiles_x = ceil_div(cv.Wd, TW), tiles_y = ceil_div(cv.Hd, TH);
     const int n_tiles = tiles_x * tiles_y;
     // Bound on rounds: far above any real run (a pass count beyond the canvas
@@ -362,8 +373,9 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, c
     const int grid = std::min(n_tiles, C.num_sms * 3);
     int64_t r = 0;
     int group = 2;
+    int32_t remaining = 0;
     for (;;) {
-        for (int g = 0; g < group && r < max_rounds; ++g, ++r) {
+        for (int g = 0; g < group && r < max_rounds && (round_limit < 0 || r < round_limit); ++g, ++r) {
             const int32_t* srcp = C.lab[r & 1].as<int32_t>();
             int32_t* dstp = C.lab[(r + 1) & 1].as<int32_t>();
             const int32_t* lin = C.tiles[r & 1].as<int32_t>();
@@ -380,30 +392,46 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, c
                     C.stamps.as<int32_t>(), stamp_next, tiles_x, tiles_y, base, last);
             IDL_LAUNCH();
         }
-        int32_t remaining = 0;
         IDL_CUDA(cudaMemcpyAsync(&remaining, counts + r, 4, cudaMemcpyDeviceToHost, C.stream));
         IDL_CUDA(cudaStreamSynchronize(C.stream));
         if (remaining == 0) break;
+        if (round_limit >= 0 && r >= round_limit) break;
         if (r >= max_rounds) throw Error(IDL_ERR_INTERNAL, "Voronoi propagation did not converge");
         group = std::min(group * 2, 8);
     }
     C.fetch_scalars();
     const int64_t lc = C.host_sc->last_change;
-    const int64_t passes = lc < 0 ? 1 : lc + 2;
+    int64_t passes = lc < 0 ? 1 : lc + 2;
     if (C.prof.enabled) {
+        // tile rounds: 8 B per inner cell (label in, label out) per processed
+        // tile and round, in micro-tile-pass equivalents for the tile count
         std::vector<int32_t> h((size_t)r + 1);
         IDL_CUDA(cudaMemcpy(h.data(), counts, h.size() * 4, cudaMemcpyDeviceToHost));
         int64_t tiles = 0, rounds = 0;
-        for (int32_t c : h) {
-            tiles += c;
-            rounds += c > 0;
+        for (int64_t i = 0; i < r; ++i) {
+            tiles += h[i];
+            rounds += h[i] > 0;
         }
-        C.prof.tiles = tiles;
+        C.prof.tiles = tiles * (TW / 8) * (TH / 8) * KSTEPS;
         C.prof.rounds = rounds;
+        C.prof.prop_bytes = (double)tiles * TW * TH * 8.0;
         C.prof.passes = passes;
         C.prof.tile_w = TW;
         C.prof.tile_h = TH;
         C.prof.steps_per_round = KSTEPS;
+    }
+    if (remaining > 0) {
+        // Hand the tail to the sparse kernel: the latest state goes to plane
+        // 0, and its first work list is every micro-tile of the tiles the
+        // next round would have run (a superset of those that can change).
+        if (r & 1) std::swap(C.lab[0], C.lab[1]);
+        C.big_tiles.ensure((size_t)remaining * 4);
+        IDL_CUDA(cudaMemcpyAsync(C.big_tiles.ptr, C.tiles[r & 1].ptr, (size_t)remaining * 4, cudaMemcpyDeviceToDevice,
+                                 C.stream));
+        const int64_t sparse = propagate_sparse_from_tiles(C, cv, pos, C.big_tiles.as<int32_t>(), remaining,
+                                                           tiles_x, TW, TH);
+        passes = sparse >= 2 ? r * KSTEPS + sparse : passes;
+        if (C.prof.enabled) C.prof.passes = passes;
     }
     return passes;
 }

@@ -136,8 +136,9 @@ __device__ __forceinline__ void advance(const int (&ids)[GROUP], int cnt, const 
         in0[k] = in1[k] = false;
         gx[k] = gy[k] = 0;
         if (k < cnt) {
-            if (lane == 0) atomicAnd(&bin[ids[k] >> 5], ~(1u << (ids[k] & 31)));
-            const int mx = ids[k] % mt_x, my = ids[k] / mt_x;
+            const int mx = ids[k] & 0xFFFF, my = ids[k] >> 16;
+            const int lin = my * mt_x + mx;
+            if (lane == 0) atomicAnd(&bin[lin >> 5], ~(1u << (lin & 31)));
             gx[k] = mx * MT + c0;
             gy[k] = my * MT + r;
             const bool row_in = gy[k] < Hd;
@@ -190,13 +191,16 @@ __device__ __forceinline__ void advance(const int (&ids)[GROUP], int cnt, const 
         if (any) {
             const unsigned left = __ballot_sync(FULL, ch0 && (lane & 3) == 0);
             const unsigned right = __ballot_sync(FULL, ch1 && (lane & 3) == 3);
-            const int mt = ids[k], mx = mt % mt_x, my = mt / mt_x;
-            int target = -1;
-            if (lane == 0) target = mt;
-            if (lane == 1 && (any & 0xFu) && my > 0) target = mt - mt_x;
-            if (lane == 2 && (any & 0xF0000000u) && my + 1 < mt_y) target = mt + mt_x;
-            if (lane == 3 && left && mx > 0) target = mt - 1;
-            if (lane == 4 && right && mx + 1 < mt_x) target = mt + 1;
+            // list entries are packed (mx | my << 16); the dedup bitmaps use
+            // the linear index my * mt_x + mx
+            const int mx = ids[k] & 0xFFFF, my = ids[k] >> 16;
+            const int mt = my * mt_x + mx;
+            int target = -1, packed = 0;
+            if (lane == 0) { target = mt; packed = ids[k]; }
+            if (lane == 1 && (any & 0xFu) && my > 0) { target = mt - mt_x; packed = ids[k] - 0x10000; }
+            if (lane == 2 && (any & 0xF0000000u) && my + 1 < mt_y) { target = mt + mt_x; packed = ids[k] + 0x10000; }
+            if (lane == 3 && left && mx > 0) { target = mt - 1; packed = ids[k] - 1; }
+            if (lane == 4 && right && mx + 1 < mt_x) { target = mt + 1; packed = ids[k] + 1; }
             bool fresh = false;
             if (target >= 0) {
                 const uint32_t bit = 1u << (target & 31);
@@ -210,7 +214,7 @@ __device__ __forceinline__ void advance(const int (&ids)[GROUP], int cnt, const 
                 base = __shfl_sync(FULL, base, 0);
                 const int rank = __popc(fb & ((1u << lane) - 1u));
                 if (base + m <= STAGE) {
-                    if (fresh) st.list[base + rank] = target;
+                    if (fresh) st.list[base + rank] = packed;
                 } else {
                     int gbase = 0;
                     if (lane == 0) {
@@ -218,7 +222,7 @@ __device__ __forceinline__ void advance(const int (&ids)[GROUP], int cnt, const 
                         gbase = atomicAdd(count_out, m);
                     }
                     gbase = __shfl_sync(FULL, gbase, 0);
-                    if (fresh) lout[gbase + rank] = target;
+                    if (fresh) lout[gbase + rank] = packed;
                 }
             }
         }
@@ -274,10 +278,13 @@ k_sparse_jacobi(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, con
     if (blockIdx.x == 0 && threadIdx.x == 0) gs->passes = t;
 }
 
-__global__ void k_iota_list(int32_t* __restrict__ list, int n, int32_t* __restrict__ count)
+// Work-list entries are micro-tile coordinates packed as mx | my << 16.
+__device__ __forceinline__ int32_t pack_mt(int mx, int my) { return mx | (my << 16); }
+
+__global__ void k_iota_list(int32_t* __restrict__ list, int n, int mt_x, int32_t* __restrict__ count)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) list[i] = i;
+    if (i < n) list[i] = pack_mt(i % mt_x, i / mt_x);
     if (i == 0) *count = n;
 }
 
@@ -297,7 +304,7 @@ __global__ void k_seed_tiles(const uint32_t* __restrict__ seed_pos, int n_new, i
         if (cx < 0 || cy < 0 || cx >= Wd || cy >= Hd) continue;
         const int mt = (cy / MT) * mt_x + cx / MT;
         const uint32_t bit = 1u << (mt & 31);
-        if (!(atomicOr(&bits[mt >> 5], bit) & bit)) list[atomicAdd(count, 1)] = mt;
+        if (!(atomicOr(&bits[mt >> 5], bit) & bit)) list[atomicAdd(count, 1)] = pack_mt(cx / MT, cy / MT);
     }
 }
 
@@ -311,8 +318,43 @@ __global__ void k_fill_bits(uint32_t* __restrict__ bits, int n_words, int n_item
 
 }  // namespace
 
+namespace {
+
+// First work list from a list of big tiles: all their micro-tiles.  Big
+// tiles are distinct, so their micro-tiles are too.
+__global__ void k_expand_tiles(const int32_t* __restrict__ big, int big_tiles_x, int sub_x, int sub_y, int mt_x,
+                               int mt_y, uint32_t* __restrict__ bits, int32_t* __restrict__ list,
+                               int32_t* __restrict__ count)
+{
+    const int32_t b = big[blockIdx.x];
+    const int bx = b % big_tiles_x, by = b / big_tiles_x;
+    for (int j = threadIdx.x; j < sub_x * sub_y; j += blockDim.x) {
+        const int mx = bx * sub_x + j % sub_x, my = by * sub_y + j / sub_x;
+        if (mx >= mt_x || my >= mt_y) continue;
+        const int mt = my * mt_x + mx;
+        atomicOr(&bits[mt >> 5], 1u << (mt & 31));
+        list[atomicAdd(count, 1)] = pack_mt(mx, my);
+    }
+}
+
+}  // namespace
+
+int64_t propagate_sparse_from_tiles(Context& C, const Canvas& cv, const uint32_t* pos, const int32_t* big_list,
+                                    int n_big, int big_tiles_x, int big_w, int big_h)
+{
+    if (big_w % MT != 0 || big_h % MT != 0) throw Error(IDL_ERR_INTERNAL, "tile sides must be micro-tile multiples");
+    return propagate_sparse_impl(C, cv, pos, nullptr, 0, big_list, n_big, big_tiles_x, big_w / MT, big_h / MT);
+}
+
 int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
                          int64_t n_new)
+{
+    return propagate_sparse_impl(C, cv, pos, seed_pos, n_new, nullptr, 0, 0, 0, 0);
+}
+
+int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
+                              int64_t n_new, const int32_t* big_list, int n_big, int big_tiles_x, int sub_x,
+                              int sub_y)
 {
     const int mt_x = ceil_div(cv.Wd, MT), mt_y = ceil_div(cv.Hd, MT);
     const int n_mt = mt_x * mt_y;
@@ -329,7 +371,13 @@ int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos, cons
     int32_t* counts = C.counts.as<int32_t>();
     int32_t* l0 = C.tiles[0].as<int32_t>();
     int32_t* l1 = C.tiles[1].as<int32_t>();
-    if (seed_pos) {
+    if (big_list) {
+        if (n_big == 0) return 0;
+        IDL_CUDA(cudaMemsetAsync(b0, 0, (size_t)n_words * 2 * 4, C.stream));
+        k_expand_tiles<<<(unsigned)n_big, 64, 0, C.stream>>>(big_list, big_tiles_x, sub_x, sub_y, mt_x, mt_y, b0,
+                                                             l0, counts);
+        IDL_LAUNCH();
+    } else if (seed_pos) {
         if (n_new == 0) return 0;
         IDL_CUDA(cudaMemsetAsync(b0, 0, (size_t)n_words * 2 * 4, C.stream));
         k_seed_tiles<<<(unsigned)((n_new + 255) / 256), 256, 0, C.stream>>>(seed_pos, (int)n_new, cv.Wd, cv.Hd,
@@ -339,7 +387,7 @@ int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos, cons
         k_fill_bits<<<(unsigned)((n_words + 255) / 256), 256, 0, C.stream>>>(b0, n_words, n_mt);
         IDL_LAUNCH();
         IDL_CUDA(cudaMemsetAsync(b1, 0, (size_t)n_words * 4, C.stream));
-        k_iota_list<<<(unsigned)((n_mt + 255) / 256), 256, 0, C.stream>>>(l0, n_mt, counts);
+        k_iota_list<<<(unsigned)((n_mt + 255) / 256), 256, 0, C.stream>>>(l0, n_mt, mt_x, counts);
         IDL_LAUNCH();
     }
     C.gsync.ensure(sizeof(GridSync));
@@ -376,9 +424,11 @@ int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos, cons
         IDL_CUDA(cudaMemcpy(hc.data(), counts, hc.size() * 4, cudaMemcpyDeviceToHost));
         int64_t tiles = 0;
         for (int32_t c : hc) tiles += c;
-        C.prof.tiles = tiles;
-        C.prof.rounds = passes;
+        // accumulated: a hybrid run has counted its tile rounds already
+        C.prof.tiles += tiles;
+        C.prof.rounds += passes;
         C.prof.passes = passes;
+        C.prof.prop_bytes += (double)tiles * MT * MT * 8.0;   // label in, label out per cell
         C.prof.tile_w = MT;
         C.prof.tile_h = MT;
         C.prof.steps_per_round = 1;

@@ -233,3 +233,25 @@ def test_triangulate_4096_200k_vs_reference_cuda(kind):
     assert len(tm) == len(r_tris)
     np.testing.assert_array_equal(np.sort(tm, axis=1), np.sort(r_tris[:, 2:5], axis=1))
     np.testing.assert_array_equal(grid, r_grid)
+
+
+@pytest.mark.parametrize("kind", ["uniform", "clustered"])
+def test_propagation_schedules_agree(kind):
+    """Tile rounds for the first passes and the persistent kernel for the
+    tail, switched at any round, give the Jacobi fixed point bit for bit."""
+    from integer_delauney_b200 import _capi, autotune
+    W, H = 700, 500
+    seeds = random_seeds(W, H, 3000, 31) if kind == "uniform" else clustered_seeds(W, H, 3000, 31, blobs=5,
+                                                                                     sigma=15.0)
+    s = oracle.sort_seeds(seeds, W, H)
+    o_tris, o_grid, _ = oracle.triangulate(W, H, s, 16)
+    ctx = _capi.context_for(0)
+    try:
+        for sched in (0, 1, 2, 5, -1):
+            ctx.set_schedule(sched)
+            tm, grid = cu.triangulate(W, H, seeds, 16)
+            np.testing.assert_array_equal(grid, o_grid, err_msg=f"schedule {sched}")
+            np.testing.assert_array_equal(_tris_array(tm), o_tris, err_msg=f"schedule {sched}")
+        assert autotune.tune(W, H, seeds, 16, candidates=(0, 1, 2), repeats=1, context=ctx) in (0, 1, 2)
+    finally:
+        ctx.set_schedule(1)
