@@ -66,9 +66,10 @@ def reduce_max(value: float, world: int) -> float:
     return float(t.item())
 
 
-# dram__bytes_read.sum + dram__bytes_write.sum of one launch of the dominant
-# kernel on this workload, from an ncu --set full capture (uniform seeds)
-TRAFFIC_PER_LAUNCH = {"propagate_ms": 1186.0e6 + 723.4e6}
+# dram__bytes_read.sum + dram__bytes_write.sum of the dominant stage's kernels
+# for one step of this workload (uniform seeds), from ncu --set full captures:
+# the tile round (69.1 + 29.0 MB) and the persistent kernel's tail (357.3 + 223.2 MB)
+TRAFFIC_PER_LAUNCH = {"propagate_ms": 69.1e6 + 29.0e6 + 357.3e6 + 223.2e6}
 
 
 class ClockSampler:
