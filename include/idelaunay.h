@@ -254,7 +254,10 @@ IDL_API int idl_voronoi_batch(idl_context* ctx, int n_images, const int32_t* dim
  * Propagation.  IDL_MODE_REFERENCE continues the Jacobi iteration from the
  * previous fixed point after writing the new seeds, the reference's own
  * incremental trajectory (src/cuda/delaunay_voronoi.cu:12-108), ties going to
- * the higher insertion id.
+ * the higher insertion id.  IDL_MODE_EXACT recomputes the exact diagram of
+ * the whole seed set (ties to the higher (x, y) rank) and detects on rank
+ * labels, so after every insert the object equals idl_triangulate of all its
+ * seeds in exact mode, bit for bit, whatever the insertion history.
  *
  * Triangles.  Detection runs on the insertion-id grid (the block rule's
  * lowest-id tie-break sees insertion ids, as in the reference) and triangles

@@ -179,7 +179,6 @@ struct StageTimer {
 int64_t run_triangulate(Context& C, int W, int H, int64_t n, const int32_t* vgrid_host_or_dev, bool vgrid_on_host,
                         int P, int mode, float* timings, int64_t* passes_out, Canvas& cv_out)
 {
-    if (mode == IDL_MODE_EXACT) invalid("voronoi_mode 'exact' is not available in this build");
     const Canvas cv = make_canvas(W + 2 * P, H + 2 * P);
     cv_out = cv;
     C.prof.valid = false;
@@ -193,8 +192,12 @@ int64_t run_triangulate(Context& C, int W, int H, int64_t n, const int32_t* vgri
     StageTimer T(C, timings != nullptr);
     int64_t passes = 0;
     if (P > 0 || !vgrid_host_or_dev) {
-        init_labels(C, cv, C.pos.as<uint32_t>(), n);
-        passes = propagate(C, mode, cv, C.pos.as<uint32_t>());
+        if (mode == IDL_MODE_EXACT) {
+            propagate_exact(C, cv, C.pos.as<uint32_t>(), n);
+        } else {
+            init_labels(C, cv, C.pos.as<uint32_t>(), n);
+            passes = propagate(C, mode, cv, C.pos.as<uint32_t>());
+        }
     } else {
         const size_t gbytes = (size_t)W * H * 2 * sizeof(int32_t);
         C.vgrid.ensure(gbytes);
@@ -395,14 +398,18 @@ int idl_voronoi(idl_context* ctx, int width, int height, const int32_t* seeds_xy
     check_dims(width, height, n_seeds);
     check_seed_count(n_seeds);
     if (!seeds_xy) invalid("seeds must not be NULL");
-    if (mode == IDL_MODE_EXACT) invalid("voronoi_mode 'exact' is not available in this build");
     DeviceGuard g(ctx->device);
     Context& C = *ctx;
     const Canvas cv = make_canvas(width, height);
     upload_seeds(C, seeds_xy, n_seeds, cudaMemcpyHostToDevice);
     sort_seeds_device(C, width, height, n_seeds, 0);
-    init_labels(C, cv, C.pos.as<uint32_t>(), n_seeds);
-    const int64_t passes = propagate(C, mode, cv, C.pos.as<uint32_t>());
+    int64_t passes = 0;
+    if (mode == IDL_MODE_EXACT) {
+        propagate_exact(C, cv, C.pos.as<uint32_t>(), n_seeds);
+    } else {
+        init_labels(C, cv, C.pos.as<uint32_t>(), n_seeds);
+        passes = propagate(C, mode, cv, C.pos.as<uint32_t>());
+    }
     const size_t bytes = (size_t)width * height * 2 * sizeof(int32_t);
     C.outgrid.ensure(bytes);
     dim3 gr(ceil_div(width, 256), height);

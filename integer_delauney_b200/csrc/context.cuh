@@ -218,6 +218,11 @@ int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos,
                               int64_t n_new, const int32_t* big_list, int n_big, int big_tiles_x, int sub_x,
                               int sub_y);
 
+// Stage (a), exact semantics (exact.cu): nearest seed, ties to the higher id,
+// for the n (x, y)-sorted seeds `pos` of the canvas; labels into C.lab[0]
+// (C.lab[1] is scratch).
+void propagate_exact(Context& C, const Canvas& cv, const uint32_t* pos, int64_t n);
+
 // Reserve a range of per-item stamp values for `steps` steps (propagate.cu).
 int32_t claim_stamps(Context& C, int n_items, int64_t steps);
 

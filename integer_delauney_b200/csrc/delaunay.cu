@@ -67,6 +67,7 @@ struct DelaunayState {
 
     // grow-only scratch
     DevBuf stage, edge_keys, edge_tmp, sort_tmp, num_sel, scores, score_keys, score_sorted, qbuf, qout, batch, verr;
+    DevBuf spos;          // exact mode: canvas positions of the seeds in (x, y) order
 
     // host mirrors (insertion order, image coordinates)
     std::vector<int32_t> hx, hy;
@@ -125,7 +126,7 @@ struct DelaunayState {
         planes = tgrid = seedmem = nullptr;
         pixmem = nullptr;
         DevBuf* all[] = {&stage, &edge_keys, &edge_tmp, &sort_tmp, &num_sel, &scores, &score_keys, &score_sorted,
-                         &qbuf, &qout, &batch, &verr};
+                         &qbuf, &qout, &batch, &verr, &spos};
         for (DevBuf* b : all) b->release();
     }
     ~DelaunayState()
@@ -214,6 +215,19 @@ __global__ void k_adopt(const int32_t* __restrict__ atlas, int apitch, int ox, i
         a[o + c] = v;
         b[o + c] = v;
     }
+}
+
+// Exact mode: plane a holds (x, y)-rank labels; move them to plane b and
+// put the insertion ids into plane a.
+__global__ void k_exact_planes(int32_t* __restrict__ a, int32_t* __restrict__ b, int pitch, int Wd,
+                               const int32_t* __restrict__ inv)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= Wd) return;
+    const size_t o = (size_t)y * pitch + x;
+    const int32_t l = a[o];
+    b[o] = l;
+    a[o] = l >= 0 ? __ldg(&inv[l]) : l;
 }
 
 __global__ void k_split(const int32_t* __restrict__ xy, int64_t k, int32_t* __restrict__ x, int32_t* __restrict__ y)
@@ -498,7 +512,11 @@ void ensure_topology(DelaunayState& D, float* timings)
             for (auto& ev : e) IDL_CUDA(cudaEventCreate(&ev));
         try {
             if (timings) IDL_CUDA(cudaEventRecord(e[0], C.stream));
-            detect_triangles(C, D.canvas(), D.planes, D.pos, D.N, D.P, timings ? e[1] : nullptr, D.rank);
+            if (D.mode == IDL_MODE_EXACT)   // plane 1 holds the labels as (x, y) ranks
+                detect_triangles(C, D.canvas(), D.planes + (size_t)D.pitch * D.Hd, D.spos.as<uint32_t>(), D.N,
+                                 D.P, timings ? e[1] : nullptr, nullptr);
+            else
+                detect_triangles(C, D.canvas(), D.planes, D.pos, D.N, D.P, timings ? e[1] : nullptr, D.rank);
             if (timings) IDL_CUDA(cudaEventRecord(e[2], C.stream));
             C.fetch_scalars();
             D.n_tri = C.host_sc->n_triangles;
@@ -667,8 +685,8 @@ int idl_delaunay_create(int device, int width, int height, int64_t max_seeds, in
     *out = nullptr;
     if (width <= 0 || height <= 0 || max_seeds <= 0) invalid("dimensions and max_seeds must be positive");
     if (max_seeds > MAX_SEEDS) invalid("max_seeds exceeds the 2097151 seeds this build can number");
-    if (mode != IDL_MODE_REFERENCE)
-        invalid("the incremental Delaunay supports voronoi_mode 'reference' only in this build");
+    if (mode != IDL_MODE_REFERENCE && mode != IDL_MODE_EXACT)
+        invalid("the incremental Delaunay supports voronoi_mode 'reference' and 'exact' in this build");
     int dev = device;
     if (dev < 0) IDL_CUDA(cudaGetDevice(&dev));
     DeviceGuard g(dev);
@@ -848,10 +866,25 @@ int idl_delaunay_insert_ordered(idl_delaunay* d, const int32_t* xy, int64_t k, c
     d->pending = true;
 
     Timer T(C, timings != nullptr);
-    k_put_seeds<<<gk, 256, 0, C.stream>>>(d->planes, d->planes + (size_t)d->pitch * d->Hd, d->pitch, d->pos + n0,
-                                          k, n0);
-    IDL_LAUNCH();
-    const int64_t passes = propagate(C, d->mode, d->canvas(), d->pos, d->pos + n0, k);
+    int64_t passes = 0;
+    if (d->mode == IDL_MODE_EXACT) {
+        // history-independent: the exact diagram of the whole seed set, in
+        // (x, y) ranks (plane 1, which detection reads) and as insertion ids
+        // (plane 0, which every other reader expects)
+        ensure_rank(*d);
+        d->spos.ensure((size_t)d->N * 4);
+        k_pack_pos<<<blocks(d->N), 256, 0, C.stream>>>(d->sx, d->sy, d->N, 0, d->spos.as<uint32_t>());
+        IDL_LAUNCH();
+        propagate_exact(C, d->canvas(), d->spos.as<uint32_t>(), d->N);
+        k_exact_planes<<<dim3(blocks(d->Wd), (unsigned)d->Hd), 256, 0, C.stream>>>(
+            d->planes, d->planes + (size_t)d->pitch * d->Hd, d->pitch, d->Wd, d->inv);
+        IDL_LAUNCH();
+    } else {
+        k_put_seeds<<<gk, 256, 0, C.stream>>>(d->planes, d->planes + (size_t)d->pitch * d->Hd, d->pitch,
+                                              d->pos + n0, k, n0);
+        IDL_LAUNCH();
+        passes = propagate(C, d->mode, d->canvas(), d->pos, d->pos + n0, k);
+    }
     const float bfs = T.stop();
     if (timings) {
         timings[IDL_T_BFS_MS] = bfs;
@@ -873,6 +906,7 @@ int idl_delaunay_adopt(idl_delaunay* d, idl_context* src, int image)
     if (bi.W != d->W || bi.H != d->H || bi.P != d->P)
         invalid("the batch image's size or border padding differs from the object's");
     if (d->N != 0) invalid("adopt needs an empty object (reset it first)");
+    if (d->mode != IDL_MODE_REFERENCE) invalid("adopt takes labels of reference semantics only");
     if (bi.n > d->max_seeds) invalid("insert would exceed max_seeds capacity");
     DeviceGuard g(d->device);
     Context& C = d->ctx();

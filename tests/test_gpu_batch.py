@@ -37,7 +37,7 @@ def _check_against_oracle(W, H, seeds, P, mode):
 # stage (a)
 # ---------------------------------------------------------------------------
 
-@pytest.mark.parametrize("mode", ["reference", "numpy"])
+@pytest.mark.parametrize("mode", ["reference", "numpy", "exact"])
 @pytest.mark.parametrize("W,H,n,seed", [
     (5, 5, 1, 0), (5, 1, 2, 1), (1, 5, 2, 2), (10, 10, 3, 3), (33, 17, 20, 4), (64, 64, 20, 5),
     (128, 128, 400, 6), (100, 70, 300, 7), (257, 129, 700, 8), (512, 512, 2000, 0),
@@ -55,7 +55,7 @@ def test_voronoi_clustered_matches_oracle():
     W = H = 384
     seeds = clustered_seeds(W, H, 3000, seed=3, blobs=6, sigma=12.0)
     s = oracle.sort_seeds(seeds, W, H)
-    for mode in ("reference", "numpy"):
+    for mode in ("reference", "numpy", "exact"):
         want, _ = oracle.voronoi(mode, W, H, s)
         got = cu.Voronoi().compute(W, H, seeds, voronoi_mode=mode)
         np.testing.assert_array_equal(got, want)
@@ -70,13 +70,16 @@ def test_numpy_mode_equals_reference_numpy_golden(golden_dir):
         seeds = z[f"{name}__seeds"]
         got = cu.Voronoi().compute(W, H, seeds, voronoi_mode="numpy")
         np.testing.assert_array_equal(got, z[f"{name}__grid"], err_msg=name)
+        # on these inputs the NumPy reference also meets the exact contract
+        got = cu.Voronoi().compute(W, H, seeds, voronoi_mode="exact")
+        np.testing.assert_array_equal(got, z[f"{name}__grid"], err_msg=name + " (exact)")
 
 
 # ---------------------------------------------------------------------------
 # stages (a) + (b) + (d)
 # ---------------------------------------------------------------------------
 
-@pytest.mark.parametrize("mode", ["reference", "numpy"])
+@pytest.mark.parametrize("mode", ["reference", "numpy", "exact"])
 @pytest.mark.parametrize("W,H,n,seed,P", [
     (10, 10, 3, 1, 0), (30, 30, 4, 2, 16), (64, 64, 20, 3, 0), (64, 64, 40, 4, 16), (96, 80, 120, 5, 8),
     (200, 150, 600, 6, 16), (300, 200, 2000, 7, 32), (128, 96, 300, 8, 1),
@@ -255,3 +258,23 @@ def test_propagation_schedules_agree(kind):
         assert autotune.tune(W, H, seeds, 16, candidates=(0, 1, 2), repeats=1, context=ctx) in (0, 1, 2)
     finally:
         ctx.set_schedule(1)
+
+
+@pytest.mark.parametrize("kind", ["uniform", "clustered"])
+def test_exact_mode_at_scale(kind):
+    """Exact mode on a large canvas, dense and clustered (long scans through
+    empty space), against the oracle's bucketed nearest-seed search; the
+    result does not depend on the order the seeds are given in."""
+    W, H = 1024, 768
+    seeds = random_seeds(W, H, 8000, 41) if kind == "uniform" else clustered_seeds(W, H, 8000, 41, blobs=6,
+                                                                                    sigma=25.0)
+    s = oracle.sort_seeds(seeds, W, H)
+    want, _ = oracle.voronoi("exact", W, H, s)
+    got = cu.Voronoi().compute(W, H, seeds, voronoi_mode="exact")
+    np.testing.assert_array_equal(got, want)
+    perm = np.random.default_rng(0).permutation(len(seeds))
+    np.testing.assert_array_equal(cu.Voronoi().compute(W, H, seeds[perm], voronoi_mode="exact"), want)
+    o_tris, o_grid, _ = oracle.triangulate(W, H, s, 16, "exact")
+    tm, grid = cu.triangulate(W, H, seeds, 16, voronoi_mode="exact")
+    np.testing.assert_array_equal(grid, o_grid)
+    np.testing.assert_array_equal(_tris_array(tm), o_tris)

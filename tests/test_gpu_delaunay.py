@@ -450,3 +450,25 @@ def test_rejected_insert_changes_nothing(cu):
     np.testing.assert_array_equal(m0, m1)
     np.testing.assert_array_equal(g0, g1)
     np.testing.assert_array_equal(d.locate(s[:50]), g0[s[:50, 1], s[:50, 0], 2])
+
+
+@pytest.mark.parametrize("sizes,P", [((300, 200, 1, 499), 16), ((1000,), 0), ((100,) * 10, 16)])
+def test_exact_mode_equals_full_recompute_after_every_insert(cu, sizes, P):
+    """In exact mode the incremental object is history-independent: after
+    each insert it equals the exact batch triangulation of all its seeds."""
+    W, H = 320, 240
+    seeds = uniform(W, H, sum(sizes), seed=len(sizes) + P)
+    d = cu.Delaunay(W, H, 2000, P, voronoi_mode="exact")
+    done = 0
+    for k in sizes:
+        m, g = d.insert(seeds[done:done + k])
+        done += k
+        m1, g1 = cu.triangulate(W, H, seeds[:done], P, voronoi_mode="exact")
+        assert m == m1
+        np.testing.assert_array_equal(g, g1)
+        np.testing.assert_array_equal(d.get_voronoi_grid(), g1[:, :, :2])
+    s = oracle.sort_seeds(seeds, W, H)
+    o_tris, o_grid, _ = oracle.triangulate(W, H, s, P, "exact")
+    np.testing.assert_array_equal(g, o_grid)
+    np.testing.assert_array_equal(np.array([m[t] for t in range(len(m))]).reshape(-1, 5), o_tris)
+    np.testing.assert_array_equal(d.sorted_rank[d.get_triangles()], o_tris[:, 2:5])
