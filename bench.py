@@ -14,6 +14,12 @@ Workload (one step = one image through the whole pipeline):
          seeds in pinned host memory: host->device copy of the seeds, all
          stages, device->host copy of the (H, W, 3) grid and the triangles.
 
+Also on the same line: the same step in exact semantics ("exact"); the
+incremental workload (2048 x 2048, 50 000 seeds + 100 inserts of 1 000) in
+reference and exact semantics; the batched workload (512 images in one call
+against the per-image loop); and the serving workload (Poisson request stream
+against the server, and a fixed prefix against the plain serial loop).
+
 Multi-GPU (torchrun): every rank triangulates its own image per step (replicas,
 no collective on the data path); the time is the max over ranks.
 
@@ -190,7 +196,7 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def incremental_case(cu, torch, rank):
+def incremental_case(cu, torch, rank, mode="reference"):
     """2048 x 2048, 50 000 uniform seeds, then 100 insert batches of 1 000
     new seeds (30 % in a 256 x 256 hotspot).  Each batch is timed through the
     public call a caller makes: insert() (propagate, topology, assignment and
@@ -204,7 +210,7 @@ def incremental_case(cu, torch, rank):
     cap = len(base) + sum(len(b) for b in batches)
 
     def fresh():
-        d = cu.Delaunay(Wi, Hi, cap, PADDING)
+        d = cu.Delaunay(Wi, Hi, cap, PADDING, voronoi_mode=mode)
         d.insert_deferred(base)
         d.finalise()
         return d
@@ -231,7 +237,7 @@ def incremental_case(cu, torch, rank):
     t_def = time.perf_counter() - t0
     lat_ms = sorted(x * 1e3 for x in lat)
     return {"workload": f"Delaunay {Wi}x{Hi}, {len(base)} uniform seeds + {len(batches)} x {len(batches[0])} "
-                        f"(30% in a 256x256 hotspot), P={PADDING}, reference mode",
+                        f"(30% in a 256x256 hotspot), P={PADDING}, {mode} mode",
             "insert_ms_mean": t_all * 1e3 / len(batches), "insert_ms_p50": lat_ms[len(lat_ms) // 2],
             "insert_ms_p99": lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))],
             "insert_mpix_s": Wi * Hi * len(batches) / t_all / 1e6,
@@ -560,6 +566,28 @@ def run_ours(args, rank, world):
     e2e = world * W * H * e_steps / (ms_e / 1e3) / 1e6
 
     inc = incremental_case(cu, torch, rank)
+    inc_exact = incremental_case(cu, torch, rank, "exact")
+
+    # the same 4096 x 4096 step in exact semantics (nearest seed, ties to the
+    # higher id; history-independent), device-resident like the headline
+    d_seeds = torch.from_numpy(seeds_u).cuda()
+    d_out = torch.empty((H, W, 3), dtype=torch.int32, device="cuda")
+
+    def exact_step():
+        _capi.check(lib.idl_triangulate_device(ctx.handle, W, H, d_seeds.data_ptr(), d_seeds.shape[0], PADDING,
+                                               _capi.MODE_EXACT, d_out.data_ptr(), None))
+    for _ in range(args.warmup):
+        exact_step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        exact_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_x = reduce_max(e0.elapsed_time(e1), world) / args.steps
+    exact = {"workload": f"triangulate {W}x{H}, {N_SEEDS} uniform seeds, P={PADDING}, voronoi_mode=exact",
+             "ms_per_step": ms_x, "mpix_s": world * W * H / (ms_x / 1e3) / 1e6}
     bat = batched_case(torch, lib, ctx, stream, rank)
     srv = serving_case(torch, rank, args.serve_seconds) if args.serve_seconds > 0 else None
 
@@ -592,6 +620,8 @@ def run_ours(args, rank, world):
                 "h2d_bytes_per_step": int(seeds_u.nbytes),
                 "d2h_bytes_per_step": int(W * H * 12 + n_tri * 20)},
         "incremental": inc,
+        "incremental_exact": inc_exact,
+        "exact": exact,
         "batched": bat,
         "serving": srv,
         "gpu_launches": int(launches),
