@@ -31,6 +31,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes
+import gc
 import json
 import os
 import statistics
@@ -220,6 +221,8 @@ def incremental_case(cu, torch, rank, mode="reference"):
         d.insert(b, as_arrays=True)
     d = fresh()
     torch.cuda.synchronize()
+    gc.collect()
+    gc.disable()                             # no collector pauses inside the timed loops
     lat = []
     t_all = time.perf_counter()
     for b in batches:
@@ -235,6 +238,7 @@ def incremental_case(cu, torch, rank, mode="reference"):
         d2.insert_deferred(b)
     d2.finalise(as_arrays=True)
     t_def = time.perf_counter() - t0
+    gc.enable()
     lat_ms = sorted(x * 1e3 for x in lat)
     return {"workload": f"Delaunay {Wi}x{Hi}, {len(base)} uniform seeds + {len(batches)} x {len(batches[0])} "
                         f"(30% in a 256x256 hotspot), P={PADDING}, {mode} mode",
@@ -324,6 +328,17 @@ def serving_case(torch, rank, seconds, slots=8):
         pre = {i: uniform(prm[0], prm[1], prm[2], seed=prm[3]) for i, (t, kind, prm) in enumerate(tr)
                if kind == "new"}
         srv = Server(budget_bytes=budget, slots=slots, border_padding=PADDING)
+        # warm-up, untimed: new diagrams from another stretch of the same
+        # distribution until the budget is full, so the timed replay sees the
+        # steady state (objects recycled, not allocated)
+        warm = [prm for _, kind, prm in serving_trace(rate, 4.0, seed=rank + 1000) if kind == "new"]
+        for W_, H_, n_, ps_ in warm:
+            srv.submit_new(W_, H_, uniform(W_, H_, n_, seed=ps_))
+        srv.drain()
+        warm_stats = dict(srv.stats)
+        gc.collect()
+        gc.freeze()                          # no collector pauses inside the timed replay
+        gc.disable()
         info = {}          # diagram id -> (W, H, sorted keys)
         ids = []           # the same ids, for uniform picks
         futs = []
@@ -372,6 +387,8 @@ def serving_case(torch, rank, seconds, slots=8):
                 failed_submit += 1
         srv.drain()
         t_end = time.perf_counter()
+        gc.enable()
+        gc.unfreeze()
         lat, n_new, n_ins, errors = [], 0, 0, 0
         for f in futs:
             e = f.exception()
@@ -382,7 +399,7 @@ def serving_case(torch, rank, seconds, slots=8):
             lat.append(r.latency * 1e3)
             n_new += r.kind == "new"
             n_ins += r.kind == "insert"
-        stats = dict(srv.stats)
+        stats = {k: v - warm_stats.get(k, 0) for k, v in srv.stats.items()}
         mem = srv.memory_used()
         srv.close()
         lat.sort()
@@ -394,7 +411,7 @@ def serving_case(torch, rank, seconds, slots=8):
                 "errors": errors, "not_submitted": failed_submit, "wall_s": t_end - t0,
                 "throughput_req_s": len(lat) / (t_end - t0), "p50_ms": pct(0.5), "p99_ms": pct(0.99),
                 "max_ms": lat[-1] if lat else None, "submit_lag_max_s": late, "memory_bytes_end": mem,
-                "objects": stats}
+                "warmup_new_diagrams": len(warm), "objects": stats}
 
     # (2) saturated: the same fixed requests through the server and the plain loop
     reqs, meta = [], []

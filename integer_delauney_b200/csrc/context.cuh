@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 #include <memory>
 #include <string>
@@ -25,15 +26,23 @@ struct DevBuf {
     template <class T>
     T* as() const { return static_cast<T*>(ptr); }
 
-    // Grow to at least `need` bytes (contents are not preserved).
+    // Grow to at least `need` bytes (contents are not preserved).  A first
+    // allocation is exact; a regrowth takes at least 1.5x the old size, so
+    // buffers sized by a count that creeps up call after call (triangle rows
+    // of a growing diagram, the scratch of requests of mixed sizes) are
+    // reallocated O(log) times, not every call -- a cudaFree waits for the
+    // whole device.
     void ensure(size_t need)
     {
         if (need <= bytes) return;
         if (fixed) invalid("request exceeds the fixed workspace of this entry point");
+        size_t grow = need;
+        if (bytes) grow = std::max(need, bytes + bytes / 2);
+        grow = (grow + 255) / 256 * 256;
         release();
         if (need == 0) return;
-        IDL_CUDA(cudaMalloc(&ptr, need));
-        bytes = need;
+        IDL_CUDA(cudaMalloc(&ptr, grow));
+        bytes = grow;
     }
     void borrow(void* p, size_t n)
     {

@@ -45,7 +45,7 @@ from . import _capi
 
 SIZE_CLASS = 128            # object canvases are rounded up to multiples of this
 SEED_HEADROOM = 50_000      # seed capacity beyond the initial set, for inserts
-GROUP_MAX = 32              # new diagrams propagated together in one launch, at most
+GROUP_MAX = 16              # new diagrams propagated together in one launch, at most
 
 
 @dataclass
