@@ -22,7 +22,7 @@ void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 size_t Context::workspace_bytes() const
 {
     const DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
-                           &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &big_tiles, &hkeys, &hvals, &ukeys, &uvals, &cnt,
+                           &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &big_tiles, &exact_dy, &hkeys, &hvals, &ukeys, &uvals, &cnt,
                            &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded, &batch_img, &batch_seed_img,
                            &batch_rows, &batch_sid, &batch_stats, &batch_bad, &scalars};
     size_t s = 0;
@@ -39,7 +39,7 @@ void Context::fetch_scalars()
 Context::~Context()
 {
     DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
-                     &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &big_tiles, &hkeys, &hvals, &ukeys, &uvals, &cnt,
+                     &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &big_tiles, &exact_dy, &hkeys, &hvals, &ukeys, &uvals, &cnt,
                      &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded, &batch_img, &batch_seed_img,
                            &batch_rows, &batch_sid, &batch_stats, &batch_bad, &scalars};
     for (DevBuf* b : all) b->release();

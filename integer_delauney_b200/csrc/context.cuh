@@ -116,6 +116,7 @@ struct Context {
     DevBuf gsync;         // grid barrier state of the persistent propagation kernel
     DevBuf bits;          // work-list dedup bitmaps of the persistent propagation kernel
     DevBuf big_tiles;     // tile rounds' last work list, handed to the persistent kernel
+    DevBuf exact_dy;      // exact mode: row distance to each cell's column-nearest seed
     int32_t stamp_epoch = 0;
     int dense_rounds = 1;  // propagation schedule from scratch (propagate.cu; idl_context_set_schedule)
 

@@ -7,7 +7,7 @@
 //
 // Separable and exact, in two data-parallel phases over the canvas:
 //   1. column phase: each cell finds the nearest seed in its own column
-//      (binary search in the column's run of the (x, y)-sorted seeds; a tie
+//      (a walk down the column's run of the (x, y)-sorted seeds; a tie
 //      between the seed above and the one below goes to the lower one, whose
 //      y -- and so id -- is larger);
 //   2. row phase: each cell scans the columns outward, k = 0, 1, 2, ..., taking
@@ -41,43 +41,61 @@ __global__ void k_col_start(const uint32_t* __restrict__ pos, int64_t n, int Wd,
     cs[c] = (int32_t)lo;
 }
 
-// Phase 1: nearest seed of each cell within its column (or UNDEF).
+// Phase 1: nearest seed of each cell within its column (or UNDEF), and its
+// row distance |dy| (so the row phase reads distances instead of gathering
+// seed positions).  One thread walks one column through a band of CHUNK rows,
+// advancing through the column's seeds as the row advances (one binary search
+// per band), so a warp of adjacent columns writes each row coalesced.
+constexpr int CHUNK = 64;
+
 __global__ void k_col_nearest(const uint32_t* __restrict__ pos, const int32_t* __restrict__ cs, int Wd, int Hd,
-                              int pitch, int32_t* __restrict__ col)
+                              int pitch, int32_t* __restrict__ col, int32_t* __restrict__ coldy)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= Wd) return;
+    const int y0 = blockIdx.y * CHUNK, y1 = min(Hd, y0 + CHUNK);
     const int32_t lo = __ldg(&cs[x]), hi = __ldg(&cs[x + 1]);
-    int32_t best = UNDEF;
-    if (lo < hi) {
-        int32_t a = lo, b = hi;   // first seed of the column with y >= this row
-        while (a < b) {
-            const int32_t m = (a + b) >> 1;
-            if ((int)pos_y(__ldg(&pos[m])) < y) a = m + 1;
-            else b = m;
+    if (lo == hi) {
+        for (int y = y0; y < y1; ++y) {
+            col[(size_t)y * pitch + x] = UNDEF;
+            coldy[(size_t)y * pitch + x] = 0;
         }
-        if (a == hi) best = hi - 1;
-        else if (a == lo) best = lo;
-        else {
-            const int below = (int)pos_y(__ldg(&pos[a])) - y, above = y - (int)pos_y(__ldg(&pos[a - 1]));
-            best = below <= above ? a : a - 1;   // tie: the larger y, the higher id
-        }
+        return;
     }
-    col[(size_t)y * pitch + x] = best;
+    int32_t a = lo, b = hi;   // first seed of the column with y >= y0
+    while (a < b) {
+        const int32_t m = (a + b) >> 1;
+        if ((int)pos_y(__ldg(&pos[m])) < y0) a = m + 1;
+        else b = m;
+    }
+    int next_y = a < hi ? (int)pos_y(__ldg(&pos[a])) : 0x7FFFFFFF;     // seed at or below
+    int prev_y = a > lo ? (int)pos_y(__ldg(&pos[a - 1])) : -0x3FFFFFFF; // seed above
+    for (int y = y0; y < y1; ++y) {
+        while (next_y < y) {   // the seed below was passed: it becomes the one above
+            prev_y = next_y;
+            ++a;
+            next_y = a < hi ? (int)pos_y(__ldg(&pos[a])) : 0x7FFFFFFF;
+        }
+        const int below = next_y - y, above = y - prev_y;   // tie: the larger y, the higher id
+        const bool take_below = a < hi && (a == lo || below <= above);
+        col[(size_t)y * pitch + x] = take_below ? a : a - 1;
+        coldy[(size_t)y * pitch + x] = take_below ? below : above;
+    }
 }
 
 // Phase 2: best column candidate of the row, scanning outward.
-__global__ void k_row_nearest(const int32_t* __restrict__ col, const uint32_t* __restrict__ pos, int Wd, int Hd,
+__global__ void k_row_nearest(const int32_t* __restrict__ col, const int32_t* __restrict__ coldy, int Wd, int Hd,
                               int pitch, int32_t* __restrict__ lab)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= Wd) return;
     const int32_t* row = col + (size_t)y * pitch;
+    const int32_t* rdy = coldy + (size_t)y * pitch;
     int32_t bl = row[x];
     long long bd = 0x7FFFFFFFFFFFFFFFll;
     if (bl >= 0) {
-        const int dy = y - (int)pos_y(__ldg(&pos[bl]));
-        bd = (long long)dy * dy;
+        const long long dy = rdy[x];
+        bd = dy * dy;
     }
     for (int k = 1;; ++k) {
         const long long kk = (long long)k * k;
@@ -88,8 +106,8 @@ __global__ void k_row_nearest(const int32_t* __restrict__ col, const uint32_t* _
             if (xx < 0 || xx >= Wd) continue;
             const int32_t l = row[xx];
             if (l < 0) continue;
-            const int dy = y - (int)pos_y(__ldg(&pos[l]));
-            const long long d = kk + (long long)dy * dy;
+            const long long dy = rdy[xx];
+            const long long d = kk + dy * dy;
             if (d < bd || (d == bd && l > bl)) {
                 bd = d;
                 bl = l;
@@ -111,16 +129,19 @@ void propagate_exact(Context& C, const Canvas& cv, const uint32_t* pos, int64_t 
     k_col_start<<<(unsigned)((cv.Wd + 1 + 255) / 256), 256, 0, C.stream>>>(pos, n, cv.Wd, cs);
     IDL_LAUNCH();
     const dim3 g((unsigned)ceil_div(cv.Wd, 256), (unsigned)cv.Hd);
-    k_col_nearest<<<g, 256, 0, C.stream>>>(pos, cs, cv.Wd, cv.Hd, cv.pitch, C.lab[1].as<int32_t>());
+    C.exact_dy.ensure(plane);
+    const dim3 gc((unsigned)ceil_div(cv.Wd, 128), (unsigned)ceil_div(cv.Hd, CHUNK));
+    k_col_nearest<<<gc, 128, 0, C.stream>>>(pos, cs, cv.Wd, cv.Hd, cv.pitch, C.lab[1].as<int32_t>(),
+                                            C.exact_dy.as<int32_t>());
     IDL_LAUNCH();
-    k_row_nearest<<<g, 256, 0, C.stream>>>(C.lab[1].as<int32_t>(), pos, cv.Wd, cv.Hd, cv.pitch,
-                                           C.lab[0].as<int32_t>());
+    k_row_nearest<<<g, 256, 0, C.stream>>>(C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>(), cv.Wd, cv.Hd,
+                                           cv.pitch, C.lab[0].as<int32_t>());
     IDL_LAUNCH();
     if (C.prof.enabled) {
         C.prof.passes = 0;
         C.prof.rounds = 2;
         C.prof.tiles = 0;
-        C.prof.prop_bytes = (double)cv.Wd * cv.Hd * 12.0;   // column labels out, in, final labels out
+        C.prof.prop_bytes = (double)cv.Wd * cv.Hd * 20.0;   // column labels and distances out and in, labels out
         C.prof.tile_w = C.prof.tile_h = 0;
         C.prof.steps_per_round = 0;
     }
