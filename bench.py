@@ -311,7 +311,9 @@ def serving_case(torch, rank, seconds, slots=8):
     latency p50/p99 from arrival to result, also at 500 req/s (a rate the
     server sustains, for a p99 without queueing); (2) throughput with every request
     of a fixed 2 000-request prefix submitted at once, server against the
-    plain serial loop over the same requests."""
+    plain serial loop over the same requests.  The server is the native loop
+    (idl_server_*): submission copies the seeds and returns, latency runs from
+    the scheduled arrival to the worker's completion timestamp."""
     from integer_delauney_b200.serving import Server, run_serial
     from integer_delauney_b200.workloads import fresh_points, serving_trace, uniform
     budget = 40 << 30
@@ -340,14 +342,15 @@ def serving_case(torch, rank, seconds, slots=8):
         gc.freeze()                          # no collector pauses inside the timed replay
         gc.disable()
         info = {}          # diagram id -> (W, H, sorted keys)
+        dims = {}          # diagram id -> (W, H), kept after eviction
         ids = []           # the same ids, for uniform picks
         futs = []
         failed_submit = 0
         late = 0.0
-        t0 = time.perf_counter() + 0.05
+        t0 = time.monotonic() + 0.05         # the server's clock: arrivals are passed in on it
         for i, (t, kind, prm) in enumerate(tr):
             at = t0 + t
-            now = time.perf_counter()
+            now = time.monotonic()
             if at > now:
                 time.sleep(at - now)
             else:
@@ -357,16 +360,17 @@ def serving_case(torch, rank, seconds, slots=8):
                 pts = pre.pop(i)
                 f = srv.submit_new(W, H, pts, arrival=at)
                 info[f.diagram_id] = (W, H, keys_of(W, pts))
+                dims[f.diagram_id] = (W, H)
                 ids.append(f.diagram_id)
                 futs.append(f)
                 continue
             n, pick, ps = prm
-            if i % 256 == 0:                    # drop the diagrams the server has evicted
+            if i % 32 == 0:                     # drop the diagrams the server has evicted
                 live = set(srv.resident())
                 ids = [d for d in ids if d in live]
                 for d in [d for d in info if d not in live]:
                     del info[d]
-            for attempt in range(4):            # a pick may have been evicted meanwhile
+            for attempt in range(8):            # a pick may have been evicted meanwhile
                 if not ids:
                     break
                 j = int(pick * len(ids)) if attempt == 0 else int(np.random.default_rng(ps + attempt).integers(
@@ -386,10 +390,12 @@ def serving_case(torch, rank, seconds, slots=8):
             else:
                 failed_submit += 1
         srv.drain()
-        t_end = time.perf_counter()
+        t_end = time.monotonic()
         gc.enable()
         gc.unfreeze()
         lat, n_new, n_ins, errors = [], 0, 0, 0
+        parts = {"new": ([], []), "insert": ([], [])}     # kind -> (queue wait ms, service ms)
+        slow = []
         for f in futs:
             e = f.exception()
             if e is not None:
@@ -399,19 +405,30 @@ def serving_case(torch, rank, seconds, slots=8):
             lat.append(r.latency * 1e3)
             n_new += r.kind == "new"
             n_ins += r.kind == "insert"
+            parts[r.kind][0].append((r.start - r.arrival) * 1e3)
+            parts[r.kind][1].append((r.done - r.start) * 1e3)
+            slow.append((r.latency * 1e3, r.kind, dims.get(r.diagram_id), r.n_seeds,
+                         (r.start - r.arrival) * 1e3, (r.done - r.start) * 1e3, r.arrival - t0))
         stats = {k: v - warm_stats.get(k, 0) for k, v in srv.stats.items()}
         mem = srv.memory_used()
         srv.close()
         lat.sort()
 
-        def pct(q):
-            return lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None
+        def pct(q, v=lat):
+            v = sorted(v)
+            return v[min(len(v) - 1, int(q * len(v)))] if v else None
+
+        breakdown = {k: {"wait_p50_ms": pct(0.5, w), "wait_p99_ms": pct(0.99, w), "service_p50_ms": pct(0.5, sv),
+                         "service_p99_ms": pct(0.99, sv)} for k, (w, sv) in parts.items()}
+        slow.sort(key=lambda x: -x[0])
+        slowest = [{"ms": round(a, 2), "kind": b, "dims": c, "seeds": d, "wait_ms": round(e, 2),
+                    "service_ms": round(f_, 2), "arrival_s": round(g, 3)} for a, b, c, d, e, f_, g in slow[:6]]
 
         return {"rate_req_s": rate, "requests": len(tr), "completed": len(lat), "new": n_new, "inserts": n_ins,
                 "errors": errors, "not_submitted": failed_submit, "wall_s": t_end - t0,
                 "throughput_req_s": len(lat) / (t_end - t0), "p50_ms": pct(0.5), "p99_ms": pct(0.99),
                 "max_ms": lat[-1] if lat else None, "submit_lag_max_s": late, "memory_bytes_end": mem,
-                "warmup_new_diagrams": len(warm), "objects": stats}
+                "warmup_new_diagrams": len(warm), "objects": stats, "breakdown": breakdown, "slowest": slowest}
 
     # (2) saturated: the same fixed requests through the server and the plain loop
     reqs, meta = [], []

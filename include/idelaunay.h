@@ -46,6 +46,8 @@ extern "C" {
 #define IDL_ERR_CUDA 2     /* CUDA runtime failure (RuntimeError) */
 #define IDL_ERR_STATE 3    /* call not valid in the object's state (RuntimeError) */
 #define IDL_ERR_INTERNAL 4 /* internal invariant broken (RuntimeError) */
+#define IDL_ERR_BUDGET 5   /* server: request does not fit the memory budget (MemoryError) */
+#define IDL_ERR_NOT_RESIDENT 6 /* server: the diagram is not resident (KeyError) */
 
 /* ---- Voronoi propagation semantics --------------------------------- */
 /* Synchronous Jacobi fixed point of src/cuda/voronoi.cu:32-53,100-113: the
@@ -404,6 +406,82 @@ IDL_API int idl_delaunay_voronoi(idl_delaunay* d, int32_t* grid_out);
 
 /* Object properties (IDL_DI_* slots; src/cuda/delaunay.cuh:249-254). */
 IDL_API int idl_delaunay_info(idl_delaunay* d, int64_t* info_out, int count);
+
+/* ---- Serving: a native request loop over resident diagrams ----------
+ * No counterpart in the reference (one caller, one image per call).  A server
+ * keeps incremental objects resident on one device and runs two kinds of
+ * request from any number of client threads:
+ *   new    -- triangulate W x H (1..4096 each) from a seed set, in (x, y)
+ *             order, and keep the diagram: its grid and triangles equal
+ *             idl_triangulate of the same input bit for bit;
+ *   insert -- add seeds to a resident diagram (idl_delaunay_insert order);
+ * on `slots` worker threads, each with its own stream and scratch.  Queued
+ * new diagrams are propagated together, several per launch
+ * (idl_voronoi_batch + idl_delaunay_adopt).  Requests whose diagram is busy
+ * or whose memory does not fit yet are passed over, not waited on.  Every
+ * resident diagram, pooled object and slot workspace is charged to
+ * budget_bytes; the least recently used idle diagram is retired into a reuse
+ * pool (idl_delaunay_reset) when memory runs short.  A request whose
+ * footprint can never fit fails with IDL_ERR_BUDGET.  A diagram's requests
+ * run in submission order, one at a time, so results do not depend on the
+ * mix.  Timestamps are nanoseconds of idl_server_clock_ns (CLOCK_MONOTONIC). */
+typedef struct idl_server idl_server;
+
+#define IDL_SR_STATUS 0      /* the request's status (also returned by idl_server_wait) */
+#define IDL_SR_KIND 1        /* 0 new, 1 insert */
+#define IDL_SR_DIAGRAM 2
+#define IDL_SR_SEEDS 3       /* the diagram's seed count after the request */
+#define IDL_SR_TRIANGLES 4
+#define IDL_SR_ARRIVAL_NS 5
+#define IDL_SR_START_NS 6
+#define IDL_SR_DONE_NS 7
+#define IDL_SR_COUNT 8
+
+#define IDL_SI_USED_BYTES 0
+#define IDL_SI_BUDGET_BYTES 1
+#define IDL_SI_RESIDENT 2
+#define IDL_SI_POOLED 3
+#define IDL_SI_QUEUED 4
+#define IDL_SI_GROUPS 5          /* grouped propagation launches */
+#define IDL_SI_GROUPED 6         /* new diagrams they served */
+#define IDL_SI_NEW_OBJECTS 7
+#define IDL_SI_REUSED_OBJECTS 8
+#define IDL_SI_EVICTED 9
+#define IDL_SI_FREED_OBJECTS 10
+#define IDL_SI_COUNT 11
+
+IDL_API int64_t idl_server_clock_ns(void);
+/* device < 0: the current device.  mode: IDL_MODE_REFERENCE (grouped
+ * propagation) or IDL_MODE_EXACT.  Errors: slots outside [1, 64], budget <= 0,
+ * another mode -> IDL_ERR_INVALID. */
+IDL_API int idl_server_create(int device, int64_t budget_bytes, int slots, int border_padding, int mode,
+                              idl_server** out);
+/* Runs what is queued, stops the workers and frees every object. */
+IDL_API int idl_server_destroy(idl_server* s);
+/* Queue a new diagram (seeds copied; n <= 200000).  fetch != 0: grid_out
+ * (H x W x 3 int32, host) receives the finalised grid and the triangles are
+ * kept for idl_server_wait; it must stay valid until then.  arrival_ns <= 0:
+ * now.  *diagram_out can take inserts at once. */
+IDL_API int idl_server_submit_new(idl_server* s, int width, int height, const int32_t* seeds_xy, int64_t n,
+                                  int fetch, int32_t* grid_out, int64_t arrival_ns, int64_t* request_out,
+                                  int64_t* diagram_out);
+/* Queue an insert; IDL_ERR_NOT_RESIDENT if the diagram is not resident. */
+IDL_API int idl_server_submit_insert(idl_server* s, int64_t diagram, const int32_t* seeds_xy, int64_t n, int fetch,
+                                     int32_t* grid_out, int64_t arrival_ns, int64_t* request_out);
+/* Wait for a request (timeout_s < 0: without limit) and collect it: its
+ * result row (IDL_SR_COUNT int64) and, for a fetched request, its triangles
+ * (5 int32 each, as idl_delaunay_triangles ids = 0) if tris_out is given --
+ * capacity too small -> IDL_ERR_INVALID and the request stays uncollected.
+ * Returns the request's own status; collecting twice -> IDL_ERR_INVALID. */
+IDL_API int idl_server_wait(idl_server* s, int64_t request, double timeout_s, int64_t* result_out,
+                            int32_t* tris_out, int64_t capacity);
+/* Wait until every queued request has run. */
+IDL_API int idl_server_drain(idl_server* s);
+/* Retire an idle diagram now, keeping its object for reuse. */
+IDL_API int idl_server_recycle(idl_server* s, int64_t diagram, int* recycled_out);
+IDL_API int idl_server_info(idl_server* s, int64_t* info_out, int count);
+/* Ids of resident diagrams (and of those whose creation is queued). */
+IDL_API int idl_server_resident(idl_server* s, int64_t* ids_out, int64_t capacity, int64_t* n_out);
 
 #ifdef __cplusplus
 }

@@ -21,6 +21,8 @@ IDL_ERR_INVALID = 1
 IDL_ERR_CUDA = 2
 IDL_ERR_STATE = 3
 IDL_ERR_INTERNAL = 4
+IDL_ERR_BUDGET = 5
+IDL_ERR_NOT_RESIDENT = 6
 
 MODE_REFERENCE = 0
 MODE_NUMPY = 1
@@ -82,7 +84,23 @@ SIGNATURES = {
     "idl_delaunay_sorted_rank": (_i32, [_vp, _vp]),
     "idl_delaunay_voronoi": (_i32, [_vp, _vp]),
     "idl_delaunay_info": (_i32, [_vp, _pi64, _i32]),
+    # serving
+    "idl_server_clock_ns": (_i64, []),
+    "idl_server_create": (_i32, [_i32, _i64, _i32, _i32, _i32, ctypes.POINTER(_vp)]),
+    "idl_server_destroy": (_i32, [_vp]),
+    "idl_server_submit_new": (_i32, [_vp, _i32, _i32, _vp, _i64, _i32, _vp, _i64, _pi64, _pi64]),
+    "idl_server_submit_insert": (_i32, [_vp, _i64, _vp, _i64, _i32, _vp, _i64, _pi64]),
+    "idl_server_wait": (_i32, [_vp, _i64, ctypes.c_double, _pi64, _vp, _i64]),
+    "idl_server_drain": (_i32, [_vp]),
+    "idl_server_recycle": (_i32, [_vp, _i64, ctypes.POINTER(_i32)]),
+    "idl_server_info": (_i32, [_vp, _pi64, _i32]),
+    "idl_server_resident": (_i32, [_vp, _pi64, _i64, _pi64]),
 }
+
+# idl_server_wait result row and idl_server_info slots
+(SR_STATUS, SR_KIND, SR_DIAGRAM, SR_SEEDS, SR_TRIANGLES, SR_ARRIVAL_NS, SR_START_NS, SR_DONE_NS, SR_COUNT) = range(9)
+(SI_USED_BYTES, SI_BUDGET_BYTES, SI_RESIDENT, SI_POOLED, SI_QUEUED, SI_GROUPS, SI_GROUPED, SI_NEW_OBJECTS,
+ SI_REUSED_OBJECTS, SI_EVICTED, SI_FREED_OBJECTS, SI_COUNT) = range(12)
 
 # idl_delaunay_info slots
 (DI_SEED_COUNT, DI_WIDTH, DI_HEIGHT, DI_BORDER_PADDING, DI_HAS_PENDING, DI_GENERATION, DI_MAX_SEEDS, DI_MODE,
@@ -127,6 +145,10 @@ def check(status: int) -> None:
     msg = last_error()
     if status == IDL_ERR_INVALID:
         raise ValueError(msg)
+    if status == IDL_ERR_BUDGET:
+        raise MemoryError(msg)
+    if status == IDL_ERR_NOT_RESIDENT:
+        raise KeyError(msg)
     raise RuntimeError(msg)
 
 

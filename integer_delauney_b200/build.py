@@ -35,7 +35,7 @@ def sources() -> list[str]:
 
 
 def headers() -> list[str]:
-    return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh")) +
+    return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh")) + glob.glob(os.path.join(HERE, "csrc", "*.h")) +
                   glob.glob(os.path.join(ROOT, "include", "*.h")))
 
 

@@ -21,12 +21,8 @@ void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 size_t Context::workspace_bytes() const
 {
-    const DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
-                           &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &big_tiles, &exact_dy, &hkeys, &hvals, &ukeys, &uvals, &cnt,
-                           &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded, &batch_img, &batch_seed_img,
-                           &batch_rows, &batch_sid, &batch_stats, &batch_bad, &scalars};
     size_t s = 0;
-    for (const DevBuf* b : all) s += b->bytes;
+    const_cast<Context*>(this)->each_buf([&](DevBuf& b) { s += b.bytes; });
     return s;
 }
 
@@ -38,11 +34,10 @@ void Context::fetch_scalars()
 
 Context::~Context()
 {
-    DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
-                     &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &big_tiles, &exact_dy, &hkeys, &hvals, &ukeys, &uvals, &cnt,
-                     &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded, &batch_img, &batch_seed_img,
-                           &batch_rows, &batch_sid, &batch_stats, &batch_bad, &scalars};
-    for (DevBuf* b : all) b->release();
+    bool ordered = false;
+    each_buf([&](DevBuf& b) { ordered |= b.async; });
+    if (ordered) cudaDeviceSynchronize();   // stream-ordered buffers may still be in use
+    each_buf([](DevBuf& b) { b.release(); });
     if (host_sc && !host_sc_borrowed) cudaFreeHost(host_sc);
     for (auto& e : timing.ev)
         if (e) cudaEventDestroy(e);
@@ -319,7 +314,14 @@ int idl_context_set_stream(idl_context* ctx, void* stream)
 {
     IDL_API_BEGIN
     if (!ctx) invalid("context must not be NULL");
-    ctx->stream = static_cast<cudaStream_t>(stream);
+    const cudaStream_t next = static_cast<cudaStream_t>(stream);
+    // Workspace growth is freed in the order of the context's stream: finish
+    // the old stream's work before later frees are ordered on the new one.
+    if (next != ctx->stream) {
+        DeviceGuard g(ctx->device);
+        IDL_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    ctx->stream = next;
     IDL_API_END
 }
 

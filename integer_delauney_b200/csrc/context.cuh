@@ -22,6 +22,12 @@ struct DevBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
     bool fixed = false;   // borrowed memory of fixed size: never allocated or freed here
+    bool async = false;   // ptr came from the stream-ordered allocator
+    // When set, growth is stream-ordered on the owner's current stream
+    // (cudaMallocAsync / cudaFreeAsync): it waits for nothing but the work
+    // already queued there, instead of for the whole device as cudaFree does
+    // -- which matters when many streams share a device (a server).
+    const cudaStream_t* stream = nullptr;
 
     template <class T>
     T* as() const { return static_cast<T*>(ptr); }
@@ -30,8 +36,7 @@ struct DevBuf {
     // allocation is exact; a regrowth takes at least 1.5x the old size, so
     // buffers sized by a count that creeps up call after call (triangle rows
     // of a growing diagram, the scratch of requests of mixed sizes) are
-    // reallocated O(log) times, not every call -- a cudaFree waits for the
-    // whole device.
+    // reallocated O(log) times, not every call.
     void ensure(size_t need)
     {
         if (need <= bytes) return;
@@ -39,9 +44,14 @@ struct DevBuf {
         size_t grow = need;
         if (bytes) grow = std::max(need, bytes + bytes / 2);
         grow = (grow + 255) / 256 * 256;
-        release();
+        drop();
         if (need == 0) return;
-        IDL_CUDA(cudaMalloc(&ptr, grow));
+        if (stream) {
+            IDL_CUDA(cudaMallocAsync(&ptr, grow, *stream));
+            async = true;
+        } else {
+            IDL_CUDA(cudaMalloc(&ptr, grow));
+        }
         bytes = grow;
     }
     void borrow(void* p, size_t n)
@@ -49,12 +59,28 @@ struct DevBuf {
         ptr = p;
         bytes = n;
         fixed = true;
+        async = false;
     }
+    // Free in stream order behind the work queued on the owner's stream.
+    void drop() noexcept
+    {
+        if (ptr && !fixed) {
+            if (async) cudaFreeAsync(ptr, *stream);
+            else cudaFree(ptr);
+        }
+        ptr = nullptr;
+        bytes = 0;
+        async = false;
+    }
+    // Free at teardown.  cudaFree does not wait for stream-ordered memory:
+    // the owner synchronises first when any of its buffers is (see
+    // Context::~Context).
     void release() noexcept
     {
         if (ptr && !fixed) cudaFree(ptr);
         ptr = nullptr;
         bytes = 0;
+        async = false;
     }
 };
 
@@ -160,6 +186,23 @@ struct Context {
         IDL_CUDA(cudaEventRecord(prof.ev[m], stream));
         prof.recorded[m] = true;
     }
+
+    // Every workspace buffer, for set-up, sizing and teardown.
+    template <class F>
+    void each_buf(F&& f)
+    {
+        DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
+                         &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &big_tiles, &exact_dy, &hkeys,
+                         &hvals, &ukeys, &uvals, &cnt, &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded,
+                         &batch_img, &batch_seed_img, &batch_rows, &batch_sid, &batch_stats, &batch_bad, &scalars};
+        for (DevBuf* b : all) f(*b);
+    }
+    Context()
+    {
+        each_buf([this](DevBuf& b) { b.stream = &stream; });
+    }
+    Context(const Context&) = delete;
+    Context& operator=(const Context&) = delete;
 
     Scalars* sc() const { return scalars.as<Scalars>(); }
     size_t workspace_bytes() const;

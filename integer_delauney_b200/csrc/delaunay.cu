@@ -31,7 +31,6 @@
 #include <algorithm>
 #include <cmath>
 #include <mutex>
-#include <unordered_set>
 #include <vector>
 
 namespace idl {
@@ -65,9 +64,21 @@ struct DelaunayState {
     int32_t *pix_tid = nullptr, *pix_sid = nullptr;
     uint8_t* pix_out = nullptr;
 
-    // grow-only scratch
+    // grow-only scratch, stream-ordered on the object's stream
     DevBuf stage, edge_keys, edge_tmp, sort_tmp, num_sel, scores, score_keys, score_sorted, qbuf, qout, batch, verr;
     DevBuf spos;          // exact mode: canvas positions of the seeds in (x, y) order
+
+    template <class F>
+    void each_scratch(F&& f)
+    {
+        DevBuf* all[] = {&stage, &edge_keys, &edge_tmp, &sort_tmp, &num_sel, &scores, &score_keys, &score_sorted,
+                         &qbuf, &qout, &batch, &verr, &spos};
+        for (DevBuf* b : all) f(*b);
+    }
+    DelaunayState()
+    {
+        each_scratch([this](DevBuf& b) { b.stream = &stream; });
+    }
 
     // host mirrors (insertion order, image coordinates)
     std::vector<int32_t> hx, hy;
@@ -87,7 +98,13 @@ struct DelaunayState {
     {
         Context& c = ws ? *ws : own;
         if (!ws && !own.scalars.ptr) ensure_scalars(own);
-        c.stream = stream;
+        if (c.stream != stream) {
+            // the context's last user queued work on another stream: let it
+            // finish before this object's work (and stream-ordered frees of
+            // the scratch) are ordered on ours
+            if (ws) IDL_CUDA(cudaStreamSynchronize(c.stream));
+            c.stream = stream;
+        }
         if (bound != &c) {
             unbind();
             saved[0] = c.lab[0];
@@ -125,9 +142,7 @@ struct DelaunayState {
         if (pixmem) cudaFreeAsync(pixmem, stream);
         planes = tgrid = seedmem = nullptr;
         pixmem = nullptr;
-        DevBuf* all[] = {&stage, &edge_keys, &edge_tmp, &sort_tmp, &num_sel, &scores, &score_keys, &score_sorted,
-                         &qbuf, &qout, &batch, &verr, &spos};
-        for (DevBuf* b : all) b->release();
+        each_scratch([](DevBuf& b) { b.drop(); });
     }
     ~DelaunayState()
     {
@@ -756,7 +771,14 @@ int idl_delaunay_set_stream(idl_delaunay* d, void* stream)
     IDL_API_BEGIN
     check_handle(d);
     const Unbinder unbind_on_exit{d};
-    d->stream = static_cast<cudaStream_t>(stream);
+    const cudaStream_t next = static_cast<cudaStream_t>(stream);
+    // Scratch is freed in the order of the object's stream: finish the old
+    // stream's work before later frees are ordered on the new one.
+    if (next != d->stream) {
+        DeviceGuard g(d->device);
+        IDL_CUDA(cudaStreamSynchronize(d->stream));
+    }
+    d->stream = next;
     IDL_API_END
 }
 

@@ -45,6 +45,34 @@ def test_status_codes_map_to_reference_exception_types():
     for st in (_capi.IDL_ERR_CUDA, _capi.IDL_ERR_STATE, _capi.IDL_ERR_INTERNAL):
         with pytest.raises(RuntimeError):
             _capi.check(st)
+    with pytest.raises(MemoryError):            # serving: never fits the memory budget
+        _capi.check(_capi.IDL_ERR_BUDGET)
+    with pytest.raises(KeyError):               # serving: diagram not resident
+        _capi.check(_capi.IDL_ERR_NOT_RESIDENT)
+
+
+def test_server_clock_is_the_monotonic_clock():
+    """Request timestamps are comparable with time.monotonic() (arrival
+    times a client passes in)."""
+    import time
+    from integer_delauney_b200 import _capi
+    lib = _capi.load()
+    a = time.monotonic_ns()
+    b = lib.idl_server_clock_ns()
+    c = time.monotonic_ns()
+    assert a - 1_000_000 <= b <= c + 1_000_000
+
+
+def test_server_rejects_bad_arguments_before_touching_a_device():
+    import ctypes
+    from integer_delauney_b200 import _capi
+    lib = _capi.load()
+    h = ctypes.c_void_p()
+    for slots, budget, mode in ((0, 1 << 30, 0), (65, 1 << 30, 0), (1, 0, 0), (1, 1 << 30, 1)):
+        assert lib.idl_server_create(0, budget, slots, 16, mode, ctypes.byref(h)) == _capi.IDL_ERR_INVALID
+        assert h.value is None
+    assert lib.idl_server_destroy(None) == _capi.IDL_OK
+    assert lib.idl_server_drain(None) == _capi.IDL_ERR_INVALID
 
 
 def test_mode_names():

@@ -138,3 +138,88 @@ def test_adopt_from_a_batch_equals_ordered_insert(cu):
         np.testing.assert_array_equal(a.finalise(as_arrays=True)[1], b.finalise(as_arrays=True)[1])
     with pytest.raises(ValueError):
         cu.Delaunay(7, 7, 10, 16)._adopt(ctx, 0)          # size differs from the batch image
+
+
+def test_exact_mode_server_equals_exact_triangulate(cu):
+    from integer_delauney_b200.serving import Server
+    news, inserts = _requests(4, n_new=5)
+    with Server(budget_bytes=40 << 30, slots=3, border_padding=16, mode="exact") as srv:
+        fn = [srv.submit_new(W, H, pts, fetch=True) for W, H, pts in news]
+        fi = [(i, srv.submit_insert(fn[i].diagram_id, add, fetch=True)) for i, add in inserts]
+        got_new = [f.result(timeout=120) for f in fn]
+        got_ins = [(i, f.result(timeout=120)) for i, f in fi]
+    for (W, H, pts), r in zip(news, got_new):
+        v, g = cu.triangulate(W, H, pts, 16, voronoi_mode="exact", as_arrays=True)
+        np.testing.assert_array_equal(v, r.verts)
+        np.testing.assert_array_equal(g, r.grid)
+    # exact mode is history-independent: after an insert the diagram equals
+    # the exact triangulation of all its seeds, in insertion order of ids
+    for (i, add), (_, r) in zip(inserts, got_ins):
+        W, H, pts = news[i]
+        d = cu.Delaunay(W, H, len(pts) + 5000, 16, voronoi_mode="exact")
+        d.insert_deferred(pts, order="xy")
+        for j, more in inserts:
+            if j == i:
+                d.insert_deferred(more)
+                if more is add:
+                    break
+        v, g = d.finalise(as_arrays=True)
+        np.testing.assert_array_equal(g, r.grid)
+        np.testing.assert_array_equal(v, r.verts)
+
+
+def test_many_client_threads(cu):
+    """Clients submitting from several threads at once get the same results
+    as one client submitting in order."""
+    import threading
+    from integer_delauney_b200.serving import Server
+    news, _ = _requests(5, n_new=24)
+    expect = [cu.triangulate(W, H, pts, 16, as_arrays=True) for W, H, pts in news]
+    out = [None] * len(news)
+    with Server(budget_bytes=40 << 30, slots=4, border_padding=16) as srv:
+        def client(k):
+            for i in range(k, len(news), 4):
+                W, H, pts = news[i]
+                out[i] = srv.submit_new(W, H, pts, fetch=True).result(timeout=120)
+        ts = [threading.Thread(target=client, args=(k,)) for k in range(4)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        info = srv.info()
+    for (v, g), r in zip(expect, out):
+        np.testing.assert_array_equal(v, r.verts)
+        np.testing.assert_array_equal(g, r.grid)
+        assert r.arrival <= r.start <= r.done
+    assert info["queued"] == 0 and info["resident"] == len(news)
+
+
+def test_collect_once_recycle_and_timestamps(cu):
+    import ctypes
+    import time
+    from integer_delauney_b200 import _capi
+    from integer_delauney_b200.serving import Server
+    lib = _capi.load()
+    with Server(budget_bytes=40 << 30, slots=2, border_padding=16) as srv:
+        at = time.monotonic() - 0.5                  # arrived half a second ago
+        f = srv.submit_new(300, 200, uniform(300, 200, 400, seed=3), arrival=at)
+        r = f.result(timeout=60)
+        assert abs(r.arrival - at) < 1e-6 and r.latency >= 0.5
+        assert r.n_seeds == 400 and r.n_triangles > 0 and r.kind == "new"
+        row = (ctypes.c_int64 * _capi.SR_COUNT)()
+        assert lib.idl_server_wait(srv._handle(), f.request_id, 1.0, row, None, 0) == _capi.IDL_ERR_INVALID
+        g = srv.submit_insert(f.diagram_id, [(5, 7)])
+        assert g.result(timeout=60).n_seeds == 401
+        assert srv.recycle(f.diagram_id)
+        assert f.diagram_id not in srv.resident()
+        with pytest.raises(KeyError):
+            srv.submit_insert(f.diagram_id, [(9, 9)])
+        # the pooled object is reused by the next diagram of its size class
+        h = srv.submit_new(310, 190, uniform(310, 190, 300, seed=4))
+        h.result(timeout=60)
+        assert srv.stats["reused_objects"] >= 1
+        # a request with a seed out of bounds fails alone
+        bad = srv.submit_new(100, 100, [(5, 5), (100, 3)])
+        with pytest.raises(ValueError):
+            bad.result(timeout=60)
+        assert bad.diagram_id not in srv.resident()
