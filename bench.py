@@ -471,6 +471,7 @@ def serving_case(torch, rank, seconds, slots=8):
         srv.close()
         return dt, ok
 
+    saturate(slots)                         # warm-up, untimed: the device memory pool grows once
     t_srv, srv_ok = saturate(slots)
     t_one, one_ok = saturate(1)
     torch.cuda.synchronize()

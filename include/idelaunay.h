@@ -327,7 +327,8 @@ IDL_API int idl_delaunay_insert_ordered(idl_delaunay* d, const int32_t* seeds_xy
                                         int order, float* timings_out);
 
 /* Make an empty object (fresh or reset, same width, height and padding) hold
- * image `image` of the last idl_voronoi_batch on `src`: its converged labels
+ * image `image` of the last idl_voronoi_batch or idl_triangulate_batch[_device]
+ * on `src`: its converged labels
  * and its seeds, numbered in (x, y) order -- the state idl_delaunay_insert_
  * ordered(order = 1) of the same seeds would reach, bit for bit, without a
  * propagation of its own.  No counterpart in the reference.  Waits for the
@@ -456,6 +457,9 @@ IDL_API int64_t idl_server_clock_ns(void);
  * another mode -> IDL_ERR_INVALID. */
 IDL_API int idl_server_create(int device, int64_t budget_bytes, int slots, int border_padding, int mode,
                               idl_server** out);
+/* Propagation schedule of every slot's contexts (idl_context_set_schedule),
+ * before the first request; IDL_ERR_STATE after it. */
+IDL_API int idl_server_set_schedule(idl_server* s, int dense_rounds);
 /* Runs what is queued, stops the workers and frees every object. */
 IDL_API int idl_server_destroy(idl_server* s);
 /* Queue a new diagram (seeds copied; n <= 200000).  fetch != 0: grid_out

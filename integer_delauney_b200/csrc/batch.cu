@@ -272,11 +272,16 @@ Plan make_plan(int n_images, const int32_t* dims, const int64_t* counts, int P)
 
 // The pipeline; seeds already in C.seeds_in.  Leaves per-image grids in
 // d_out (or C.outgrid) and image-local triangle rows in C.tris.
-// What idl_delaunay_adopt needs of the last labels-only batch on a context.
-struct LabelsOnly {
+// What idl_delaunay_adopt (and batch_fetch) need of the last batch on a
+// context: the atlas layout, and after the whole pipeline, where each
+// image's grid and triangle rows are.
+struct BatchPlan {
     std::vector<BImg> imgs;
     int P = 0, pitch = 0;
     int64_t n_seeds = 0;
+    bool full = false;               // grids in `grids`, image-local rows in C.tris
+    const int32_t* grids = nullptr;  // device, n_px x 3 int32
+    std::vector<int64_t> tri_off;    // n_images + 1 row offsets
 };
 
 void run_batch(Context& C, const Plan& pl, int P, int n_images, int32_t* d_out, int64_t* tri_counts,
@@ -358,15 +363,13 @@ void run_batch(Context& C, const Plan& pl, int P, int n_images, int32_t* d_out, 
     mark(1);
     propagate(C, IDL_MODE_REFERENCE, cv, C.pos.as<uint32_t>());
     mark(2);
-    if (labels_only) {
-        auto lo = std::make_shared<LabelsOnly>();
-        lo->imgs = pl.imgs;
-        lo->P = P;
-        lo->pitch = cv.pitch;
-        lo->n_seeds = n;
-        C.batch_plan = lo;
-        return;
-    }
+    auto bp = std::make_shared<BatchPlan>();
+    bp->imgs = pl.imgs;
+    bp->P = P;
+    bp->pitch = cv.pitch;
+    bp->n_seeds = n;
+    C.batch_plan = bp;
+    if (labels_only) return;
     detect_triangles(C, cv, C.lab[0].as<int32_t>(), C.pos.as<uint32_t>(), n, 0, timings ? ev[3] : nullptr);
 
     // per-image counts, offsets and windows; raster; compose
@@ -404,6 +407,10 @@ void run_batch(Context& C, const Plan& pl, int P, int n_images, int32_t* d_out, 
     C.have_result = true;
     if (tri_counts)
         for (int i = 0; i < n_images; ++i) tri_counts[i] = hc[i];
+    bp->tri_off.assign((size_t)n_images + 1, 0);
+    for (int i = 0; i < n_images; ++i) bp->tri_off[i + 1] = bp->tri_off[i] + hc[i];
+    bp->grids = out;
+    bp->full = true;
     if (timings) {
         float a = 0, b = 0, c = 0, d = 0;
         IDL_CUDA(cudaEventElapsedTime(&a, ev[1], ev[2]));
@@ -421,9 +428,40 @@ void run_batch(Context& C, const Plan& pl, int P, int n_images, int32_t* d_out, 
 
 }  // namespace
 
+void triangulate_batch_keep(Context& C, int n_images, const int32_t* dims, const int64_t* counts,
+                            const int32_t* seeds_xy, int P, int64_t* tri_counts)
+{
+    if (!dims || !counts) invalid("dims and seed_counts must not be NULL");
+    const Plan pl = make_plan(n_images, dims, counts, P);
+    if (!seeds_xy) invalid("seeds must not be NULL");
+    DeviceGuard g(C.device);
+    C.have_result = false;
+    C.batch_plan.reset();
+    C.seeds_in.ensure((size_t)pl.n_seeds * 8);
+    IDL_CUDA(cudaMemcpyAsync(C.seeds_in.ptr, seeds_xy, (size_t)pl.n_seeds * 8, cudaMemcpyHostToDevice, C.stream));
+    run_batch(C, pl, P, n_images, nullptr, tri_counts, nullptr);
+}
+
+void batch_fetch(Context& C, int k, int32_t* grid_out, int32_t* tris_out, int64_t capacity)
+{
+    const auto* bp = static_cast<const BatchPlan*>(C.batch_plan.get());
+    if (!bp || !bp->full || k < 0 || k >= (int)bp->imgs.size())
+        throw Error(IDL_ERR_STATE, "no triangulated batch image " + std::to_string(k) + " on this context");
+    const BImg& m = bp->imgs[k];
+    if (grid_out)
+        IDL_CUDA(cudaMemcpyAsync(grid_out, bp->grids + (size_t)m.px_off * 3, (size_t)m.W * m.H * 12,
+                                 cudaMemcpyDeviceToHost, C.stream));
+    const int64_t rows = bp->tri_off[k + 1] - bp->tri_off[k];
+    if (tris_out && rows) {
+        if (capacity < rows * 5) invalid("triangle buffer too small");
+        IDL_CUDA(cudaMemcpyAsync(tris_out, C.tris.as<int32_t>() + bp->tri_off[k] * 5, (size_t)rows * 20,
+                                 cudaMemcpyDeviceToHost, C.stream));
+    }
+}
+
 bool batch_image(const Context& C, int k, BatchImage& out)
 {
-    const auto* lo = static_cast<const LabelsOnly*>(C.batch_plan.get());
+    const auto* lo = static_cast<const BatchPlan*>(C.batch_plan.get());
     if (!lo || k < 0 || k >= (int)lo->imgs.size()) return false;
     const BImg& m = lo->imgs[k];
     out.W = m.W;

@@ -172,7 +172,7 @@ struct Context {
     bool host_sc_borrowed = false;  // host_sc points at static storage, not cudaMallocHost memory
 
     const void* owner = nullptr; // object whose intermediates the buffers hold (shared workspaces)
-    std::shared_ptr<void> batch_plan;  // layout of the last labels-only batch (batch.cu)
+    std::shared_ptr<void> batch_plan;  // layout of the last batch (batch.cu)
     int64_t last_n_tri = 0;      // triangles of the last triangulation (host copy)
     bool have_result = false;
 
@@ -297,7 +297,8 @@ void assign_pixels(Context& C, int W, int H, const int32_t* xs, const int32_t* y
 
 void ensure_scalars(Context& C);
 
-// One image of the last labels-only batch on a context (idl_voronoi_batch):
+// One image of the last batch on a context (idl_voronoi_batch or a batched
+// triangulation):
 // its padded canvas sits at (ox, oy) of the atlas label planes C.lab[0/1]
 // (row pitch `pitch`), its seeds are C.xs/C.ys[seed_off, seed_off + n) in
 // (x, y) order with atlas labels seed_off + local id (batch.cu).
@@ -306,6 +307,17 @@ struct BatchImage {
     int64_t seed_off, n;
 };
 bool batch_image(const Context& C, int k, BatchImage& out);
+
+// The whole batched pipeline (idl_triangulate_batch) on host seeds, its
+// result kept on the context: per-image triangle counts to tri_counts; the
+// atlas labels for idl_delaunay_adopt and each image's grid and triangle
+// rows for batch_fetch (batch.cu).
+void triangulate_batch_keep(Context& C, int n_images, const int32_t* dims, const int64_t* counts,
+                            const int32_t* seeds_xy, int P, int64_t* tri_counts);
+// Queue on C.stream the copies of image k of the last triangulated batch:
+// its grid (H x W x 3 int32) and its triangle rows (5 int32 each, image-local
+// as idl_delaunay_triangles ids = 0 reports them) into host buffers.
+void batch_fetch(Context& C, int k, int32_t* grid_out, int32_t* tris_out, int64_t capacity);
 
 }  // namespace idl
 

@@ -144,11 +144,28 @@ struct DelaunayState {
         pixmem = nullptr;
         each_scratch([](DevBuf& b) { b.drop(); });
     }
+    // Marks the end of the object's work queued so far on its stream.  A
+    // stream change makes the new stream wait for it (a device-side wait on
+    // this object's own work, not on the rest of the old stream's), so the
+    // object's data -- and the stream-ordered frees of its scratch -- stay
+    // ordered after everything it did before.
+    cudaEvent_t last_use = nullptr;
+    void note_use() noexcept
+    {
+        if (!last_use) return;
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (cur != device) cudaSetDevice(device);
+        cudaEventRecord(last_use, stream);
+        if (cur >= 0 && cur != device) cudaSetDevice(cur);
+    }
+
     ~DelaunayState()
     {
         unbind();
         if (ws && ws->owner == this) ws->owner = nullptr;
         free_owned();
+        if (last_use) cudaEventDestroy(last_use);
     }
 };
 
@@ -672,7 +689,6 @@ void layout(DelaunayState& d, int width, int height, int64_t max_seeds, int P)
     IDL_CUDA(cudaMemsetAsync(d.planes, 0xFF, plane * 2 * sizeof(int32_t), d.stream));
     IDL_CUDA(cudaMemsetAsync(d.tgrid, 0xFF, (size_t)d.Wd * d.Hd * sizeof(int32_t), d.stream));
     IDL_CUDA(cudaMemsetAsync(d.values, 0, (size_t)max_seeds * sizeof(float), d.stream));
-    IDL_CUDA(cudaStreamSynchronize(d.stream));
 }
 
 void check_handle(const idl_delaunay* d)
@@ -680,9 +696,15 @@ void check_handle(const idl_delaunay* d)
     if (!d) invalid("Delaunay handle must not be NULL");
 }
 
+// Every entry point ends by undoing the workspace binding and noting the
+// object's last work on its stream.
 struct Unbinder {
     DelaunayState* d;
-    ~Unbinder() { d->unbind(); }
+    ~Unbinder()
+    {
+        d->unbind();
+        d->note_use();
+    }
 };
 
 }  // namespace
@@ -729,7 +751,10 @@ int idl_delaunay_create(int device, int width, int height, int64_t max_seeds, in
             invalid("padded canvas side exceeds the 32767 pixels this build addresses");
         d->mode = mode;
         layout(*d, width, height, max_seeds, P);
-        IDL_CUDA(cudaDeviceSynchronize());
+        // the allocations are ordered on the creating stream; a later
+        // set_stream orders the object's new stream after them
+        IDL_CUDA(cudaEventCreateWithFlags(&d->last_use, cudaEventDisableTiming));
+        IDL_CUDA(cudaEventRecord(d->last_use, d->stream));
     } catch (...) {
         delete d;
         throw;
@@ -761,7 +786,9 @@ int idl_delaunay_destroy(idl_delaunay* d)
     IDL_API_BEGIN
     if (!d) return IDL_OK;
     DeviceGuard g(d->device);
-    cudaStreamSynchronize(d->stream);
+    // wait for this object's own work only (not the rest of its stream's)
+    if (d->last_use) cudaEventSynchronize(d->last_use);
+    else cudaStreamSynchronize(d->stream);
     delete d;
     IDL_API_END
 }
@@ -772,11 +799,10 @@ int idl_delaunay_set_stream(idl_delaunay* d, void* stream)
     check_handle(d);
     const Unbinder unbind_on_exit{d};
     const cudaStream_t next = static_cast<cudaStream_t>(stream);
-    // Scratch is freed in the order of the object's stream: finish the old
-    // stream's work before later frees are ordered on the new one.
-    if (next != d->stream) {
+    // The new stream waits for the object's work so far on the old one.
+    if (next != d->stream && d->last_use) {
         DeviceGuard g(d->device);
-        IDL_CUDA(cudaStreamSynchronize(d->stream));
+        IDL_CUDA(cudaStreamWaitEvent(next, d->last_use, 0));
     }
     d->stream = next;
     IDL_API_END
@@ -923,7 +949,7 @@ int idl_delaunay_adopt(idl_delaunay* d, idl_context* src, int image)
     const Unbinder unbind_on_exit{d};
     if (!src) invalid("context must not be NULL");
     BatchImage bi;
-    if (!batch_image(*src, image, bi)) invalid("the context holds no labels-only batch with that image");
+    if (!batch_image(*src, image, bi)) invalid("the context holds no batch with that image");
     if (src->device != d->device) invalid("the batch was computed on another device");
     if (bi.W != d->W || bi.H != d->H || bi.P != d->P)
         invalid("the batch image's size or border padding differs from the object's");

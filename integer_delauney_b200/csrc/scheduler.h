@@ -19,7 +19,7 @@
 //     the pool and, failing that, by dropping pooled objects, largest first;
 //   * queued new diagrams that fit are grouped with the first (up to
 //     GROUP_MAX, one 4128^2 atlas of padded canvases, MAX_REQUEST_SEEDS
-//     seeds) so that one propagation launch serves them all;
+//     seeds) so that one pass of the batched pipeline serves them all;
 //   * a new diagram whose own footprint exceeds the budget fails at once;
 //     one that does not fit while nothing is running (so nothing can free
 //     memory) fails too, instead of waiting for good.
@@ -69,16 +69,25 @@ inline Capacity capacity(int W, int H, int64_t max_seeds, int P)
     return c;
 }
 
-// Scratch one workspace context grows for the largest request: micro-tile
-// lists and bitmaps, hash table, triangle rows, and a batch's label planes.
+// Scratch a context grows to triangulate a canvas of Wd x Hd with `seeds`
+// seeds: micro-tile lists and bitmaps, hash table, work lists, triangle rows.
+inline int64_t scratch_bytes(int64_t Wd, int64_t Hd, int64_t seeds)
+{
+    const int64_t n_mt = ((Wd + 7) / 8) * ((Hd + 7) / 8);
+    int64_t hash = 1024;
+    while (hash < 8 * seeds + 1024) hash <<= 1;
+    return n_mt * 8 + n_mt / 4 + 16 * (Wd + Hd) + 32 * hash + 48 * seeds + Wd * Hd / 8;
+}
+
+// Memory one worker slot holds at most: its diagram workspace, and its batch
+// context triangulating a full group (one atlas of MAX_SIDE^2 padded, its
+// label planes, raster and composed grids, seed arrays).
 inline int64_t slot_reserve(int P)
 {
     const int64_t Wd = MAX_SIDE + 2 * P, Hd = Wd;
-    const int64_t n_mt = ((Wd + 7) / 8) * ((Hd + 7) / 8);
-    int64_t hash = 1024;
-    while (hash < 8 * MAX_REQUEST_SEEDS + 1024) hash <<= 1;
-    return n_mt * 8 + n_mt / 4 + 16 * (Wd + Hd) + 32 * hash + 48 * MAX_REQUEST_SEEDS + Wd * Hd / 8 +
-           (Wd + 31) / 32 * 32 * Hd * 8;
+    const int64_t pitch = (Wd + 31) / 32 * 32;
+    const int64_t px = (int64_t)MAX_SIDE * MAX_SIDE;
+    return 2 * scratch_bytes(Wd, Hd, MAX_REQUEST_SEEDS) + pitch * Hd * 8 + px * 16 + 32 * MAX_REQUEST_SEEDS;
 }
 
 struct Request {

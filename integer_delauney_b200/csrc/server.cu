@@ -7,14 +7,18 @@
 // every diagram the slot runs shares (idl_delaunay_set_workspace) and a batch
 // context.  Scheduling and memory admission are the policy of scheduler.h,
 // run under the server's lock; a worker executes what it is handed:
-//   * a group of new diagrams: one idl_voronoi_batch launch propagates all of
-//     them (reference mode), then each object is reset and takes its image's
-//     labels (idl_delaunay_adopt) -- bit for bit the state an (x, y)-ordered
-//     insert reaches; if the batch rejects the group, each request runs on
-//     its own (idl_delaunay_insert_ordered) so that only the bad one fails;
-//   * an insert: idl_delaunay_insert_ordered into the resident object;
-// then brings the topology and pixel arrays up to date (finalise; with
-// `fetch`, into the caller's host grid, triangles kept for idl_server_wait)
+//   * a group of new diagrams (reference mode): one pass of the batched
+//     pipeline (idl_triangulate_batch's) triangulates all of them; each
+//     object is reset and takes its image's labels (idl_delaunay_adopt) --
+//     bit for bit the state an (x, y)-ordered insert reaches -- and the
+//     request's result (triangle count; with `fetch`, the grid and triangle
+//     rows) comes from the batch, whose per-image results equal the
+//     single-image pipeline's; the object's own topology follows lazily.  If
+//     the batch rejects the group, each request runs on its own
+//     (idl_delaunay_insert_ordered) so that only the bad one fails;
+//   * an insert (or a new diagram in exact mode): idl_delaunay_insert_ordered
+//     into the object, then finalise (with `fetch`, into the caller's host
+//     grid, triangles kept for idl_server_wait);
 // and synchronises its stream, so a result is complete when it is reported.
 // All of it is C++: a request costs a Python caller one call to submit and
 // one to collect.
@@ -72,8 +76,9 @@ struct idl_server {
     std::vector<std::thread> workers;
     int running = 0;   // workers executing a work list
     bool closing = false;
+    bool submitted = false;
 
-    idl_server(int64_t budget, int P, int n_slots) : sched(budget, P, 2 * (int64_t)n_slots * slot_reserve(P)) {}
+    idl_server(int64_t budget, int P, int n_slots) : sched(budget, P, (int64_t)n_slots * slot_reserve(P)) {}
 };
 
 namespace {
@@ -102,11 +107,17 @@ void deliver_failures(idl_server& S, std::vector<Failed>& failed)
 }
 
 // One request on the slot's stream; the outcome's status says how it ended.
-// For a new diagram, obj_out receives the object used (fresh or pooled, or
-// null if none could be created) and cap_out / dev_bytes its allocations.
-void execute(idl_server& S, Slot& slot, const Item& it, bool adopt, int image, int64_t start, Outcome& o,
+// `batch_tris` >= 0: a new diagram that is image `image` of the batch just
+// triangulated on the slot's batch context, with that many triangles -- the
+// object adopts its labels and the result (and fetched grid and rows) comes
+// from the batch; the object's own topology follows lazily when an insert
+// needs it.  For a new diagram, obj_out receives the object used (fresh or
+// pooled, or null if none could be created) and cap_out / dev_bytes its
+// allocations.
+void execute(idl_server& S, Slot& slot, const Item& it, int64_t batch_tris, int image, int64_t start, Outcome& o,
              void*& obj_out, Capacity& cap_out, int64_t& dev_bytes)
 {
+    const bool adopt = batch_tris >= 0;
     const Request& r = it.req;
     const int P = S.sched.padding();
     idl_delaunay* obj = static_cast<idl_delaunay*>(it.obj);
@@ -139,7 +150,13 @@ void execute(idl_server& S, Slot& slot, const Item& it, bool adopt, int image, i
             check_status(idl_delaunay_insert_ordered(obj, xy, n, nullptr, 0, nullptr));
             o.n_seeds = it.base_seeds + n;
         }
-        if (r.fetch) {
+        if (adopt) {
+            o.n_triangles = batch_tris;
+            if (r.fetch) {
+                o.tris.resize((size_t)batch_tris * 5);
+                idl::batch_fetch(*slot.batch, image, r.grid_out, o.tris.data(), (int64_t)o.tris.size());
+            }
+        } else if (r.fetch) {
             check_status(idl_delaunay_finalise(obj, r.grid_out, &o.n_triangles, nullptr));
             o.tris.resize((size_t)o.n_triangles * 5);
             int64_t got = 0;
@@ -200,7 +217,10 @@ void worker_loop(idl_server* Sp, int index)
         }
         destroy_all(to_free);
         const int64_t start = clock_ns();
-        bool adopt = false;
+        // a group of new diagrams: one pass of the batched pipeline for all
+        // of them; if it rejects the group (a request's bad seeds), each runs
+        // on its own so that only the bad one fails
+        std::vector<int64_t> batch_tris(work.size(), -1);
         if (work[0].req.kind == NEW && S.mode == IDL_MODE_REFERENCE) {
             std::vector<int32_t> dims, seeds;
             std::vector<int64_t> counts;
@@ -210,9 +230,13 @@ void worker_loop(idl_server* Sp, int index)
                 counts.push_back(it.req.n_seeds());
                 seeds.insert(seeds.end(), it.req.seeds.begin(), it.req.seeds.end());
             }
-            adopt = idl_voronoi_batch(slot.batch, (int)work.size(), dims.data(), counts.data(),
-                                      seeds.empty() ? nullptr : seeds.data(), S.sched.padding(),
-                                      IDL_MODE_REFERENCE) == IDL_OK;
+            try {
+                idl::triangulate_batch_keep(*slot.batch, (int)work.size(), dims.data(), counts.data(),
+                                            seeds.empty() ? nullptr : seeds.data(), S.sched.padding(),
+                                            batch_tris.data());
+            } catch (const std::exception&) {
+                std::fill(batch_tris.begin(), batch_tris.end(), -1);
+            }
             std::lock_guard<std::mutex> lk(S.mu);
             S.sched.count_group((int)work.size());
         }
@@ -222,7 +246,7 @@ void worker_loop(idl_server* Sp, int index)
             void* obj = nullptr;
             Capacity cap;
             int64_t dev_bytes = 0;
-            execute(S, slot, it, adopt, (int)k, start, o, obj, cap, dev_bytes);
+            execute(S, slot, it, batch_tris[k], (int)k, start, o, obj, cap, dev_bytes);
             void* drop = nullptr;
             {
                 std::lock_guard<std::mutex> lk(S.mu);
@@ -307,6 +331,19 @@ int idl_server_create(int device, int64_t budget_bytes, int slots, int border_pa
     IDL_API_END
 }
 
+int idl_server_set_schedule(idl_server* s, int dense_rounds)
+{
+    IDL_API_BEGIN
+    check_server(s);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->submitted) throw idl::Error(IDL_ERR_STATE, "the schedule is set before the first request");
+    for (auto& sl : s->slots) {
+        check_status(idl_context_set_schedule(sl.ws, dense_rounds));
+        check_status(idl_context_set_schedule(sl.batch, dense_rounds));
+    }
+    IDL_API_END
+}
+
 int idl_server_destroy(idl_server* s)
 {
     IDL_API_BEGIN
@@ -344,6 +381,7 @@ int idl_server_submit_new(idl_server* s, int width, int height, const int32_t* s
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->closing) throw idl::Error(IDL_ERR_STATE, "server is closing");
         s->sched.add_new(r);
+        s->submitted = true;
         s->outcomes[r.id] = Outcome{};
         if (request_out) *request_out = r.id;
         if (diagram_out) *diagram_out = r.diagram;

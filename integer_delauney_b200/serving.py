@@ -85,13 +85,15 @@ MAX_REQUEST_SEEDS = 200_000
 
 
 def slot_reserve(padding: int) -> int:
-    """Budget the server reserves per workspace context (two per slot: one for
-    diagrams, one for grouped propagation) -- slot_reserve() of
-    csrc/scheduler.h."""
+    """Budget the server reserves per worker slot (slot_reserve() of
+    csrc/scheduler.h): a diagram workspace, and a batch context triangulating
+    a full group (one atlas of MAX_SIDE^2 padded: label planes, raster,
+    composed grids, seed arrays)."""
     Wd = Hd = MAX_SIDE + 2 * padding
     pitch = (Wd + 31) // 32 * 32
-    return (estimate_bytes(MAX_SIDE, MAX_SIDE, MAX_REQUEST_SEEDS, padding) -
-            estimate_bytes(MAX_SIDE, MAX_SIDE, MAX_REQUEST_SEEDS, padding, workspace=False) + pitch * Hd * 8)
+    scratch = (estimate_bytes(MAX_SIDE, MAX_SIDE, MAX_REQUEST_SEEDS, padding) -
+               estimate_bytes(MAX_SIDE, MAX_SIDE, MAX_REQUEST_SEEDS, padding, workspace=False))
+    return 2 * scratch + pitch * Hd * 8 + MAX_SIDE * MAX_SIDE * 16 + 32 * MAX_REQUEST_SEEDS
 
 
 _KIND = {0: "new", 1: "insert"}
@@ -186,6 +188,12 @@ class Server:
         _capi.check(self._lib.idl_server_create(self.device, self.budget, int(slots), self.padding,
                                                 _capi.mode_id(mode), ctypes.byref(h)))
         self._h = h.value
+
+    def set_schedule(self, dense_rounds: int) -> None:
+        """Propagation schedule of the workers' contexts (Context.set_schedule;
+        -1: tile rounds to convergence, no device-wide persistent kernel).
+        Before the first request."""
+        _capi.check(self._lib.idl_server_set_schedule(self._handle(), int(dense_rounds)))
 
     def _handle(self) -> int:
         if self._h is None:

@@ -87,8 +87,8 @@ def test_new_requests_equal_the_batch_pipeline(cu):
 def test_small_budget_recycles_objects_and_keeps_results(cu):
     from integer_delauney_b200.serving import SEED_HEADROOM, estimate_bytes, slot_reserve
     news = [(200, 180, uniform(200, 180, 300, seed=i)) for i in range(12)]
-    # two slots reserve two workspaces each; room for three diagrams besides
-    budget = 3 * estimate_bytes(256, 256, 300 + SEED_HEADROOM, 16, workspace=False) + 4 * slot_reserve(16)
+    # two slots' reserves; room for three diagrams besides
+    budget = 3 * estimate_bytes(256, 256, 300 + SEED_HEADROOM, 16, workspace=False) + 2 * slot_reserve(16)
     a_new, _ = _alone(cu, news, [])
     m_new, _, stats = _mixed(news, [], budget=budget, slots=2)
     for a, m in zip(a_new, m_new):
