@@ -100,8 +100,11 @@ IDL_API int idl_context_workspace_bytes(idl_context* ctx, int64_t* bytes_out);
  * `dense_rounds` rounds of 8 passes run as tile rounds (one HBM round trip per
  * 8 passes over every tile that can change), the rest in the persistent
  * sparse kernel; 0 = sparse kernel only, < 0 = tile rounds to convergence.
- * Results do not depend on it, only the time does.  Default 1.  No
- * counterpart in the reference (its schedule is one full pass per launch). */
+ * A continued propagation (an incremental object's insert using this context)
+ * runs in the sparse kernel, or with dense_rounds < 0 as tile rounds starting
+ * from the tiles around the new seeds.  Results do not depend on it, only the
+ * time does.  Default 1.  No counterpart in the reference (its schedule is
+ * one full pass per launch). */
 IDL_API int idl_context_set_schedule(idl_context* ctx, int dense_rounds);
 
 /* Record per-stage CUDA events on the context's stream for every following
@@ -457,9 +460,11 @@ IDL_API int64_t idl_server_clock_ns(void);
  * another mode -> IDL_ERR_INVALID. */
 IDL_API int idl_server_create(int device, int64_t budget_bytes, int slots, int border_padding, int mode,
                               idl_server** out);
-/* Propagation schedule of every slot's contexts (idl_context_set_schedule),
- * before the first request; IDL_ERR_STATE after it. */
-IDL_API int idl_server_set_schedule(idl_server* s, int dense_rounds);
+/* Propagation schedules (idl_context_set_schedule) of every slot: of the
+ * grouped new diagrams (group_rounds) and of inserts (insert_rounds; < 0 runs
+ * them as tile rounds from the new seeds' tiles instead of the device-wide
+ * persistent kernel).  Before the first request; IDL_ERR_STATE after it. */
+IDL_API int idl_server_set_schedule(idl_server* s, int group_rounds, int insert_rounds);
 /* Runs what is queued, stops the workers and frees every object. */
 IDL_API int idl_server_destroy(idl_server* s);
 /* Queue a new diagram (seeds copied; n <= 200000).  fetch != 0: grid_out

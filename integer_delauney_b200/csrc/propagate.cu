@@ -288,6 +288,23 @@ __global__ void k_iota(int32_t* __restrict__ a, int n, int32_t* __restrict__ cou
 
 __global__ void k_set_i64(long long* p, long long v) { *p = v; }
 
+// First work list of a continued propagation: the tiles holding the n new
+// seeds and their 8 neighbours (a wave from a seed reaches at most KSTEPS <=
+// TW cells into the next tile in one round), each listed once.
+__global__ void k_seed_round_tiles(const uint32_t* __restrict__ seed_pos, int64_t n, int tiles_x, int tiles_y,
+                                   int32_t* __restrict__ stamp, int32_t stamp_val, int32_t* __restrict__ list,
+                                   int32_t* __restrict__ count)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * 9) return;
+    const uint32_t p = seed_pos[i / 9];
+    const int k = (int)(i % 9);
+    const int nx = (int)pos_x(p) / TW + k % 3 - 1, ny = (int)pos_y(p) / TH + k / 3 - 1;
+    if (nx < 0 || nx >= tiles_x || ny < 0 || ny >= tiles_y) return;
+    const int t = ny * tiles_x + nx;
+    if (atomicExch(&stamp[t], stamp_val) != stamp_val) list[atomicAdd(count, 1)] = t;
+}
+
 __global__ void k_write_seeds(int32_t* __restrict__ a, int32_t* __restrict__ b, int pitch,
                               const uint32_t* __restrict__ pos, int64_t n)
 {
@@ -339,14 +356,18 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, c
     C.prof.tiles = C.prof.rounds = C.prof.passes = 0;
     C.prof.prop_bytes = 0.0;
     // Reference semantics.  A continued propagation (seed_pos) is local from
-    // its first pass: the sparse kernel alone.  From scratch, the first
-    // passes change most of the canvas, which the tile rounds (KSTEPS passes
-    // per HBM round trip, no per-pass bookkeeping) do best; once the changes
-    // thin out, the sparse kernel takes over the tail, whose single passes
-    // touch few cells.  C.dense_rounds sets the switch (0: sparse only,
-    // < 0: tile rounds to convergence).
+    // its first pass: the sparse kernel alone, or with C.dense_rounds < 0 tile
+    // rounds starting from the tiles around the new seeds (plain launches, no
+    // device-wide persistent grid, so streams of other work overlap them).
+    // From scratch, the first passes change most of the canvas, which the
+    // tile rounds (KSTEPS passes per HBM round trip, no per-pass bookkeeping)
+    // do best; once the changes thin out, the sparse kernel takes over the
+    // tail, whose single passes touch few cells.  C.dense_rounds sets the
+    // switch (0: sparse only, < 0: tile rounds to convergence).
+    const bool seeded_rounds = mode == IDL_MODE_REFERENCE && seed_pos && C.dense_rounds < 0;
     const bool hybrid = mode == IDL_MODE_REFERENCE && !seed_pos && C.dense_rounds != 0;
-    if (mode == IDL_MODE_REFERENCE && !hybrid) return propagate_sparse(C, cv, pos, seed_pos, n_new);
+    if (mode == IDL_MODE_REFERENCE && !hybrid && !seeded_rounds) return propagate_sparse(C, cv, pos, seed_pos, n_new);
+    if (seed_pos && n_new == 0) return 0;
     const int64_t round_limit = hybrid && C.dense_rounds > 0 ? C.dense_rounds : -1;
     const int tiles_x = ceil_div(cv.Wd, TW), tiles_y = ceil_div(cv.Hd, TH);
     const int n_tiles = tiles_x * tiles_y;
@@ -364,7 +385,13 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, c
     IDL_CUDA(cudaMemsetAsync(C.counts.ptr, 0, count_len * 4, C.stream));
     int32_t* counts = C.counts.as<int32_t>();
 
-    k_iota<<<(unsigned)((n_tiles + 255) / 256), 256, 0, C.stream>>>(C.tiles[0].as<int32_t>(), n_tiles, counts);
+    if (seeded_rounds) {
+        k_seed_round_tiles<<<(unsigned)((n_new * 9 + 255) / 256), 256, 0, C.stream>>>(
+            seed_pos, n_new, tiles_x, tiles_y, C.stamps.as<int32_t>(), epoch + int32_t(max_rounds) + 2,
+            C.tiles[0].as<int32_t>(), counts);   // a stamp value of the claimed range no round uses
+    } else {
+        k_iota<<<(unsigned)((n_tiles + 255) / 256), 256, 0, C.stream>>>(C.tiles[0].as<int32_t>(), n_tiles, counts);
+    }
     IDL_LAUNCH();
     long long* last = reinterpret_cast<long long*>(&C.sc()->last_change);
     k_set_i64<<<1, 1, 0, C.stream>>>(last, -1);

@@ -331,15 +331,15 @@ int idl_server_create(int device, int64_t budget_bytes, int slots, int border_pa
     IDL_API_END
 }
 
-int idl_server_set_schedule(idl_server* s, int dense_rounds)
+int idl_server_set_schedule(idl_server* s, int group_rounds, int insert_rounds)
 {
     IDL_API_BEGIN
     check_server(s);
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->submitted) throw idl::Error(IDL_ERR_STATE, "the schedule is set before the first request");
     for (auto& sl : s->slots) {
-        check_status(idl_context_set_schedule(sl.ws, dense_rounds));
-        check_status(idl_context_set_schedule(sl.batch, dense_rounds));
+        check_status(idl_context_set_schedule(sl.batch, group_rounds));
+        check_status(idl_context_set_schedule(sl.ws, insert_rounds));
     }
     IDL_API_END
 }

@@ -189,11 +189,12 @@ class Server:
                                                 _capi.mode_id(mode), ctypes.byref(h)))
         self._h = h.value
 
-    def set_schedule(self, dense_rounds: int) -> None:
-        """Propagation schedule of the workers' contexts (Context.set_schedule;
-        -1: tile rounds to convergence, no device-wide persistent kernel).
-        Before the first request."""
-        _capi.check(self._lib.idl_server_set_schedule(self._handle(), int(dense_rounds)))
+    def set_schedule(self, group_rounds: int, insert_rounds: int) -> None:
+        """Propagation schedules (Context.set_schedule) of the grouped new
+        diagrams and of inserts (-1 for inserts: tile rounds from the new
+        seeds' tiles, no device-wide persistent kernel).  Before the first
+        request."""
+        _capi.check(self._lib.idl_server_set_schedule(self._handle(), int(group_rounds), int(insert_rounds)))
 
     def _handle(self) -> int:
         if self._h is None:

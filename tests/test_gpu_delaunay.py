@@ -472,3 +472,37 @@ def test_exact_mode_equals_full_recompute_after_every_insert(cu, sizes, P):
     np.testing.assert_array_equal(g, o_grid)
     np.testing.assert_array_equal(np.array([m[t] for t in range(len(m))]).reshape(-1, 5), o_tris)
     np.testing.assert_array_equal(d.sorted_rank[d.get_triangles()], o_tris[:, 2:5])
+
+
+def test_insert_as_tile_rounds_equals_sparse_kernel(cu):
+    """A workspace context with schedule < 0 runs an insert's continued
+    propagation as tile rounds from the new seeds' tiles; the result equals the
+    persistent sparse kernel's (the default) after every insert, bit for bit
+    -- both are the synchronous Jacobi fixed point continued from the last."""
+    from integer_delauney_b200 import _capi
+    from integer_delauney_b200.workloads import fresh_points
+    W, H = 733, 517
+    base = uniform(W, H, 2500, seed=21)
+    ctx = _capi.Context(0)
+    ctx.set_schedule(-1)
+    a = cu.Delaunay(W, H, 9000, 16)
+    b = cu.Delaunay(W, H, 9000, 16)
+    b.use_workspace(ctx)
+    keys = np.sort(base[:, 1].astype(np.int64) * W + base[:, 0])
+    batches = [base]
+    for i, n in enumerate((1, 40, 600, 1500)):
+        add = fresh_points(W, H, n, keys, seed=100 + i)
+        if i == 2:                                  # a dense hotspot in one corner
+            add = fresh_points(90, 70, n // 2, np.zeros(0, np.int64), seed=300)
+            k2 = add[:, 1].astype(np.int64) * W + add[:, 0]
+            add = add[~np.isin(k2, keys)]
+        batches.append(add)
+        keys = np.sort(np.concatenate([keys, add[:, 1].astype(np.int64) * W + add[:, 0]]))
+    for add in batches:
+        a.insert_deferred(add)
+        b.insert_deferred(add)
+        np.testing.assert_array_equal(a.get_voronoi_grid(), b.get_voronoi_grid())
+    va, ga = a.finalise(as_arrays=True)
+    vb, gb = b.finalise(as_arrays=True)
+    np.testing.assert_array_equal(va, vb)
+    np.testing.assert_array_equal(ga, gb)
