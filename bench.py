@@ -449,9 +449,11 @@ def serving_case(torch, rank, seconds, slots=8):
             meta[j] = (W, H, np.sort(np.concatenate([k, keys_of(W, pts)])))
             meta.append(None)              # meta stays index-aligned with reqs
             reqs.append(("insert", j, pts))
-    def saturate(n_slots):
+    def saturate(n_slots, schedule=None):
         torch.cuda.synchronize()
         srv = Server(budget_bytes=budget, slots=n_slots, border_padding=PADDING)
+        if schedule is not None:
+            srv.set_schedule(*schedule)
         t1 = time.perf_counter()
         fut_of = {}
         sfuts = []
@@ -474,6 +476,7 @@ def serving_case(torch, rank, seconds, slots=8):
     saturate(slots)                         # warm-up, untimed: the device memory pool grows once
     t_srv, srv_ok = saturate(slots)
     t_one, one_ok = saturate(1)
+    t_pk, pk_ok = saturate(slots, (1, 1))      # inserts in the persistent kernel instead of tile rounds
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     out = run_serial(reqs, PADDING, budget)
@@ -483,6 +486,7 @@ def serving_case(torch, rank, seconds, slots=8):
     saturated = {"requests": len(reqs), "slots": slots,
                  "server_s": t_srv, "server_req_s": srv_ok / t_srv, "server_ok": srv_ok,
                  "server_1slot_req_s": one_ok / t_one,
+                 "server_insert_persistent_kernel_req_s": pk_ok / t_pk,
                  "serial_s": t_ser, "serial_req_s": ser_ok / t_ser, "serial_ok": ser_ok,
                  "speedup_vs_serial": (srv_ok / t_srv) / (ser_ok / t_ser),
                  "speedup_vs_1slot": (srv_ok / t_srv) / (one_ok / t_one)}

@@ -461,9 +461,10 @@ IDL_API int64_t idl_server_clock_ns(void);
 IDL_API int idl_server_create(int device, int64_t budget_bytes, int slots, int border_padding, int mode,
                               idl_server** out);
 /* Propagation schedules (idl_context_set_schedule) of every slot: of the
- * grouped new diagrams (group_rounds) and of inserts (insert_rounds; < 0 runs
- * them as tile rounds from the new seeds' tiles instead of the device-wide
- * persistent kernel).  Before the first request; IDL_ERR_STATE after it. */
+ * grouped new diagrams (group_rounds, default 1) and of inserts (insert_rounds,
+ * default -1: tile rounds from the new seeds' tiles, plain launches that
+ * overlap other slots' work; 0 or more: the device-wide persistent kernel).
+ * Before the first request; IDL_ERR_STATE after it. */
 IDL_API int idl_server_set_schedule(idl_server* s, int group_rounds, int insert_rounds);
 /* Runs what is queued, stops the workers and frees every object. */
 IDL_API int idl_server_destroy(idl_server* s);
