@@ -24,7 +24,7 @@
  *   or_triangulate         src/cuda/triangulation.cu:143-365
  *
  * Parity is pinned in tests/ against golden vectors generated from the
- * reference's own NumPy implementation (tests/golden/) and, on a GPU box, the
+ * reference's own NumPy implementation (tests/golden/) and, on a B200, the
  * reference's own CUDA batch path built into oracle/_ref.
  *
  * Build: see oracle/Makefile (gcc -O2 -fopenmp -ffp-contract=off).
