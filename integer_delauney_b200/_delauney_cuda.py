@@ -276,6 +276,38 @@ class DeviceArrayView:
         return {"shape": (self._count,), "typestr": self._typestr, "data": (self._ptr, True),
                 "strides": None, "version": 3}
 
+    def _raw(self, keep):
+        """An object exposing the same memory through a writable interface
+        (torch refuses read-only ones), holding `keep` alive."""
+        raw = type("_Raw", (), {"__cuda_array_interface__": {
+            "shape": (self._count,), "typestr": self._typestr, "data": (self._ptr, False),
+            "strides": None, "version": 3}})()
+        raw._keep = keep
+        return raw
+
+    def to_torch(self):
+        """The view as a torch tensor on the object's device, without a copy
+        (1-D, int32 or uint8): for consumers that take tensors or DLPack --
+        not in the reference, whose views stop at the CUDA array interface.
+        The tensor keeps the Delaunay alive, but like the view it is only
+        meaningful until the object's next insert or finalise.  torch has no
+        read-only tensors: writes through it land in the object's arrays."""
+        self._check_fresh()
+        if torch is None:
+            raise RuntimeError("to_torch() needs torch")
+        dev = self._owner._device
+        if not self._count:
+            return torch.empty(0, dtype=torch.int32 if self._typestr == "<i4" else torch.uint8, device=f"cuda:{dev}")
+        return torch.as_tensor(self._raw(self), device=f"cuda:{dev}")
+
+    def __dlpack__(self, stream=None, **kwargs):
+        """DLPack export (zero-copy, through ``to_torch``): ``torch.from_dlpack(view)``
+        and other DLPack consumers read the device memory in place."""
+        return self.to_torch().__dlpack__(stream=stream, **kwargs)
+
+    def __dlpack_device__(self):
+        return (2, int(self._owner._device))   # kDLCUDA, device ordinal
+
     def to_host(self) -> np.ndarray:
         """Host NumPy copy of the view's content."""
         self._check_fresh()
@@ -284,10 +316,7 @@ class DeviceArrayView:
             raise RuntimeError("to_host() needs torch for the device copy")
         out = np.empty(self._count, dtype=dtype)
         if self._count:
-            # torch refuses read-only interfaces; the copy below only reads
-            inner = type("_Raw", (), {"__cuda_array_interface__": {
-                "shape": (self._count,), "typestr": self._typestr, "data": (self._ptr, False),
-                "strides": None, "version": 3}})()
+            inner = self._raw(None)   # the copy below only reads
             with torch.cuda.device(self._owner._device):
                 torch.cuda.current_stream().synchronize()
                 out[:] = torch.as_tensor(inner, device=f"cuda:{self._owner._device}").cpu().numpy()

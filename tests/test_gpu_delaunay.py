@@ -246,6 +246,15 @@ class TestFinaliseDevice:
             assert cai["data"][1] is True and cai["version"] == 3
             np.testing.assert_array_equal(read_device(cai, want.dtype), want)
             np.testing.assert_array_equal(view.to_host(), want)
+            # zero-copy handoff: a torch tensor and a DLPack import alias the same memory
+            import torch
+            t = view.to_torch()
+            assert t.data_ptr() == cai["data"][0] and t.is_cuda and t.numel() == self.W * self.H
+            np.testing.assert_array_equal(t.cpu().numpy(), want)
+            u = torch.from_dlpack(view)
+            assert u.data_ptr() == cai["data"][0]
+            np.testing.assert_array_equal(u.cpu().numpy(), want)
+            assert view.__dlpack_device__() == (2, torch.cuda.current_device())
 
     def test_stale_views_raise(self, cu):
         d = cu.Delaunay(self.W, self.H, 512, -1)
@@ -258,6 +267,8 @@ class TestFinaliseDevice:
                 v.__cuda_array_interface__
             with pytest.raises(RuntimeError):
                 v.to_host()
+            with pytest.raises(RuntimeError):
+                v.to_torch()
         _, t1, _, _ = d.finalise_device()
         _, t2, _, _ = d.finalise_device()
         with pytest.raises(RuntimeError):
