@@ -295,12 +295,29 @@ def batched_case(torch, lib, ctx, stream, rank):
 
     ms_b, launches_b = timed(batch, 5)
     ms_l, launches_l = timed(loop, 2)
+    exact = _capi.mode_id("exact")
+
+    def batch_exact():
+        _capi.check(lib.idl_triangulate_batch_device(ctx.handle, len(imgs), dims.ctypes.data, counts.ctypes.data,
+                                                     seeds.data_ptr(), PADDING, exact, out.data_ptr(),
+                                                     tri_counts.ctypes.data))
+
+    def loop_exact():
+        for i, (w, h, _) in enumerate(imgs):
+            _capi.check(lib.idl_triangulate_device(ctx.handle, w, h, seeds.data_ptr() + int(s_off[i]) * 8,
+                                                   int(counts[i]), PADDING, exact,
+                                                   out.data_ptr() + int(p_off[i]) * 12, ctypes.byref(n_tri)))
+
+    ms_bx, _ = timed(batch_exact, 5)
+    ms_lx, _ = timed(loop_exact, 2)
     total = float(px.sum())
     return {"workload": f"{len(imgs)} images, sides log-uniform 64..1024, density 0.1..2 %, "
                         f"{int(counts.sum())} seeds, {int(total)} pixels, P={PADDING}, reference mode",
             "batch_ms": ms_b, "batch_mpix_s": total / (ms_b / 1e3) / 1e6, "batch_launches": int(launches_b),
             "loop_ms": ms_l, "loop_mpix_s": total / (ms_l / 1e3) / 1e6, "loop_launches": int(launches_l),
-            "speedup_vs_loop": ms_l / ms_b}
+            "speedup_vs_loop": ms_l / ms_b,
+            "exact_mode": {"batch_ms": ms_bx, "batch_mpix_s": total / (ms_bx / 1e3) / 1e6, "loop_ms": ms_lx,
+                           "speedup_vs_loop": ms_lx / ms_bx}}
 
 
 def serving_case(torch, rank, seconds, slots=8):

@@ -212,7 +212,10 @@ IDL_API int idl_voronoi_noalloc(int width, int height, const int32_t* d_seeds_xy
  * propagation launch, one detection, one raster and one composition launch
  * for the whole batch, and a fixed number of host synchronisations.  Each
  * image's grid and triangles equal idl_triangulate on that image alone, bit
- * for bit.  Limits: mode IDL_MODE_REFERENCE; at most 2097151 seeds in total;
+ * for bit.  In IDL_MODE_EXACT the propagation launch is replaced by the
+ * separable exact search (three launches over all images, each image kept
+ * within its own canvas).  Limits: modes IDL_MODE_REFERENCE and IDL_MODE_EXACT;
+ * at most 2097151 seeds in total;
  * the padded canvases must shelf-pack into a 32767 x 32767 atlas (about
  * 10^9 padded pixels), otherwise IDL_ERR_INVALID asks for a smaller batch.
  *   dims         host n_images * 2 int32: (width, height) per image
@@ -239,7 +242,9 @@ IDL_API int idl_triangulate_batch_device(idl_context* ctx, int n_images, const i
  * converged labels of every image stay in the context for idl_delaunay_adopt
  * (until the context's next triangulation or batch call).  No counterpart in
  * the reference; a server uses it to propagate many new diagrams in one
- * launch.  Arguments as idl_triangulate_batch. */
+ * launch.  Arguments as idl_triangulate_batch; IDL_MODE_REFERENCE only.  Only
+ * a batch in IDL_MODE_REFERENCE (this call's, or idl_triangulate_batch's) can
+ * be adopted. */
 IDL_API int idl_voronoi_batch(idl_context* ctx, int n_images, const int32_t* dims, const int64_t* seed_counts,
                               const int32_t* seeds_xy, int border_padding, int mode);
 

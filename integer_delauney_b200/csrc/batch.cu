@@ -111,6 +111,120 @@ __global__ void k_b_seeds(int32_t* __restrict__ a, int32_t* __restrict__ b, int 
     b[o] = (int32_t)i;
 }
 
+// ---- exact semantics over the atlas -------------------------------------
+// The separable nearest-seed search of the single-image exact mode (exact.cu),
+// run for every image of the atlas at once and kept inside each image: a
+// column walk uses only its image's seeds, a row scan only its image's
+// columns, so no label crosses a wall.  Labels are global seed ids, as the
+// Jacobi path leaves them.
+struct XImg {
+    int ox, oy, Wp, Hp;    // padded canvas origin and size in the atlas
+    int col_off, row_off;  // first entry of this image in the column / row tables
+    long long s0, s1;      // its seeds: global ids [s0, s1), (x, y)-sorted
+};
+constexpr int XCHUNK = 64;
+
+// cs[col_off + c] = first seed of the image with atlas x >= ox + c, c in [0, Wp].
+__global__ void k_bx_col_start(const uint32_t* __restrict__ pos, const XImg* __restrict__ xi,
+                               const int32_t* __restrict__ colimg, int64_t n_cols, int32_t* __restrict__ cs)
+{
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_cols) return;
+    const XImg m = xi[colimg[g]];
+    const int c = m.ox + (int)(g - m.col_off);
+    long long lo = m.s0, hi = m.s1;
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if ((int)pos_x(__ldg(&pos[mid])) < c) lo = mid + 1;
+        else hi = mid;
+    }
+    cs[g] = (int32_t)lo;
+}
+
+// Nearest seed of each cell within its image column (a tie between the seed
+// above and the one below goes to the lower one, the higher id), and its row
+// distance; one thread walks one column through a band of XCHUNK rows.
+__global__ void k_bx_col_nearest(const uint32_t* __restrict__ pos, const XImg* __restrict__ xi,
+                                 const int32_t* __restrict__ colimg, const int32_t* __restrict__ cs, int64_t n_cols,
+                                 int pitch, int32_t* __restrict__ col, int32_t* __restrict__ coldy)
+{
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_cols) return;
+    const XImg m = xi[colimg[g]];
+    const int c = (int)(g - m.col_off);
+    const int y0 = blockIdx.y * XCHUNK;
+    if (c >= m.Wp || y0 >= m.Hp) return;   // the image's extra start entry, or past its rows
+    const int y1 = min(m.Hp, y0 + XCHUNK);
+    const int x = m.ox + c;
+    const int32_t lo = cs[g], hi = cs[g + 1];
+    if (lo == hi) {
+        for (int y = y0; y < y1; ++y) {
+            col[(size_t)(m.oy + y) * pitch + x] = UNDEF;
+            coldy[(size_t)(m.oy + y) * pitch + x] = 0;
+        }
+        return;
+    }
+    int32_t a = lo, b = hi;   // first seed of the column at or below the band
+    while (a < b) {
+        const int32_t mid = (a + b) >> 1;
+        if ((int)pos_y(__ldg(&pos[mid])) < m.oy + y0) a = mid + 1;
+        else b = mid;
+    }
+    int next_y = a < hi ? (int)pos_y(__ldg(&pos[a])) : 0x7FFFFFFF;
+    int prev_y = a > lo ? (int)pos_y(__ldg(&pos[a - 1])) : -0x3FFFFFFF;
+    for (int y = y0; y < y1; ++y) {
+        const int ya = m.oy + y;
+        while (next_y < ya) {
+            prev_y = next_y;
+            ++a;
+            next_y = a < hi ? (int)pos_y(__ldg(&pos[a])) : 0x7FFFFFFF;
+        }
+        const int below = next_y - ya, above = ya - prev_y;
+        const bool take_below = a < hi && (a == lo || below <= above);
+        col[(size_t)ya * pitch + x] = take_below ? a : a - 1;
+        coldy[(size_t)ya * pitch + x] = take_below ? below : above;
+    }
+}
+
+// Best column candidate of each cell of an image row, scanning outward until
+// no column further away can beat or tie it.
+__global__ void k_bx_row_nearest(const int32_t* __restrict__ col, const int32_t* __restrict__ coldy,
+                                 const XImg* __restrict__ xi, const int32_t* __restrict__ rowimg, int pitch,
+                                 int32_t* __restrict__ lab)
+{
+    const int64_t r = blockIdx.x;
+    const XImg m = xi[rowimg[r]];
+    const int x = blockIdx.y * blockDim.x + threadIdx.x;
+    if (x >= m.Wp) return;
+    const int y = m.oy + (int)(r - m.row_off);
+    const int32_t* row = col + (size_t)y * pitch + m.ox;
+    const int32_t* rdy = coldy + (size_t)y * pitch + m.ox;
+    int32_t bl = row[x];
+    long long bd = 0x7FFFFFFFFFFFFFFFll;
+    if (bl >= 0) {
+        const long long dy = rdy[x];
+        bd = dy * dy;
+    }
+    for (int k = 1;; ++k) {
+        const long long kk = (long long)k * k;
+        if (kk > bd || (x - k < 0 && x + k >= m.Wp)) break;
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const int xx = side ? x + k : x - k;
+            if (xx < 0 || xx >= m.Wp) continue;
+            const int32_t l = row[xx];
+            if (l < 0) continue;
+            const long long dy = rdy[xx];
+            const long long d = kk + dy * dy;
+            if (d < bd || (d == bd && l > bl)) {
+                bd = d;
+                bl = l;
+            }
+        }
+    }
+    lab[(size_t)y * pitch + m.ox + x] = bl;
+}
+
 __device__ __forceinline__ int tri_image(const int32_t* row, const int32_t* __restrict__ sid_img)
 {
     return sid_img[min(row[2], min(row[3], row[4]))];
@@ -280,12 +394,64 @@ struct BatchPlan {
     int P = 0, pitch = 0;
     int64_t n_seeds = 0;
     bool full = false;               // grids in `grids`, image-local rows in C.tris
+    bool exact = false;              // labels of the exact semantics (not adoptable)
     const int32_t* grids = nullptr;  // device, n_px x 3 int32
     std::vector<int64_t> tri_off;    // n_images + 1 row offsets
 };
 
+// Exact-semantics labels of every image into C.lab[0] (the atlas's walls
+// stay); C.lab[1] and C.exact_dy are scratch.
+void exact_atlas(Context& C, const Plan& pl, int P, const Canvas& cv)
+{
+    const int n_images = (int)pl.imgs.size();
+    std::vector<XImg> xi(n_images);
+    std::vector<int32_t> colimg, rowimg;
+    int max_wp = 0, max_hp = 0;
+    for (int i = 0; i < n_images; ++i) {
+        const BImg& b = pl.imgs[i];
+        XImg& m = xi[i];
+        m.ox = b.ox;
+        m.oy = b.oy;
+        m.Wp = b.W + 2 * P;
+        m.Hp = b.H + 2 * P;
+        m.col_off = (int)colimg.size();
+        m.row_off = (int)rowimg.size();
+        m.s0 = b.seed_off;
+        m.s1 = i + 1 < n_images ? pl.imgs[i + 1].seed_off : pl.n_seeds;
+        colimg.insert(colimg.end(), (size_t)m.Wp + 1, i);
+        rowimg.insert(rowimg.end(), (size_t)m.Hp, i);
+        max_wp = std::max(max_wp, m.Wp);
+        max_hp = std::max(max_hp, m.Hp);
+    }
+    const int64_t n_cols = (int64_t)colimg.size(), n_rows = (int64_t)rowimg.size();
+    C.batch_ximg.ensure(xi.size() * sizeof(XImg));
+    C.batch_colimg.ensure((size_t)n_cols * 4);
+    C.batch_rowimg.ensure((size_t)n_rows * 4);
+    C.counts.ensure((size_t)n_cols * 4);
+    C.exact_dy.ensure((size_t)cv.pitch * cv.Hd * 4);
+    IDL_CUDA(cudaMemcpyAsync(C.batch_ximg.ptr, xi.data(), xi.size() * sizeof(XImg), cudaMemcpyHostToDevice,
+                             C.stream));
+    IDL_CUDA(cudaMemcpyAsync(C.batch_colimg.ptr, colimg.data(), (size_t)n_cols * 4, cudaMemcpyHostToDevice,
+                             C.stream));
+    IDL_CUDA(cudaMemcpyAsync(C.batch_rowimg.ptr, rowimg.data(), (size_t)n_rows * 4, cudaMemcpyHostToDevice,
+                             C.stream));
+    const XImg* d_xi = C.batch_ximg.as<XImg>();
+    const int32_t* d_colimg = C.batch_colimg.as<int32_t>();
+    int32_t* cs = C.counts.as<int32_t>();
+    const uint32_t* pos = C.pos.as<uint32_t>();
+    k_bx_col_start<<<nblk(n_cols), 256, 0, C.stream>>>(pos, d_xi, d_colimg, n_cols, cs);
+    IDL_LAUNCH();
+    k_bx_col_nearest<<<dim3(nblk(n_cols, 128), (unsigned)((max_hp + XCHUNK - 1) / XCHUNK)), 128, 0, C.stream>>>(
+        pos, d_xi, d_colimg, cs, n_cols, cv.pitch, C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>());
+    IDL_LAUNCH();
+    k_bx_row_nearest<<<dim3((unsigned)n_rows, (unsigned)((max_wp + 255) / 256)), 256, 0, C.stream>>>(
+        C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>(), d_xi, C.batch_rowimg.as<int32_t>(), cv.pitch,
+        C.lab[0].as<int32_t>());
+    IDL_LAUNCH();
+}
+
 void run_batch(Context& C, const Plan& pl, int P, int n_images, int32_t* d_out, int64_t* tri_counts,
-               float* timings, bool labels_only = false)
+               float* timings, bool labels_only = false, int mode = IDL_MODE_REFERENCE)
 {
     C.batch_plan.reset();
     const int64_t n = pl.n_seeds;
@@ -357,17 +523,22 @@ void run_batch(Context& C, const Plan& pl, int P, int n_images, int32_t* d_out, 
     k_b_open<<<dim3(64, n_images), 256, 0, C.stream>>>(C.lab[0].as<int32_t>(), C.lab[1].as<int32_t>(), cv.pitch,
                                                        d_imgs, P);
     IDL_LAUNCH();
-    k_b_seeds<<<nblk(n), 256, 0, C.stream>>>(C.lab[0].as<int32_t>(), C.lab[1].as<int32_t>(), cv.pitch,
-                                            C.pos.as<uint32_t>(), n);
-    IDL_LAUNCH();
     mark(1);
-    propagate(C, IDL_MODE_REFERENCE, cv, C.pos.as<uint32_t>());
+    if (mode == IDL_MODE_EXACT) {
+        exact_atlas(C, pl, P, cv);
+    } else {
+        k_b_seeds<<<nblk(n), 256, 0, C.stream>>>(C.lab[0].as<int32_t>(), C.lab[1].as<int32_t>(), cv.pitch,
+                                                C.pos.as<uint32_t>(), n);
+        IDL_LAUNCH();
+        propagate(C, IDL_MODE_REFERENCE, cv, C.pos.as<uint32_t>());
+    }
     mark(2);
     auto bp = std::make_shared<BatchPlan>();
     bp->imgs = pl.imgs;
     bp->P = P;
     bp->pitch = cv.pitch;
     bp->n_seeds = n;
+    bp->exact = mode == IDL_MODE_EXACT;
     C.batch_plan = bp;
     if (labels_only) return;
     detect_triangles(C, cv, C.lab[0].as<int32_t>(), C.pos.as<uint32_t>(), n, 0, timings ? ev[3] : nullptr);
@@ -462,7 +633,7 @@ void batch_fetch(Context& C, int k, int32_t* grid_out, int32_t* tris_out, int64_
 bool batch_image(const Context& C, int k, BatchImage& out)
 {
     const auto* lo = static_cast<const BatchPlan*>(C.batch_plan.get());
-    if (!lo || k < 0 || k >= (int)lo->imgs.size()) return false;
+    if (!lo || lo->exact || k < 0 || k >= (int)lo->imgs.size()) return false;
     const BImg& m = lo->imgs[k];
     out.W = m.W;
     out.H = m.H;
@@ -509,7 +680,8 @@ int idl_triangulate_batch(idl_context* ctx, int n_images, const int32_t* dims, c
     IDL_API_BEGIN
     if (!ctx) invalid("context must not be NULL");
     if (!dims || !seed_counts) invalid("dims and seed_counts must not be NULL");
-    if (mode != IDL_MODE_REFERENCE) invalid("batched triangulation supports voronoi_mode 'reference' only");
+    if (mode != IDL_MODE_REFERENCE && mode != IDL_MODE_EXACT)
+        invalid("batched triangulation supports voronoi_mode 'reference' and 'exact'");
     const int P = border_padding == IDL_AUTO_BORDER_PADDING ? IDL_DEFAULT_BORDER_PADDING
                                                             : std::max(0, border_padding);
     const Plan pl = make_plan(n_images, dims, seed_counts, P);
@@ -519,7 +691,7 @@ int idl_triangulate_batch(idl_context* ctx, int n_images, const int32_t* dims, c
     C.have_result = false;
     C.seeds_in.ensure((size_t)pl.n_seeds * 8);
     IDL_CUDA(cudaMemcpyAsync(C.seeds_in.ptr, seeds_xy, (size_t)pl.n_seeds * 8, cudaMemcpyHostToDevice, C.stream));
-    run_batch(C, pl, P, n_images, nullptr, tri_counts_out, timings_out);
+    run_batch(C, pl, P, n_images, nullptr, tri_counts_out, timings_out, false, mode);
     if (grids_out)
         IDL_CUDA(cudaMemcpyAsync(grids_out, C.outgrid.ptr, (size_t)pl.n_px * 12, cudaMemcpyDeviceToHost, C.stream));
     IDL_CUDA(cudaStreamSynchronize(C.stream));
@@ -533,7 +705,8 @@ int idl_triangulate_batch_device(idl_context* ctx, int n_images, const int32_t* 
     IDL_API_BEGIN
     if (!ctx) invalid("context must not be NULL");
     if (!dims || !seed_counts) invalid("dims and seed_counts must not be NULL");
-    if (mode != IDL_MODE_REFERENCE) invalid("batched triangulation supports voronoi_mode 'reference' only");
+    if (mode != IDL_MODE_REFERENCE && mode != IDL_MODE_EXACT)
+        invalid("batched triangulation supports voronoi_mode 'reference' and 'exact'");
     const int P = border_padding == IDL_AUTO_BORDER_PADDING ? IDL_DEFAULT_BORDER_PADDING
                                                             : std::max(0, border_padding);
     const Plan pl = make_plan(n_images, dims, seed_counts, P);
@@ -544,7 +717,7 @@ int idl_triangulate_batch_device(idl_context* ctx, int n_images, const int32_t* 
     C.seeds_in.ensure((size_t)pl.n_seeds * 8);
     IDL_CUDA(cudaMemcpyAsync(C.seeds_in.ptr, d_seeds_xy, (size_t)pl.n_seeds * 8, cudaMemcpyDeviceToDevice,
                              C.stream));
-    run_batch(C, pl, P, n_images, d_grids_out, tri_counts_out, nullptr);
+    run_batch(C, pl, P, n_images, d_grids_out, tri_counts_out, nullptr, false, mode);
     IDL_API_END
 }
 

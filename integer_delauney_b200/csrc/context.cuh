@@ -166,6 +166,7 @@ struct Context {
     DevBuf batch_sid;       // image of each sorted seed
     DevBuf batch_stats;     // per-image triangle counts, longest sides, triangle offsets
     DevBuf batch_bad;       // first out-of-bounds / duplicate seed index
+    DevBuf batch_ximg, batch_colimg, batch_rowimg;  // exact semantics: image table, column / row -> image
 
     DevBuf scalars;       // one Scalars
     Scalars* host_sc = nullptr;  // pinned mirror
@@ -194,7 +195,8 @@ struct Context {
         DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
                          &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &big_tiles, &exact_dy, &hkeys,
                          &hvals, &ukeys, &uvals, &cnt, &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded,
-                         &batch_img, &batch_seed_img, &batch_rows, &batch_sid, &batch_stats, &batch_bad, &scalars};
+                         &batch_img, &batch_seed_img, &batch_rows, &batch_sid, &batch_stats, &batch_bad,
+                         &batch_ximg, &batch_colimg, &batch_rowimg, &scalars};
         for (DevBuf* b : all) f(*b);
     }
     Context()

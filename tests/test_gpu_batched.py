@@ -48,6 +48,30 @@ def test_matches_oracle(cu):
         np.testing.assert_array_equal(v, tris[:, 2:5])
 
 
+@pytest.mark.parametrize("P", [16, 0])
+def test_exact_mode_each_image_equals_single_image_call(cu, P):
+    """Exact semantics over the atlas: each image's nearest-seed search stays
+    inside its own canvas, so every image equals the single-image exact
+    pipeline (and, for the small ones, the oracle)."""
+    imgs = mixed_images()
+    got = cu.triangulate_batch(imgs, P, as_arrays=True, voronoi_mode="exact")
+    for k, ((w, h, s), (v, g)) in enumerate(zip(imgs, got)):
+        v1, g1 = cu.triangulate(w, h, s, P, as_arrays=True, voronoi_mode="exact")
+        np.testing.assert_array_equal(v, v1)
+        np.testing.assert_array_equal(g, g1)
+        if k < 8:
+            tris, grid, _ = oracle.triangulate(w, h, oracle.sort_seeds(s, w, h), P, "exact")
+            np.testing.assert_array_equal(g, grid)
+            np.testing.assert_array_equal(v, tris[:, 2:5])
+    # the configuration's shape: many images of uneven size in one batch
+    imgs = batched_images(64, seed=12)
+    got = cu.triangulate_batch(imgs, P, as_arrays=True, voronoi_mode="exact")
+    for (w, h, s), (v, g) in zip(imgs, got):
+        v1, g1 = cu.triangulate(w, h, s, P, as_arrays=True, voronoi_mode="exact")
+        np.testing.assert_array_equal(v, v1)
+        np.testing.assert_array_equal(g, g1)
+
+
 def test_batched_configuration_sample(cu):
     imgs = batched_images(96, seed=11)
     got = cu.triangulate_batch(imgs, -1, as_arrays=True)
