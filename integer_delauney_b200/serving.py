@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import collections
 import ctypes
+import threading
 import time
 from dataclasses import dataclass
 from typing import Optional
@@ -183,7 +184,9 @@ class Server:
         self.device = torch.cuda.current_device() if device is None else int(device)
         self.budget = int(budget_bytes)
         self.padding = cu.resolve_padding(border_padding)
-        self._dims: dict[int, tuple] = {}
+        self._dims: dict[int, tuple] = {}       # diagram id -> (W, H), for fetched inserts
+        self._dims_lock = threading.Lock()
+        self._news = 0
         h = ctypes.c_void_p()
         _capi.check(self._lib.idl_server_create(self.device, self.budget, int(slots), self.padding,
                                                 _capi.mode_id(mode), ctypes.byref(h)))
@@ -214,7 +217,14 @@ class Server:
         _capi.check(self._lib.idl_server_submit_new(
             self._handle(), int(width), int(height), s.ctypes.data if len(s) else None, len(s), int(fetch),
             grid.ctypes.data if fetch else None, self._arrival_ns(arrival), ctypes.byref(rid), ctypes.byref(did)))
-        self._dims[did.value] = (int(width), int(height))
+        with self._dims_lock:
+            self._dims[did.value] = (int(width), int(height))
+            self._news += 1
+            prune = self._news % 4096 == 0
+        if prune:                               # forget diagrams the server no longer holds
+            live = set(self.resident())
+            with self._dims_lock:
+                self._dims = {k: v for k, v in self._dims.items() if k in live or k >= did.value}
         return Ticket(self, rid.value, did.value, fetch, grid)
 
     def submit_insert(self, diagram_id: int, seeds, fetch: bool = False,
@@ -223,9 +233,11 @@ class Server:
         s = self._cu.parse_seeds(seeds)
         grid = None
         if fetch:
-            if diagram_id not in self._dims:
+            with self._dims_lock:
+                dims = self._dims.get(diagram_id)
+            if dims is None:
                 raise KeyError(f"diagram {diagram_id} is not resident")
-            W, H = self._dims[diagram_id]
+            W, H = dims
             grid = np.empty((H, W, 3), np.int32)
         rid = ctypes.c_int64()
         _capi.check(self._lib.idl_server_submit_insert(
@@ -268,7 +280,8 @@ class Server:
         ok = ctypes.c_int(0)
         _capi.check(self._lib.idl_server_recycle(self._handle(), int(diagram_id), ctypes.byref(ok)))
         if ok.value:
-            self._dims.pop(int(diagram_id), None)
+            with self._dims_lock:
+                self._dims.pop(int(diagram_id), None)
         return bool(ok.value)
 
     @staticmethod
