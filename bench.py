@@ -35,7 +35,6 @@ import gc
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time

@@ -27,7 +27,6 @@ from __future__ import annotations
 import collections
 import ctypes
 import threading
-import time
 from dataclasses import dataclass
 from typing import Optional
 
