@@ -247,6 +247,11 @@ int main()
         std::fprintf(stderr, "%d checks failed\n", failures);
         return 1;
     }
+    // the figures the Python layer mirrors (serving.slot_reserve, estimate_bytes(workspace=False))
+    std::printf("slot_reserve %d %lld\n", 16, (long long)slot_reserve(16));
+    std::printf("slot_reserve %d %lld\n", 0, (long long)slot_reserve(0));
+    std::printf("fresh %d %d %lld %d %lld\n", 300, 200, 5000LL, 16, (long long)capacity(300, 200, 5000, 16).bytes());
+    std::printf("fresh %d %d %lld %d %lld\n", 4096, 17, 1LL, 0, (long long)capacity(4096, 17, 1, 0).bytes());
     std::printf("scheduler: all checks passed\n");
     return 0;
 }

@@ -20,3 +20,12 @@ def test_scheduler_policy(tmp_path):
     out = subprocess.run([exe], capture_output=True, text=True, timeout=60)
     assert out.returncode == 0, out.stderr
     assert "all checks passed" in out.stdout
+    # the Python layer's budget figures equal the scheduler's
+    from integer_delauney_b200.serving import estimate_bytes, slot_reserve
+    for line in out.stdout.splitlines():
+        f = line.split()
+        if f[0] == "slot_reserve":
+            assert slot_reserve(int(f[1])) == int(f[2])
+        elif f[0] == "fresh":
+            W, H, n, P, want = map(int, f[1:])
+            assert estimate_bytes(W, H, n, P, workspace=False) == want
