@@ -23,9 +23,13 @@ against the server, and a fixed prefix against the plain serial loop).
 Multi-GPU (torchrun): every rank triangulates its own image per step (replicas,
 no collective on the data path); the time is the max over ranks.
 
-`--impl reference` times the reference algorithm on the host CPU cores (the
-oracle port of src/cuda/voronoi.cu + triangulation.cu, OpenMP) on a bounded
-sample of the same workload, on rank 0 only.
+`--impl reference` times the reference's own CUDA triangulate, compiled from
+its sources for sm_100a (oracle/_ref), through its stock host path on the same
+full workload, on rank 0 only (the oracle port on the host cores if that build
+is absent).  The same measurement appears on this arm's line as `ref_cuda`,
+beside `cpu_baseline` (the oracle port on all host cores: the 512 x 512 CPU
+configuration measured outright, the 4096 x 4096 image extrapolated from a
+sample of assignment rows and marked so).
 """
 from __future__ import annotations
 
@@ -142,9 +146,12 @@ class ClockSampler:
 
 
 def cpu_baseline(sample_rows: int = 0):
-    """Reference algorithm on the host cores: full Jacobi + detection on the
-    padded canvas, the reference's per-pixel assignment on a sample of rows,
-    extrapolated to the image.  Returns (Mpix/s, seconds, description)."""
+    """The reference algorithm on the host cores (the oracle port of
+    src/cuda/voronoi.cu + triangulation.cu, OpenMP): full Jacobi + detection
+    on the padded 4096 x 4096 canvas, the reference's per-pixel assignment on
+    a sample of rows, extrapolated to the image; and the whole pipeline,
+    measured outright, on the 512 x 512 / 2 000-seed CPU configuration.
+    Returns the cpu_baseline object."""
     import oracle
     from integer_delauney_b200.workloads import uniform
 
@@ -166,31 +173,86 @@ def cpu_baseline(sample_rows: int = 0):
     t3 = time.perf_counter()
     est = (t1 - t0) + (t2 - t1) + (t3 - t2) * (H / rows)
     desc = (f"oracle port, {threads} threads: full Jacobi ({passes} passes) + detection on the "
-            f"{Wd}x{Hd} canvas, reference per-pixel assignment on {rows} of {H} rows "
-            f"(extrapolated); measured {t3 - t0:.1f} s")
-    return W * H / est / 1e6, est, desc, threads
+            f"{Wd}x{Hd} canvas, reference per-pixel assignment on {rows} of {H} rows, extrapolated to "
+            f"{H} rows")
+    # the CPU configuration, whole pipeline, no extrapolation
+    c1 = oracle.sort_seeds(uniform(512, 512, 2000, seed=0), 512, 512)
+    c1_s = []
+    for _ in range(3):
+        t = time.perf_counter()
+        oracle.triangulate(512, 512, c1, PADDING, "reference")
+        c1_s.append(time.perf_counter() - t)
+    c1_t = statistics.median(c1_s)
+    return {"value": W * H / est / 1e6, "unit": "Mpixel/s", "cores": threads, "kind": "port", "sample": desc,
+            "extrapolated": True, "estimated_s": est, "measured_s": t3 - t0,
+            "cpu_config": {"workload": f"triangulate 512x512, 2000 uniform seeds, P={PADDING}, whole pipeline "
+                                       f"measured", "s": c1_t, "mpix_s": 512 * 512 / c1_t / 1e6}}
+
+
+def ref_cuda_baseline(seeds: np.ndarray, reps: int, warmup: int = 1):
+    """The reference's own CUDA triangulate compiled from its sources for
+    sm_100a (oracle/_ref/libref_cuda.so, built by oracle/build_ref.sh): its
+    stock path (src/cuda/bindings/triangulate.hpp:15-43 -> triangulation.cu:
+    143-365) with host seeds in and the (H, W, 3) grid and triangles out, on
+    this GPU and one host core, wall clock per call (the path synchronises
+    itself).  Returns (ms per call list, triangle count) or None when the
+    library was not built."""
+    import oracle
+    if not oracle.ref_available():
+        return None
+    for _ in range(warmup):
+        oracle.ref_triangulate_stock(W, H, seeds, PADDING)
+    ms = []
+    n_tri = 0
+    for _ in range(reps):
+        t = time.perf_counter()
+        tris, _ = oracle.ref_triangulate_stock(W, H, seeds, PADDING)
+        ms.append((time.perf_counter() - t) * 1e3)
+        n_tri = len(tris)
+    return ms, n_tri
+
+
+REF_CUDA_DESC = ("the reference's own triangulate compiled from its sources for sm_100a "
+                 "(src/cuda/voronoi.cu + triangulation.cu via its stock host path): host loops on one "
+                 "core, kernels on this GPU; host seeds in, (H, W, 3) grid and triangles out; wall clock")
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's own CUDA path on the full
+    4096 x 4096 / 200 000-seed workload, every step measured (no sample);
+    the oracle port on the host cores when the reference build is absent."""
     if rank != 0:
         return
-    for _ in range(args.warmup):
-        cpu_baseline(args.ref_rows)
-    vals, secs = [], []
-    desc, threads = "", 0
-    for _ in range(args.steps):
-        v, est, desc, threads = cpu_baseline(args.ref_rows)
-        vals.append(v)
-        secs.append(est)
-    value = statistics.median(vals)
+    from integer_delauney_b200.workloads import uniform
+    seeds = uniform(W, H, N_SEEDS, seed=0)
+    r = ref_cuda_baseline(seeds, args.steps, args.warmup)
+    if r is not None:
+        ms_list, n_tri = r
+        ms = statistics.median(ms_list)
+        value = W * H / (ms / 1e3) / 1e6
+        base = {"value": value, "unit": "Mpixel/s", "cores": 1, "kind": "reference",
+                "sample": f"full workload every step ({args.steps} steps); " + REF_CUDA_DESC,
+                "ms_per_call": ms_list, "triangles": n_tri}
+    else:
+        vals, secs = [], []
+        base = {}
+        for _ in range(args.warmup):
+            cpu_baseline(args.ref_rows)
+        for _ in range(args.steps):
+            base = cpu_baseline(args.ref_rows)
+            vals.append(base["value"])
+            secs.append(base["estimated_s"])
+        value = statistics.median(vals)
+        ms = statistics.median(secs) * 1e3
+        base["value"] = value
     line = {
         "metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": statistics.median(secs) * 1e3, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "impl": "reference",
         "config": {"workload": f"triangulate {W}x{H}, {N_SEEDS} uniform seeds, P={PADDING}, reference mode",
                    "parallelism": f"replicas x{world}"},
-        "cpu_baseline": {"value": value, "unit": "Mpixel/s", "cores": threads, "kind": "port", "sample": desc},
+        "cpu_baseline": base,
         "e2e": {"value": value, "unit": "Mpixel/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -648,10 +710,18 @@ def run_ours(args, rank, world):
 
     if rank != 0:
         return
-    base = None
+    base = ref_cuda = None
     if not args.no_cpu_baseline:
-        v, est, desc, threads = cpu_baseline(args.ref_rows)
-        base = {"value": v, "unit": "Mpixel/s", "cores": threads, "kind": "port", "sample": desc}
+        base = cpu_baseline(args.ref_rows)
+        r = ref_cuda_baseline(seeds_u, 3)
+        if r is not None:
+            ms_r = statistics.median(r[0])
+            ref_cuda = {"ms_per_call": ms_r, "mpix_s": W * H / (ms_r / 1e3) / 1e6, "calls": r[0],
+                        "triangles": r[1], "what": REF_CUDA_DESC,
+                        "ratio_e2e": (ms_r / (ms_e / e_steps)), "ratio_device": ms_r / (ms / args.steps)}
+    if srv is not None:
+        for k in ("realtime", "realtime_500"):
+            print(json.dumps({"serving_" + k + "_slowest": srv[k].pop("slowest")}), file=sys.stderr, flush=True)
     line = {
         "metric": METRIC, "value": value, "unit": "Mpixel/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -682,6 +752,7 @@ def run_ours(args, rank, world):
         "gpu_launches": int(launches),
         "clocks": clocks,
         "cpu_baseline": base,
+        "ref_cuda": ref_cuda,
     }
     print(json.dumps(line), flush=True)
 

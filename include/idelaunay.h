@@ -83,6 +83,21 @@ IDL_API const char* idl_last_error(void);
 IDL_API int idl_version(void);
 /* Number of CUDA kernels this library has launched in this process. */
 IDL_API long long idl_launch_count(void);
+/* Number of device and pinned host allocations (cudaMalloc, cudaMallocAsync,
+ * cudaMallocHost) this library has made in this process. */
+IDL_API long long idl_alloc_count(void);
+
+/* Failure detection self-test.  No counterpart in the reference, whose BFS
+ * loop has no device-side wait.  Runs the grid-wide barrier of the persistent
+ * propagation kernel on its own (one block per SM, four barriers, on the
+ * context's stream) with at most `spin_limit` polls per wait (1..2^24), waiting
+ * for `missing_arrivals` (0..1024) blocks more than the grid holds.  With 0
+ * every barrier completes: IDL_OK.  With more, the arrivals never come, every
+ * block's wait runs out, the kernel raises its error flag and returns, and the
+ * call reports IDL_ERR_INTERNAL "grid barrier timed out" -- the status the
+ * propagation entry points return on a barrier timeout; the context stays
+ * usable. */
+IDL_API int idl_selftest_grid_barrier(idl_context* ctx, int missing_arrivals, unsigned int spin_limit);
 
 /* ---- context: device, stream, persistent workspace ------------------ */
 /* The reference allocates and frees device buffers on every call
@@ -191,8 +206,11 @@ IDL_API int idl_triangles_device(idl_context* ctx, const int32_t** d_tris, const
  * embed the library under an allocator of their own.  Same result as
  * idl_voronoi, but with device pointers, on `stream` (a cudaStream_t, NULL =
  * legacy default stream) and the current device, and all workspace taken
- * from one static device array of about 9.8 MB that every GPU loading the
- * library reserves until the process exits.
+ * from one static device array of about 9.8 MB, which a GPU holds from the
+ * first call on it (when lazy module loading, the CUDA default, loads the
+ * array's module there; at context creation under CUDA_MODULE_LOADING=EAGER)
+ * until the process exits.  That first call therefore does commit device
+ * memory and can fail under an exhausted quota: make it at set-up.
  *   limits   width, height <= 1024 and n_seeds <= 65536 (larger is rejected
  *            with IDL_ERR_INVALID); modes IDL_MODE_REFERENCE, IDL_MODE_NUMPY.
  *   d_seeds_xy  device n_seeds * 2 int32, any order.

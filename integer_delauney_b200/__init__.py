@@ -3,8 +3,10 @@
 Mirrors src/delauney/__init__.py of timdahmen/integer_delauney: the same
 public names, with the CUDA classes resolved lazily from ``_delauney_cuda`` so
 that importing the package works on a machine without a GPU.  A caller of the
-reference switches with ``import integer_delauney_b200 as delauney`` (or by
-aliasing the module name).
+reference switches with ``import integer_delauney_b200 as delauney``, or by
+registering this package and its ``_delauney_cuda`` module under the names
+``delauney`` and ``delauney._delauney_cuda`` in ``sys.modules`` before the
+first import.
 """
 from __future__ import annotations
 

@@ -44,6 +44,8 @@ SIGNATURES = {
     "idl_last_error": (ctypes.c_char_p, []),
     "idl_version": (_i32, []),
     "idl_launch_count": (ctypes.c_longlong, []),
+    "idl_alloc_count": (ctypes.c_longlong, []),
+    "idl_selftest_grid_barrier": (_i32, [_vp, _i32, ctypes.c_uint]),
     "idl_context_create": (_i32, [_i32, ctypes.POINTER(_vp)]),
     "idl_context_destroy": (_i32, [_vp]),
     "idl_context_set_stream": (_i32, [_vp, _vp]),

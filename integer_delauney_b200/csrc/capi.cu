@@ -14,10 +14,12 @@ namespace idl {
 namespace {
 thread_local std::string g_last_error;
 std::atomic<long long> g_launches{0};
+std::atomic<long long> g_allocs{0};
 }
 
 void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_alloc() { g_allocs.fetch_add(1, std::memory_order_relaxed); }
 
 size_t Context::workspace_bytes() const
 {
@@ -46,7 +48,10 @@ Context::~Context()
 void ensure_scalars(Context& C)
 {
     C.scalars.ensure(sizeof(Scalars));
-    if (!C.host_sc) IDL_CUDA(cudaMallocHost(reinterpret_cast<void**>(&C.host_sc), sizeof(Scalars)));
+    if (!C.host_sc) {
+        count_alloc();
+        IDL_CUDA(cudaMallocHost(reinterpret_cast<void**>(&C.host_sc), sizeof(Scalars)));
+    }
 }
 
 namespace {
@@ -278,6 +283,17 @@ const char* idl_last_error(void) { return g_last_error.c_str(); }
 int idl_version(void) { return 100; }
 
 long long idl_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+long long idl_alloc_count(void) { return g_allocs.load(std::memory_order_relaxed); }
+
+int idl_selftest_grid_barrier(idl_context* ctx, int missing_arrivals, unsigned int spin_limit)
+{
+    IDL_API_BEGIN
+    if (!ctx) invalid("context must not be NULL");
+    DeviceGuard g(ctx->device);
+    grid_barrier_selftest(*ctx, missing_arrivals, spin_limit);
+    IDL_API_END
+}
 
 int idl_context_create(int device, idl_context** out)
 {

@@ -46,6 +46,9 @@ inline void cuda_check(cudaError_t err, const char* expr, const char* file, int 
 namespace idl {
 // Kernels this library has launched in this process (idl_launch_count()).
 void count_launch();
+// Device and pinned host allocations this library has made in this process
+// (idl_alloc_count()).
+void count_alloc();
 }  // namespace idl
 
 #define IDL_CUDA(expr) ::idl::cuda_check((expr), #expr, __FILE__, __LINE__)

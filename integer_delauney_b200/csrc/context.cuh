@@ -46,6 +46,7 @@ struct DevBuf {
         grow = (grow + 255) / 256 * 256;
         drop();
         if (need == 0) return;
+        count_alloc();
         if (stream) {
             IDL_CUDA(cudaMallocAsync(&ptr, grow, *stream));
             async = true;
@@ -272,6 +273,12 @@ int64_t propagate_sparse_from_tiles(Context& C, const Canvas& cv, const uint32_t
 int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
                               int64_t n_new, const int32_t* big_list, int n_big, int big_tiles_x, int sub_x,
                               int sub_y);
+
+// Run the persistent kernel's grid barrier alone (sparse_jacobi.cu) on one
+// block per SM, waiting for `missing_arrivals` more blocks than the grid has,
+// with at most `spin_limit` polls per wait.  Throws IDL_ERR_INTERNAL ("grid
+// barrier timed out") when a wait ran out, exactly as propagation reports it.
+void grid_barrier_selftest(Context& C, int missing_arrivals, unsigned spin_limit);
 
 // Stage (a), exact semantics (exact.cu): nearest seed, ties to the higher id,
 // for the n (x, y)-sorted seeds `pos` of the canvas; labels into C.lab[0]

@@ -742,6 +742,7 @@ int idl_delaunay_create(int device, int width, int height, int64_t max_seeds, in
         d->tgrid_bytes = (size_t)Wd * Hd * sizeof(int32_t);
         d->pix_bytes = (size_t)width * height * 9;
         d->seed_cap = max_seeds;
+        for (int k = 0; k < 4; ++k) count_alloc();
         IDL_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d->planes), d->planes_bytes, d->stream));
         IDL_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&d->tgrid), d->tgrid_bytes, d->stream));
         IDL_CUDA(cudaMallocAsync(&d->pixmem, d->pix_bytes, d->stream));

@@ -11,9 +11,15 @@
 // How.  All workspace of the stage-(a) pipeline (seed ordering bitmap and
 // scans, sorted seed tables, both label planes, the propagation work lists,
 // bitmaps, counters and barrier state) is carved out of one file-scope
-// `static __device__` array of NA_SCRATCH_BYTES.  The loader reserves it
-// on every GPU that loads this library, for the life of the process.  The
-// caller passes the seeds and the output grid in device memory.
+// `static __device__` array of NA_SCRATCH_BYTES.  The caller passes the seeds
+// and the output grid in device memory.  A GPU holds the array from the moment
+// this file's module is loaded on it until the process exits.  Under CUDA's
+// lazy module loading (the default since CUDA 12.2) that moment is the first
+// call of this entry point on the device: its cudaGetSymbolAddress loads the
+// module and commits the array, so that one call does take device memory and
+// can fail if a quota is already used up.  Make it at set-up, outside any
+// quota- or latency-critical section, or run with CUDA_MODULE_LOADING=EAGER
+// to commit the array when the context is created.
 //
 // Set-up.  The array's name is only a host-side stand-in in host code, so the
 // device address is fetched with cudaGetSymbolAddress, once per device, with
@@ -57,7 +63,7 @@ constexpr size_t NA_SCRATCH_BYTES =
 }  // namespace
 }  // namespace idl
 
-// The workspace itself (about 9.8 MB), reserved on every device that loads the library.
+// The workspace itself (about 9.8 MB); a device holds it once this module is loaded there.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[idl::NA_SCRATCH_BYTES];
 
 namespace idl {

@@ -50,9 +50,11 @@ struct GridSync {
     int passes;   // passes run (the last one changed nothing)
 };
 
-// Grid-wide barrier with a bounded wait.  On timeout the error flag is raised
-// and every block leaves the kernel, so a bug cannot hang the GPU.
-__device__ __forceinline__ bool grid_sync(GridSync* gs, unsigned nblocks, unsigned& gen_local)
+// Grid-wide barrier with a bounded wait: at most `spin_limit` polls per
+// block.  On timeout the error flag is raised and every block leaves the
+// kernel, so a bug cannot hang the GPU.
+__device__ __forceinline__ bool grid_sync(GridSync* gs, unsigned nblocks, unsigned& gen_local,
+                                          unsigned spin_limit = SPIN_LIMIT)
 {
     __shared__ int s_ok;
     __syncthreads();
@@ -67,7 +69,7 @@ __device__ __forceinline__ bool grid_sync(GridSync* gs, unsigned nblocks, unsign
         } else {
             unsigned spins = 0;
             while (gen.load(cuda::memory_order_acquire) != target) {
-                if (++spins > SPIN_LIMIT) {
+                if (++spins > spin_limit) {
                     err.fetch_or(1, cuda::memory_order_relaxed);
                     ok = 0;
                     break;
@@ -278,6 +280,18 @@ k_sparse_jacobi(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, con
     if (blockIdx.x == 0 && threadIdx.x == 0) gs->passes = t;
 }
 
+// The barrier above on its own: `rounds` barriers of a grid that waits for
+// `expected` arrivals.  With expected > gridDim.x some arrivals never come, so
+// every block's wait runs out after spin_limit polls and the error flag is set.
+__global__ void k_barrier_selftest(GridSync* gs, unsigned expected, unsigned spin_limit, int rounds)
+{
+    unsigned gen_local = 0;
+    int r = 0;
+    for (; r < rounds; ++r)
+        if (!grid_sync(gs, expected, gen_local, spin_limit)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) gs->passes = r;
+}
+
 // Work-list entries are micro-tile coordinates packed as mx | my << 16.
 __device__ __forceinline__ int32_t pack_mt(int mx, int my) { return mx | (my << 16); }
 
@@ -338,6 +352,27 @@ __global__ void k_expand_tiles(const int32_t* __restrict__ big, int big_tiles_x,
 }
 
 }  // namespace
+
+void grid_barrier_selftest(Context& C, int missing_arrivals, unsigned spin_limit)
+{
+    if (missing_arrivals < 0 || missing_arrivals > 1024) invalid("missing_arrivals must be in [0, 1024]");
+    if (spin_limit < 1 || spin_limit > SPIN_LIMIT) invalid("spin_limit must be in [1, 2^24]");
+    constexpr int rounds = 4;
+    C.gsync.ensure(sizeof(GridSync));
+    GridSync* gs = C.gsync.as<GridSync>();
+    IDL_CUDA(cudaMemsetAsync(gs, 0, sizeof(GridSync), C.stream));
+    unsigned expected = (unsigned)C.num_sms + (unsigned)missing_arrivals;
+    int r = rounds;
+    void* args[] = {&gs, &expected, &spin_limit, &r};
+    IDL_CUDA(cudaLaunchCooperativeKernel((const void*)k_barrier_selftest, dim3(C.num_sms), dim3(128), args, 0,
+                                         C.stream));
+    count_launch();
+    GridSync h{};
+    IDL_CUDA(cudaMemcpyAsync(&h, gs, sizeof(GridSync), cudaMemcpyDeviceToHost, C.stream));
+    IDL_CUDA(cudaStreamSynchronize(C.stream));
+    if (h.error) throw Error(IDL_ERR_INTERNAL, "grid barrier timed out");
+    if (h.passes != rounds) throw Error(IDL_ERR_INTERNAL, "grid barrier self-test did not complete its rounds");
+}
 
 int64_t propagate_sparse_from_tiles(Context& C, const Canvas& cv, const uint32_t* pos, const int32_t* big_list,
                                     int n_big, int big_tiles_x, int big_w, int big_h)

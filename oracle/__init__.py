@@ -337,3 +337,129 @@ def ref_triangulate(W: int, H: int, sorted_seeds, P: int = DEFAULT_BORDER_PADDIN
         if rc != 0:
             raise RuntimeError(_ref().ref_last_error().decode())
         return tris[:n.value].copy(), out, pad
+
+
+def _ref_dl_lib():
+    L = _ref()
+    if not getattr(L, "_idl_dl_bound", False):
+        vp = ctypes.c_void_p
+        L.ref_dl_create.restype = vp
+        L.ref_dl_create.argtypes = [ctypes.c_int] * 4
+        L.ref_dl_destroy.restype = None
+        L.ref_dl_destroy.argtypes = [vp]
+        L.ref_dl_seed_count.restype = ctypes.c_int
+        L.ref_dl_seed_count.argtypes = [vp]
+        L.ref_dl_insert_deferred.restype = ctypes.c_int
+        L.ref_dl_insert_deferred.argtypes = [vp, _i32p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.ref_dl_finalise.restype = ctypes.c_int
+        L.ref_dl_finalise.argtypes = [vp, _i32p, _i32p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+        L.ref_dl_voronoi_grid.restype = ctypes.c_int
+        L.ref_dl_voronoi_grid.argtypes = [vp, _i32p]
+        L.ref_dl_triangles.restype = ctypes.c_int
+        L.ref_dl_triangles.argtypes = [vp, _i32p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+        L.ref_dl_sorted_rank.restype = ctypes.c_int
+        L.ref_dl_sorted_rank.argtypes = [vp, _i32p]
+        L._idl_dl_bound = True
+    return L
+
+
+class RefDelaunay:
+    """The reference's own incremental ``Delaunay`` class (src/cuda/delaunay.cuh),
+    run on the GPU through oracle/_ref/libref_cuda.so.
+
+    Seeds are passed in insertion order, exactly as the reference binding
+    (src/cuda/bindings/py_delaunay.hpp) hands them to ``insert_deferred``.
+    """
+
+    def __init__(self, W: int, H: int, max_seeds: int, P: int = DEFAULT_BORDER_PADDING):
+        self.W, self.H = int(W), int(H)
+        self._L = _ref_dl_lib()
+        self._h = self._L.ref_dl_create(self.W, self.H, int(max_seeds), int(P))
+        if not self._h:
+            raise RuntimeError(self._L.ref_last_error().decode())
+
+    def close(self):
+        if self._h:
+            self._L.ref_dl_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _check(self, rc):
+        if rc == 1:
+            raise RuntimeError(self._L.ref_last_error().decode())
+        return rc
+
+    @property
+    def seed_count(self) -> int:
+        return int(self._L.ref_dl_seed_count(self._h))
+
+    def insert_deferred(self, seeds) -> int:
+        """Returns the Jacobi passes the reference ran for this batch."""
+        s = np.ascontiguousarray(np.asarray(seeds, dtype=np.int32).reshape(-1, 2))
+        it = ctypes.c_int(0)
+        self._check(self._L.ref_dl_insert_deferred(self._h, s, len(s), ctypes.byref(it)))
+        return int(it.value)
+
+    def _tris(self, fn, *head):
+        cap = 4 * max(self.seed_count, 1) + 64
+        while True:
+            out = np.empty((cap, 5), dtype=np.int32)
+            n = ctypes.c_int64(0)
+            rc = self._check(fn(self._h, *head, out, cap, ctypes.byref(n)))
+            if rc == 2:
+                cap = int(n.value)
+                continue
+            return out[:n.value].copy()
+
+    def finalise(self):
+        """(tris (N_tri, 5) int32 in the reference's slot order, grid (H, W, 3))."""
+        grid = np.empty((self.H, self.W, 3), dtype=np.int32)
+        tris = self._tris(self._L.ref_dl_finalise, grid)
+        return tris, grid
+
+    def insert(self, seeds):
+        self.insert_deferred(seeds)
+        return self.finalise()
+
+    def get_voronoi_grid(self) -> np.ndarray:
+        out = np.empty((self.H, self.W, 2), dtype=np.int32)
+        self._check(self._L.ref_dl_voronoi_grid(self._h, out))
+        return out
+
+    def get_triangles(self) -> np.ndarray:
+        """(N_tri, 5): canonical (x, y) in image coordinates and insertion ids."""
+        return self._tris(self._L.ref_dl_triangles)
+
+    @property
+    def sorted_rank(self) -> np.ndarray:
+        out = np.empty(self.seed_count, dtype=np.int32)
+        self._check(self._L.ref_dl_sorted_rank(self._h, out))
+        return out
+
+
+def ref_triangulate_stock(W: int, H: int, seeds, P: int = DEFAULT_BORDER_PADDING):
+    """The reference's stock triangulate() on the GPU: host validation and
+    (x, y) sort, then cuda_compute_triangulation building its own padded
+    diagram (src/cuda/bindings/triangulate.hpp:15-43).  Seeds in caller order.
+    Returns (tris (N, 5) int32, grid (H, W, 3) int32)."""
+    L = _ref()
+    if not getattr(L, "_idl_stock_bound", False):
+        L.ref_triangulate_stock.restype = ctypes.c_int
+        L.ref_triangulate_stock.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int,
+                                            _i32p, _i32p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]
+        L._idl_stock_bound = True
+    s = np.ascontiguousarray(np.asarray(seeds, dtype=np.int32).reshape(-1, 2))
+    out = np.empty((H, W, 3), dtype=np.int32)
+    cap = 4 * len(s) + 64
+    while True:
+        tris = np.empty((cap, 5), dtype=np.int32)
+        n = ctypes.c_int64(0)
+        rc = L.ref_triangulate_stock(W, H, s, len(s), int(P), out, tris, cap, ctypes.byref(n))
+        if rc == 2:
+            cap = int(n.value)
+            continue
+        if rc != 0:
+            raise RuntimeError(L.ref_last_error().decode())
+        return tris[:n.value].copy(), out

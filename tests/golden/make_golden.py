@@ -74,6 +74,16 @@ TRI_CASES = [
 ]
 
 
+def reference_root() -> str:
+    """The reference source tree: $IDL_REFERENCE_SRC, else BASELINE.json's reference_path."""
+    env = os.environ.get("IDL_REFERENCE_SRC")
+    if env:
+        return env
+    import json
+    with open(os.path.join(HERE, "..", "..", "BASELINE.json")) as f:
+        return json.load(f)["reference_path"]
+
+
 def main(src):
     sys.path.insert(0, src)
     from delauney.reference.voronoi import Voronoi
@@ -103,4 +113,4 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(reference_root(), "src"))

@@ -6,8 +6,10 @@ held to a fixed device-memory quota or pool, hosts embedding the library under
 their own allocator.  Its workspace is one static device array shared by every
 call, so this checks, through the C ABI, that two calls in a row on different
 inputs each reproduce what the ordinary entry point (idl_voronoi, via
-Voronoi().compute) returns, bit for bit -- the second call must not see
-anything the first one left in the shared array.
+Voronoi().compute) and the CPU oracle return, bit for bit -- the second call
+must not see anything the first one left in the shared array -- and that
+once the device's array is set up a call makes no allocation at all (the
+library's own allocation counter, idl_alloc_count, does not move).
 
 Kept in a file of its own that pytest collects last, so that a run stopping at
 the first failure has already run every other test; it passes alone in a fresh
@@ -18,6 +20,7 @@ import ctypes
 import numpy as np
 import pytest
 
+import oracle
 from tests.conftest import random_seeds
 
 pytestmark = pytest.mark.gpu
@@ -41,12 +44,18 @@ def _noalloc(W, H, seeds, mode):
 
 @pytest.mark.parametrize("mode", ["reference", "numpy"])
 def test_noalloc_matches_voronoi_on_two_calls_in_a_row(mode):
+    lib = _capi.load()
     cases = [(512, 512, 2000, 0), (300, 200, 900, 1)]   # the second call is smaller than the first
-    for W, H, n, seed in cases:
+    for i, (W, H, n, seed) in enumerate(cases):
         seeds = random_seeds(W, H, n, seed)
-        got, passes = _noalloc(W, H, seeds, mode)
         want = cu.Voronoi().compute(W, H, seeds, voronoi_mode=mode)
+        a0 = lib.idl_alloc_count()
+        got, passes = _noalloc(W, H, seeds, mode)
+        if i > 0:       # the first call on a device may set up its workspace view
+            assert lib.idl_alloc_count() == a0, "the no-allocation entry point allocated"
         np.testing.assert_array_equal(got, want)
+        o, _ = oracle.voronoi(mode, W, H, oracle.sort_seeds(seeds, W, H))
+        np.testing.assert_array_equal(got, o)
         assert passes >= 1
 
 
