@@ -731,7 +731,8 @@ def run_ours(args, rank, world):
                    "global_batch": world, "parallelism": f"replicas x{world}",
                    "l2": "working set > L2 (label planes 2 x 68 MB, output 201 MB); no flush"},
         "stages_ms": {k[:-3]: round(v, 4) for k, v in stage.items()},
-        "propagation": {"schedule_dense_rounds": schedule, "passes": p0["passes"], "rounds": p0["rounds"],
+        "propagation": {"schedule_dense_rounds": schedule[0], "tile_shape": schedule[1], "passes": p0["passes"],
+                        "rounds": p0["rounds"],
                         "tiles": p0["tiles"],
                         "tile": [p0["tile_w"], p0["tile_h"]], "steps_per_round": p0["steps_per_round"]},
         "roofline": {"bound": "hbm", "kernel": dom_kernel[:-3], "achieved": achieved, "peak": hbm,

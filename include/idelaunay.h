@@ -112,8 +112,8 @@ IDL_API int idl_context_synchronize(idl_context* ctx);
 IDL_API int idl_context_workspace_bytes(idl_context* ctx, int64_t* bytes_out);
 
 /* Propagation schedule from scratch (reference semantics): the first
- * `dense_rounds` rounds of 8 passes run as tile rounds (one HBM round trip per
- * 8 passes over every tile that can change), the rest in the persistent
+ * `dense_rounds` tile rounds (one HBM round trip per round of several passes,
+ * over every tile that can change; see idl_context_set_tile), the rest in the persistent
  * sparse kernel; 0 = sparse kernel only, < 0 = tile rounds to convergence.
  * A continued propagation (an incremental object's insert using this context)
  * runs in the sparse kernel, or with dense_rounds < 0 as tile rounds starting
@@ -121,6 +121,15 @@ IDL_API int idl_context_workspace_bytes(idl_context* ctx, int64_t* bytes_out);
  * time does.  Default 1.  No counterpart in the reference (its schedule is
  * one full pass per launch). */
 IDL_API int idl_context_set_schedule(idl_context* ctx, int dense_rounds);
+
+/* Tile shape of a from-scratch propagation's tile rounds (reference
+ * semantics), as an index: 0 = 48 x 48 cells advanced 8 passes per round
+ * (default), 1 = 48 x 112 / 8 passes, 2 = 56 x 56 / 4 passes,
+ * 3 = 40 x 104 / 12 passes.  Results do not depend on it, only the time does.
+ * *n_shapes_out (may be NULL) receives the number of shapes; an index outside
+ * [0, n) is IDL_ERR_INVALID.  No counterpart in the reference (fixed 16 x 16
+ * blocks, one pass per launch, src/cuda/voronoi.cu:97-98). */
+IDL_API int idl_context_set_tile(idl_context* ctx, int shape, int* n_shapes_out);
 
 /* Record per-stage CUDA events on the context's stream for every following
  * triangulation call (off by default; the reference's PhaseTimer,

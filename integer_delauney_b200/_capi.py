@@ -51,6 +51,7 @@ SIGNATURES = {
     "idl_context_set_stream": (_i32, [_vp, _vp]),
     "idl_context_synchronize": (_i32, [_vp]),
     "idl_context_set_schedule": (_i32, [_vp, _i32]),
+    "idl_context_set_tile": (_i32, [_vp, _i32, ctypes.POINTER(_i32)]),
     "idl_context_workspace_bytes": (_i32, [_vp, _pi64]),
     "idl_context_set_profiling": (_i32, [_vp, _i32]),
     "idl_context_last_profile": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _i32]),
@@ -192,6 +193,12 @@ class Context:
     def set_schedule(self, dense_rounds: int) -> None:
         """Propagation schedule from scratch (idl_context_set_schedule)."""
         check(self._lib.idl_context_set_schedule(self.handle, int(dense_rounds)))
+
+    def set_tile(self, shape: int) -> int:
+        """Tile shape of the tile rounds (idl_context_set_tile); returns the number of shapes."""
+        n = _i32(0)
+        check(self._lib.idl_context_set_tile(self.handle, int(shape), ctypes.byref(n)))
+        return int(n.value)
 
     def set_profiling(self, enable: bool) -> None:
         check(self._lib.idl_context_set_profiling(self.handle, 1 if enable else 0))

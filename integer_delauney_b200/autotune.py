@@ -1,15 +1,25 @@
-"""Autotuning of the propagation schedule.
+"""Autotuning of the propagation schedule and tile shape.
 
 From scratch, the reference-semantics propagation runs its first passes as
-tile rounds (8 passes per HBM round trip over every tile that can still
-change) and hands the tail to the persistent sparse kernel
-(idl_context_set_schedule).  Where the switch pays depends on the seed
-density and layout: dense, uniform seed sets change most of the canvas for
-the first few passes, clustered ones leave long thin fronts.  ``tune`` times
-one representative input under each candidate schedule on the device and
-keeps the fastest for that input's class (canvas size and density, both on a
-log scale), so a stream of similar inputs is tuned once.  Every schedule gives
-the same result bit for bit; only the time differs.
+tile rounds (several passes per HBM round trip over every tile that can still
+change) and hands the tail to the persistent sparse kernel.  Two knobs decide
+its speed, never its result:
+
+* the schedule (idl_context_set_schedule): how many tile rounds run before the
+  sparse kernel takes over (0 = sparse kernel only, -1 = tile rounds to
+  convergence);
+* the tile shape (idl_context_set_tile): the inner tile of a round and the
+  passes it advances per round trip (48 x 48 / 8, 48 x 112 / 8, 56 x 56 / 4,
+  40 x 104 / 12).  Larger tiles waste less work on halos, more passes per round
+  trip suit thin fronts crossing empty space, fewer suit dense seed sets.
+
+Where each pays depends on the seed density and layout: dense, uniform seed
+sets change most of the canvas for the first few passes, clustered ones leave
+long thin fronts.  ``tune`` times one representative input under every
+candidate (schedule, shape) on the device and keeps the fastest for that
+input's class (canvas size and density, both on a log scale), so a stream of
+similar inputs is tuned once.  Every candidate gives the same result bit for
+bit; only the time differs.
 """
 from __future__ import annotations
 
@@ -20,8 +30,8 @@ import numpy as np
 
 from . import _capi
 
-CANDIDATES = (0, 1, 2, 3)
-_cache: dict[tuple, int] = {}
+SCHEDULES = (0, 1, 2, 3, -1)
+_cache: dict[tuple, tuple[int, int]] = {}
 
 
 def input_class(width: int, height: int, n_seeds: int) -> tuple:
@@ -31,10 +41,25 @@ def input_class(width: int, height: int, n_seeds: int) -> tuple:
     return (int(math.log2(px)), int(math.log2(max(1, int(n_seeds)) / px * 1e6 + 1)))
 
 
+def candidates(n_shapes: int, schedules: Iterable[int] = SCHEDULES) -> list[tuple[int, int]]:
+    """Every (schedule, shape) pair; the sparse-only schedule has no tile rounds,
+    so it is tried once."""
+    out = []
+    for sched in schedules:
+        for shape in ([0] if sched == 0 else range(n_shapes)):
+            out.append((int(sched), int(shape)))
+    return out
+
+
+def apply(ctx: _capi.Context, choice: tuple[int, int]) -> None:
+    ctx.set_schedule(choice[0])
+    ctx.set_tile(choice[1])
+
+
 def tune(width: int, height: int, seeds, border_padding: int = _capi.AUTO_BORDER_PADDING,
-         candidates: Iterable[int] = CANDIDATES, repeats: int = 3, context: Optional[_capi.Context] = None,
-         force: bool = False) -> int:
-    """Pick the fastest propagation schedule for inputs like this one, set it
+         schedules: Iterable[int] = SCHEDULES, repeats: int = 3, context: Optional[_capi.Context] = None,
+         force: bool = False) -> tuple[int, int]:
+    """Pick the fastest (schedule, tile shape) for inputs like this one, set it
     on ``context`` (the current device's default context if None) and return
     it.  Times idl_triangulate_device with CUDA events on the current stream."""
     import torch
@@ -42,21 +67,22 @@ def tune(width: int, height: int, seeds, border_padding: int = _capi.AUTO_BORDER
     key = input_class(width, height, len(s))
     ctx = context or _capi.context_for(torch.cuda.current_device())
     if key in _cache and not force:
-        ctx.set_schedule(_cache[key])
+        apply(ctx, _cache[key])
         return _cache[key]
     lib = _capi.load()
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     d_seeds = torch.from_numpy(s).cuda()
     d_out = torch.empty((int(height), int(width), 3), dtype=torch.int32, device="cuda")
+    n_shapes = ctx.set_tile(0)
 
     def run():
         _capi.check(lib.idl_triangulate_device(ctx.handle, int(width), int(height), d_seeds.data_ptr(), len(s),
                                                int(border_padding), _capi.MODE_REFERENCE, d_out.data_ptr(), None))
 
     best, best_ms = None, float("inf")
-    for sched in candidates:
-        ctx.set_schedule(sched)
+    for choice in candidates(n_shapes, schedules):
+        apply(ctx, choice)
         run()                                   # warm-up: workspace at its high-water mark
         times = []
         for _ in range(max(1, repeats)):
@@ -68,7 +94,7 @@ def tune(width: int, height: int, seeds, border_padding: int = _capi.AUTO_BORDER
             times.append(e0.elapsed_time(e1))
         ms = min(times)
         if ms < best_ms:
-            best, best_ms = sched, ms
+            best, best_ms = choice, ms
     _cache[key] = best
-    ctx.set_schedule(best)
+    apply(ctx, best)
     return best

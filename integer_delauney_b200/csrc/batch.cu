@@ -530,7 +530,7 @@ void run_batch(Context& C, const Plan& pl, int P, int n_images, int32_t* d_out, 
         k_b_seeds<<<nblk(n), 256, 0, C.stream>>>(C.lab[0].as<int32_t>(), C.lab[1].as<int32_t>(), cv.pitch,
                                                 C.pos.as<uint32_t>(), n);
         IDL_LAUNCH();
-        propagate(C, IDL_MODE_REFERENCE, cv, C.pos.as<uint32_t>());
+        propagate(C, IDL_MODE_REFERENCE, cv, C.pos.as<uint32_t>(), n);
     }
     mark(2);
     auto bp = std::make_shared<BatchPlan>();

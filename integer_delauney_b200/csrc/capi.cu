@@ -196,7 +196,7 @@ int64_t run_triangulate(Context& C, int W, int H, int64_t n, const int32_t* vgri
             propagate_exact(C, cv, C.pos.as<uint32_t>(), n);
         } else {
             init_labels(C, cv, C.pos.as<uint32_t>(), n);
-            passes = propagate(C, mode, cv, C.pos.as<uint32_t>());
+            passes = propagate(C, mode, cv, C.pos.as<uint32_t>(), n);
         }
     } else {
         const size_t gbytes = (size_t)W * H * 2 * sizeof(int32_t);
@@ -349,6 +349,16 @@ int idl_context_set_schedule(idl_context* ctx, int dense_rounds)
     IDL_API_END
 }
 
+int idl_context_set_tile(idl_context* ctx, int shape, int* n_shapes_out)
+{
+    IDL_API_BEGIN
+    if (!ctx) invalid("context must not be NULL");
+    if (n_shapes_out) *n_shapes_out = key_tile_shapes();
+    if (shape < 0 || shape >= key_tile_shapes()) invalid("tile shape index out of range");
+    ctx->key_tile = shape;
+    IDL_API_END
+}
+
 int idl_context_synchronize(idl_context* ctx)
 {
     IDL_API_BEGIN
@@ -426,7 +436,7 @@ int idl_voronoi(idl_context* ctx, int width, int height, const int32_t* seeds_xy
         propagate_exact(C, cv, C.pos.as<uint32_t>(), n_seeds);
     } else {
         init_labels(C, cv, C.pos.as<uint32_t>(), n_seeds);
-        passes = propagate(C, mode, cv, C.pos.as<uint32_t>());
+        passes = propagate(C, mode, cv, C.pos.as<uint32_t>(), n_seeds);
     }
     const size_t bytes = (size_t)width * height * 2 * sizeof(int32_t);
     C.outgrid.ensure(bytes);

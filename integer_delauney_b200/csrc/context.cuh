@@ -146,6 +146,7 @@ struct Context {
     DevBuf exact_dy;      // exact mode: row distance to each cell's column-nearest seed
     int32_t stamp_epoch = 0;
     int dense_rounds = 1;  // propagation schedule from scratch (propagate.cu; idl_context_set_schedule)
+    int key_tile = 0;      // tile shape of the owner-key tile round (propagate.cu; idl_context_set_tile)
 
     // topology
     DevBuf hkeys, hvals;  // hash table of triangle keys -> first witness
@@ -247,21 +248,27 @@ void rank_seeds_device(Context& C, int W, int H, const int32_t* xs, const int32_
                        int32_t* rank, int32_t* inv, int32_t* xs_sorted, int32_t* ys_sorted);
 
 // Stage (a) on the Wd x Hd detection canvas whose labels are in C.lab[0]
-// (both planes must hold the same starting state).  Returns the pass count
-// (propagate.cu).  `first_tiles`: nullptr = every tile starts active;
-// otherwise a device list of `n_first` tile ids.
+// (both planes must hold the same starting state); the result is left in
+// C.lab[0].  Returns the pass count (propagate.cu).  From scratch (seed_pos ==
+// nullptr) the n_seeds seeds of `pos` are the canvas's seeds in id order,
+// which must be their (x, y) order (per image of a batch atlas); in reference
+// semantics that propagation runs on owner keys (stencil.cuh), and
+// C.lab[1] is scratch afterwards.  With seed_pos the state is a fixed point
+// except at n_new freshly written seed cells, and ids may be in any order.
 struct Canvas {
     int Wd, Hd, pitch;
 };
-int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos = nullptr,
-                  int64_t n_new = 0);
+int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, int64_t n_seeds,
+                  const uint32_t* seed_pos = nullptr, int64_t n_new = 0);
+// Number of owner-key tile round shapes (Context::key_tile indexes them).
+int key_tile_shapes();
 
 // Reference-semantics propagation as one persistent kernel (sparse_jacobi.cu).
 // `seed_pos` (may be nullptr): the state is a fixed point except at these
 // n_new freshly written seed cells (packed canvas positions), so only the
 // micro-tiles around them start active; otherwise every micro-tile does.
 int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos = nullptr,
-                         int64_t n_new = 0);
+                         int64_t n_new = 0, bool keys = false);
 
 // As propagate_sparse from scratch, with the first work list built from a
 // device list of n_big tiles of big_w x big_h cells (big_tiles_x per row;
@@ -269,10 +276,10 @@ int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos, cons
 // holds the starting state, and every micro-tile outside the list must hold
 // the same state in both planes.
 int64_t propagate_sparse_from_tiles(Context& C, const Canvas& cv, const uint32_t* pos, const int32_t* big_list,
-                                    int n_big, int big_tiles_x, int big_w, int big_h);
+                                    int n_big, int big_tiles_x, int big_w, int big_h, bool keys = false);
 int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
                               int64_t n_new, const int32_t* big_list, int n_big, int big_tiles_x, int sub_x,
-                              int sub_y);
+                              int sub_y, bool keys);
 
 // Run the persistent kernel's grid barrier alone (sparse_jacobi.cu) on one
 // block per SM, waiting for `missing_arrivals` more blocks than the grid has,

@@ -932,7 +932,7 @@ int idl_delaunay_insert_ordered(idl_delaunay* d, const int32_t* xy, int64_t k, c
         k_put_seeds<<<gk, 256, 0, C.stream>>>(d->planes, d->planes + (size_t)d->pitch * d->Hd, d->pitch,
                                               d->pos + n0, k, n0);
         IDL_LAUNCH();
-        passes = propagate(C, d->mode, d->canvas(), d->pos, d->pos + n0, k);
+        passes = propagate(C, d->mode, d->canvas(), d->pos, n0 + k, d->pos + n0, k);
     }
     const float bfs = T.stop();
     if (timings) {

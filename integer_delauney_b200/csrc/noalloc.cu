@@ -167,7 +167,7 @@ int idl_voronoi_noalloc(int width, int height, const int32_t* d_seeds_xy, int64_
     cv.pitch = (width + 31) / 32 * 32;
     sort_seeds_device(C, width, height, n_seeds, 0);
     init_labels(C, cv, C.pos.as<uint32_t>(), n_seeds);
-    const int64_t passes = propagate(C, mode, cv, C.pos.as<uint32_t>());
+    const int64_t passes = propagate(C, mode, cv, C.pos.as<uint32_t>(), n_seeds);
     dim3 g(ceil_div(width, 256), height);
     k_noalloc_compose2<<<g, 256, 0, C.stream>>>(C.lab[0].as<int32_t>(), cv.pitch, width, height,
                                                 C.pos.as<uint32_t>(), d_grid_out);

@@ -279,6 +279,245 @@ k_round(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pitch, i
     }
 }
 
+// ---------------------------------------------------------------------------
+// Reference semantics on owner keys (stencil.cuh): the tile round of k_round
+// with the label planes holding packed owner positions, so a candidate's
+// distance is pure arithmetic on its key and every cell update is branch-free.
+// Geometry is a template: NW warps of 8 rows each, 2 columns per lane, so the
+// region is 64 x 8NW cells; KS Jacobi steps per HBM round trip leave an inner
+// tile of (64 - 2KS) x (8NW - 2KS).
+// ---------------------------------------------------------------------------
+template <int NW, int KS>
+struct KeyTile {
+    static constexpr int RW = 64, ROWS = 8, RH = NW * ROWS;
+    static constexpr int TW = RW - 2 * KS, TH = RH - 2 * KS;
+    static constexpr int THREADS = NW * 32;
+    static_assert(KS >= 1 && KS <= TW && KS <= TH, "a round's light cone must stay within the neighbour tiles");
+    static_assert(TW % 8 == 0 && TH % 8 == 0, "tiles must be whole 8 x 8 micro-tiles for the sparse hand-off");
+    static_assert(KS % 2 == 0, "a lane's two columns must start on an even column for paired loads");
+};
+
+template <int NW>
+struct KeyEdges {
+    int32_t lab[2][NW][2][64];   // [parity][warp][0 = top row, 1 = bottom row][column]
+    uint32_t chg[2][NW][2][2];   // [parity][warp][top/bottom][column 0/1 of each lane]: lane ballots
+};
+
+template <int NW>
+__device__ __forceinline__ void key_publish(KeyEdges<NW>& E, int par, int warp, int lane, const int32_t (&L)[8][2],
+                                            uint32_t chg)
+{
+    E.lab[par][warp][0][2 * lane] = L[0][0];
+    E.lab[par][warp][0][2 * lane + 1] = L[0][1];
+    E.lab[par][warp][1][2 * lane] = L[7][0];
+    E.lab[par][warp][1][2 * lane + 1] = L[7][1];
+    const uint32_t t0 = __ballot_sync(FULL, chg & 1u), t1 = __ballot_sync(FULL, chg & 2u);
+    const uint32_t b0 = __ballot_sync(FULL, chg & (1u << 14)), b1 = __ballot_sync(FULL, chg & (1u << 15));
+    if (lane == 0) {
+        E.chg[par][warp][0][0] = t0;
+        E.chg[par][warp][0][1] = t1;
+        E.chg[par][warp][1][0] = b0;
+        E.chg[par][warp][1][1] = b1;
+    }
+}
+
+// One cell's Jacobi step on keys: the best of its own owner (k, d) and four
+// candidate keys; cells below UNDEF (outside the canvas, batch walls) never change.
+__device__ __forceinline__ void key_cell(int32_t& k, int32_t& d, int32_t a, int32_t b, int32_t c, int32_t e, int x,
+                                         int y)
+{
+    int32_t bk = k, bd = d;
+    relax_key(bk, bd, a, x, y);
+    relax_key(bk, bd, b, x, y);
+    relax_key(bk, bd, c, x, y);
+    relax_key(bk, bd, e, x, y);
+    const bool fixed = k < UNDEF;
+    k = fixed ? k : bk;
+    d = fixed ? d : bd;
+}
+
+template <int NW, int KS>
+__global__ void __launch_bounds__(NW * 32, (NW <= 8 ? 3 : 2))
+k_round_keys(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pitch, int Wd, int Hd,
+             const int32_t* __restrict__ list_in, const int32_t* __restrict__ count_in,
+             int32_t* __restrict__ list_out, int32_t* __restrict__ count_out, int32_t* __restrict__ stamp,
+             int32_t stamp_next, int tiles_x, int tiles_y, long long step_base, long long* __restrict__ last_change)
+{
+    using T = KeyTile<NW, KS>;
+    constexpr int ROWS = T::ROWS;
+    __shared__ KeyEdges<NW> E;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int cx0 = 2 * lane, cy0 = warp * ROWS;
+
+    uint32_t inner = 0;
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r)
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+            if (cx0 + c >= KS && cx0 + c < KS + T::TW && cy0 + r >= KS && cy0 + r < KS + T::TH)
+                inner |= 1u << (2 * r + c);
+
+    const int n_items = *count_in;
+    for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+        const int t = list_in[item];
+        const int tx = t % tiles_x, ty = t / tiles_x;
+        const int gx = tx * T::TW - KS + cx0;
+        const int gyb = ty * T::TH - KS + cy0;
+
+        int32_t L[ROWS][2], D[ROWS][2];
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r) {
+            const int gy = gyb + r;
+            const bool row_in = gy >= 0 && gy < Hd;
+            int32_t l0 = OUTSIDE, l1 = OUTSIDE;
+            if (row_in) {
+                const int32_t* row = src + (size_t)gy * pitch;
+                if (gx >= 0 && gx + 1 < Wd) {
+                    const int2 v = *reinterpret_cast<const int2*>(row + gx);
+                    l0 = v.x;
+                    l1 = v.y;
+                } else {
+                    if (gx >= 0 && gx < Wd) l0 = row[gx];
+                    if (gx + 1 >= 0 && gx + 1 < Wd) l1 = row[gx + 1];
+                }
+            }
+            L[r][0] = l0;
+            L[r][1] = l1;
+            D[r][0] = l0 >= 0 ? key_dist2(gx, gy, l0) : FAR;
+            D[r][1] = l1 >= 0 ? key_dist2(gx + 1, gy, l1) : FAR;
+        }
+        key_publish<NW>(E, 1, warp, lane, L, 0xFFFFFFFFu);
+        __syncthreads();
+
+        uint32_t chg = 0;
+        int last_step = -1;
+        int par = 1;
+#pragma unroll 1
+        for (int s = 0; s < KS; ++s) {
+            uint32_t new_chg = 0;
+            const int pp = par;
+            int32_t up0 = warp > 0 ? E.lab[pp][warp - 1][1][cx0] : OUTSIDE;
+            int32_t up1 = warp > 0 ? E.lab[pp][warp - 1][1][cx0 + 1] : OUTSIDE;
+            const int32_t dn0 = warp < NW - 1 ? E.lab[pp][warp + 1][0][cx0] : OUTSIDE;
+            const int32_t dn1 = warp < NW - 1 ? E.lab[pp][warp + 1][0][cx0 + 1] : OUTSIDE;
+            uint32_t dirty;
+            if (s == 0) {
+                dirty = 0xFFFFu;
+            } else {
+                dirty = chg | (chg << 2) | (chg >> 2) | ((chg & 0x5555u) << 1) | ((chg & 0xAAAAu) >> 1);
+                const uint32_t lc = __shfl_up_sync(FULL, chg, 1), rc = __shfl_down_sync(FULL, chg, 1);
+                if (lane > 0) dirty |= (lc & 0xAAAAu) >> 1;
+                if (lane < 31) dirty |= (rc & 0x5555u) << 1;
+                if (warp > 0) {
+                    dirty |= (E.chg[pp][warp - 1][1][0] >> lane) & 1u;
+                    dirty |= ((E.chg[pp][warp - 1][1][1] >> lane) & 1u) << 1;
+                }
+                if (warp < NW - 1) {
+                    dirty |= ((E.chg[pp][warp + 1][0][0] >> lane) & 1u) << 14;
+                    dirty |= ((E.chg[pp][warp + 1][0][1] >> lane) & 1u) << 15;
+                }
+                dirty &= 0xFFFFu;
+            }
+            if (__any_sync(FULL, dirty != 0)) {
+#pragma unroll
+                for (int r = 0; r < ROWS; ++r) {
+                    const int32_t o0 = L[r][0], o1 = L[r][1];
+                    int32_t left = __shfl_up_sync(FULL, o1, 1);
+                    int32_t right = __shfl_down_sync(FULL, o0, 1);
+                    if (lane == 0) left = OUTSIDE;
+                    if (lane == 31) right = OUTSIDE;
+                    const int32_t b0 = r + 1 < ROWS ? L[r + 1][0] : dn0;
+                    const int32_t b1 = r + 1 < ROWS ? L[r + 1][1] : dn1;
+                    const int gy = gyb + r;
+                    key_cell(L[r][0], D[r][0], left, o1, up0, b0, gx, gy);
+                    key_cell(L[r][1], D[r][1], o0, right, up1, b1, gx + 1, gy);
+                    new_chg |= (uint32_t(L[r][0] != o0) << (2 * r)) | (uint32_t(L[r][1] != o1) << (2 * r + 1));
+                    up0 = o0;
+                    up1 = o1;
+                }
+            }
+            par ^= 1;
+            key_publish<NW>(E, par, warp, lane, L, new_chg);
+            chg = new_chg;
+            if (__syncthreads_or((new_chg & inner) != 0u)) last_step = s;
+        }
+
+        // inner cells only: a lane's two columns are both inner or both not
+#pragma unroll
+        for (int r = 0; r < ROWS; ++r) {
+            const int gy = gyb + r;
+            if (!((inner >> (2 * r)) & 1u) || gy >= Hd) continue;
+            int32_t* row = dst + (size_t)gy * pitch;
+            if (gx + 1 < Wd) {
+                *reinterpret_cast<int2*>(row + gx) = make_int2(L[r][0], L[r][1]);
+            } else if (gx < Wd) {
+                row[gx] = L[r][0];
+            }
+        }
+
+        if (last_step >= 0) {
+            if (threadIdx.x == 0) atomicMax(last_change, step_base + last_step);
+            if (threadIdx.x < 9) {
+                const int nx = tx + int(threadIdx.x % 3) - 1, ny = ty + int(threadIdx.x / 3) - 1;
+                if (nx >= 0 && nx < tiles_x && ny >= 0 && ny < tiles_y) {
+                    const int nt = ny * tiles_x + nx;
+                    if (atomicExch(&stamp[nt], stamp_next) != stamp_next) {
+                        const int slot = atomicAdd(count_out, 1);
+                        list_out[slot] = nt;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Seed cells of both planes take their seeds' keys (the rest of the planes
+// already holds UNDEF, or walls for a batch atlas).
+__global__ void k_seed_keys(int32_t* __restrict__ a, int32_t* __restrict__ b, int pitch,
+                            const uint32_t* __restrict__ pos, int64_t n)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t p = pos[i];
+    const size_t o = (size_t)pos_y(p) * pitch + pos_x(p);
+    const int32_t k = key_from_pos(p);
+    a[o] = k;
+    b[o] = k;
+}
+
+// Keys back to ids: `ids` (the other plane, free once both planes agree)
+// takes at each seed cell that seed's id; every owned cell of `lab` then
+// looks its owner's id up at the owner's own cell.  Only seed cells of `ids`
+// are read, and `lab` is the only plane written.
+__global__ void k_seed_ids(int32_t* __restrict__ ids, int pitch, const uint32_t* __restrict__ pos, int64_t n)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t p = pos[i];
+    ids[(size_t)pos_y(p) * pitch + pos_x(p)] = (int32_t)i;
+}
+
+__global__ void k_keys_to_ids(int32_t* __restrict__ lab, const int32_t* __restrict__ ids, int pitch, int Wd)
+{
+    int32_t* row = lab + (size_t)blockIdx.y * pitch;
+    for (int x = (blockIdx.x * blockDim.x + threadIdx.x) * 4; x < Wd; x += gridDim.x * blockDim.x * 4) {
+        if (x + 3 < Wd) {
+            int4 v = *reinterpret_cast<const int4*>(row + x);
+            if (v.x >= 0) v.x = __ldg(&ids[(size_t)key_y(v.x) * pitch + key_x(v.x)]);
+            if (v.y >= 0) v.y = __ldg(&ids[(size_t)key_y(v.y) * pitch + key_x(v.y)]);
+            if (v.z >= 0) v.z = __ldg(&ids[(size_t)key_y(v.z) * pitch + key_x(v.z)]);
+            if (v.w >= 0) v.w = __ldg(&ids[(size_t)key_y(v.w) * pitch + key_x(v.w)]);
+            *reinterpret_cast<int4*>(row + x) = v;
+        } else {
+            for (int c = x; c < Wd; ++c) {
+                const int32_t k = row[c];
+                if (k >= 0) row[c] = __ldg(&ids[(size_t)key_y(k) * pitch + key_x(k)]);
+            }
+        }
+    }
+}
+
 __global__ void k_iota(int32_t* __restrict__ a, int n, int32_t* __restrict__ count)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -350,26 +589,87 @@ int32_t claim_stamps(Context& C, int n_items, int64_t steps)
     return epoch;
 }
 
-int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
-                  int64_t n_new)
+namespace {
+
+// Owner-key tile round shapes (C.key_tile): warps per CTA x steps per round.
+struct KeyShape {
+    int nw, ks, tw, th;
+};
+constexpr KeyShape KEY_SHAPES[] = {
+    {8, 8, KeyTile<8, 8>::TW, KeyTile<8, 8>::TH},        // 48 x 48 inner tile, 8 passes per round trip
+    {16, 8, KeyTile<16, 8>::TW, KeyTile<16, 8>::TH},     // 48 x 112, 8 passes
+    {8, 4, KeyTile<8, 4>::TW, KeyTile<8, 4>::TH},        // 56 x 56, 4 passes
+    {16, 12, KeyTile<16, 12>::TW, KeyTile<16, 12>::TH},  // 40 x 104, 12 passes
+};
+constexpr int N_KEY_SHAPES = int(sizeof(KEY_SHAPES) / sizeof(KEY_SHAPES[0]));
+
+template <int NW, int KS>
+void launch_round_keys(Context& C, int per_sm, const int32_t* src, int32_t* dst, const Canvas& cv, const int32_t* lin,
+                       const int32_t* cin, int32_t* lout, int32_t* cout, int32_t* stamp, int32_t stamp_next,
+                       int tiles_x, int tiles_y, long long base, long long* last)
+{
+    const int grid = std::min(tiles_x * tiles_y, C.num_sms * per_sm);
+    k_round_keys<NW, KS><<<grid, NW * 32, 0, C.stream>>>(src, dst, cv.pitch, cv.Wd, cv.Hd, lin, cin, lout, cout, stamp,
+                                                         stamp_next, tiles_x, tiles_y, base, last);
+}
+
+int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
+                         int64_t n_new, bool keys);
+
+}  // namespace
+
+int key_tile_shapes() { return N_KEY_SHAPES; }
+
+int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, int64_t n_seeds,
+                  const uint32_t* seed_pos, int64_t n_new)
 {
     C.prof.tiles = C.prof.rounds = C.prof.passes = 0;
     C.prof.prop_bytes = 0.0;
+    if (mode != IDL_MODE_REFERENCE || seed_pos) return propagate_rounds(C, mode, cv, pos, seed_pos, n_new, false);
+    // From scratch in reference semantics: run on owner keys, then map every
+    // owned cell back to its owner's id.
+    if (n_seeds > 0) {
+        k_seed_keys<<<(unsigned)((n_seeds + 255) / 256), 256, 0, C.stream>>>(
+            C.lab[0].as<int32_t>(), C.lab[1].as<int32_t>(), cv.pitch, pos, n_seeds);
+        IDL_LAUNCH();
+    }
+    const int64_t passes = propagate_rounds(C, mode, cv, pos, nullptr, 0, true);
+    // the result is in plane 0 (both planes agree); plane 1 takes the ids at the seed cells
+    if (n_seeds > 0) {
+        k_seed_ids<<<(unsigned)((n_seeds + 255) / 256), 256, 0, C.stream>>>(C.lab[1].as<int32_t>(), cv.pitch, pos,
+                                                                           n_seeds);
+        IDL_LAUNCH();
+        const int gx = std::max(1, std::min(ceil_div(cv.Wd, 4 * 256), 4));
+        k_keys_to_ids<<<dim3(gx, cv.Hd), 256, 0, C.stream>>>(C.lab[0].as<int32_t>(), C.lab[1].as<int32_t>(),
+                                                              cv.pitch, cv.Wd);
+        IDL_LAUNCH();
+    }
+    return passes;
+}
+
+namespace {
+
+int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
+                         int64_t n_new, bool keys)
+{
     // Reference semantics.  A continued propagation (seed_pos) is local from
     // its first pass: the sparse kernel alone, or with C.dense_rounds < 0 tile
     // rounds starting from the tiles around the new seeds (plain launches, no
     // device-wide persistent grid, so streams of other work overlap them).
     // From scratch, the first passes change most of the canvas, which the
-    // tile rounds (KSTEPS passes per HBM round trip, no per-pass bookkeeping)
+    // tile rounds (several passes per HBM round trip, no per-pass bookkeeping)
     // do best; once the changes thin out, the sparse kernel takes over the
     // tail, whose single passes touch few cells.  C.dense_rounds sets the
     // switch (0: sparse only, < 0: tile rounds to convergence).
     const bool seeded_rounds = mode == IDL_MODE_REFERENCE && seed_pos && C.dense_rounds < 0;
     const bool hybrid = mode == IDL_MODE_REFERENCE && !seed_pos && C.dense_rounds != 0;
-    if (mode == IDL_MODE_REFERENCE && !hybrid && !seeded_rounds) return propagate_sparse(C, cv, pos, seed_pos, n_new);
+    if (mode == IDL_MODE_REFERENCE && !hybrid && !seeded_rounds)
+        return propagate_sparse(C, cv, pos, seed_pos, n_new, keys);
     if (seed_pos && n_new == 0) return 0;
     const int64_t round_limit = hybrid && C.dense_rounds > 0 ? C.dense_rounds : -1;
-    const int tiles_x = ceil_div(cv.Wd, TW), tiles_y = ceil_div(cv.Hd, TH);
+    const KeyShape shape = KEY_SHAPES[std::min(std::max(C.key_tile, 0), N_KEY_SHAPES - 1)];
+    const int tw = keys ? shape.tw : TW, th = keys ? shape.th : TH, steps = keys ? shape.ks : KSTEPS;
+    const int tiles_x = ceil_div(cv.Wd, tw), tiles_y = ceil_div(cv.Hd, th);
     const int n_tiles = tiles_x * tiles_y;
     // Bound on rounds: far above any real run (a pass count beyond the canvas
     // area cannot occur since every change strictly improves one of Wd*Hd keys
@@ -407,16 +707,36 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, c
             int32_t* dstp = C.lab[(r + 1) & 1].as<int32_t>();
             const int32_t* lin = C.tiles[r & 1].as<int32_t>();
             int32_t* lout = C.tiles[(r + 1) & 1].as<int32_t>();
-            const long long base = (long long)r * KSTEPS;
+            const long long base = (long long)r * steps;
             const int32_t stamp_next = epoch + int32_t(r) + 1;
-            if (mode == IDL_MODE_NUMPY)
+            int32_t* stamp = C.stamps.as<int32_t>();
+            if (keys) {
+                switch (C.key_tile) {
+                case 1:
+                    launch_round_keys<16, 8>(C, 2, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
+                                             stamp_next, tiles_x, tiles_y, base, last);
+                    break;
+                case 2:
+                    launch_round_keys<8, 4>(C, 3, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
+                                            stamp_next, tiles_x, tiles_y, base, last);
+                    break;
+                case 3:
+                    launch_round_keys<16, 12>(C, 2, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
+                                              stamp_next, tiles_x, tiles_y, base, last);
+                    break;
+                default:
+                    launch_round_keys<8, 8>(C, 3, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
+                                            stamp_next, tiles_x, tiles_y, base, last);
+                }
+            } else if (mode == IDL_MODE_NUMPY) {
                 k_round<IDL_MODE_NUMPY><<<grid, THREADS, 0, C.stream>>>(
-                    srcp, dstp, cv.pitch, cv.Wd, cv.Hd, pos, lin, counts + r, lout, counts + r + 1,
-                    C.stamps.as<int32_t>(), stamp_next, tiles_x, tiles_y, base, last);
-            else
+                    srcp, dstp, cv.pitch, cv.Wd, cv.Hd, pos, lin, counts + r, lout, counts + r + 1, stamp,
+                    stamp_next, tiles_x, tiles_y, base, last);
+            } else {
                 k_round<IDL_MODE_REFERENCE><<<grid, THREADS, 0, C.stream>>>(
-                    srcp, dstp, cv.pitch, cv.Wd, cv.Hd, pos, lin, counts + r, lout, counts + r + 1,
-                    C.stamps.as<int32_t>(), stamp_next, tiles_x, tiles_y, base, last);
+                    srcp, dstp, cv.pitch, cv.Wd, cv.Hd, pos, lin, counts + r, lout, counts + r + 1, stamp,
+                    stamp_next, tiles_x, tiles_y, base, last);
+            }
             IDL_LAUNCH();
         }
         IDL_CUDA(cudaMemcpyAsync(&remaining, counts + r, 4, cudaMemcpyDeviceToHost, C.stream));
@@ -439,13 +759,13 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, c
             tiles += h[i];
             rounds += h[i] > 0;
         }
-        C.prof.tiles = tiles * (TW / 8) * (TH / 8) * KSTEPS;
+        C.prof.tiles = tiles * (tw / 8) * (th / 8) * steps;
         C.prof.rounds = rounds;
-        C.prof.prop_bytes = (double)tiles * TW * TH * 8.0;
+        C.prof.prop_bytes = (double)tiles * tw * th * 8.0;
         C.prof.passes = passes;
-        C.prof.tile_w = TW;
-        C.prof.tile_h = TH;
-        C.prof.steps_per_round = KSTEPS;
+        C.prof.tile_w = tw;
+        C.prof.tile_h = th;
+        C.prof.steps_per_round = steps;
     }
     if (remaining > 0) {
         // Hand the tail to the sparse kernel: the latest state goes to plane
@@ -456,11 +776,13 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, c
         IDL_CUDA(cudaMemcpyAsync(C.big_tiles.ptr, C.tiles[r & 1].ptr, (size_t)remaining * 4, cudaMemcpyDeviceToDevice,
                                  C.stream));
         const int64_t sparse = propagate_sparse_from_tiles(C, cv, pos, C.big_tiles.as<int32_t>(), remaining,
-                                                           tiles_x, TW, TH);
-        passes = sparse >= 2 ? r * KSTEPS + sparse : passes;
+                                                           tiles_x, tw, th, keys);
+        passes = sparse >= 2 ? r * steps + sparse : passes;
         if (C.prof.enabled) C.prof.passes = passes;
     }
     return passes;
 }
+
+}  // namespace
 
 }  // namespace idl

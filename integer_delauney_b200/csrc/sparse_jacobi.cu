@@ -110,6 +110,17 @@ __device__ __forceinline__ void best_of4(int32_t& b, int32_t n0, int32_t n1, int
     b = bl;
 }
 
+// best_of4 on owner keys (stencil.cuh): no seed-table loads.
+__device__ __forceinline__ void best_of4_keys(int32_t& b, int32_t n0, int32_t n1, int32_t n2, int32_t n3, int x,
+                                              int y)
+{
+    int32_t bd = b >= 0 ? key_dist2(x, y, b) : FAR;
+    relax_key(b, bd, n0, x, y);
+    relax_key(b, bd, n1, x, y);
+    relax_key(b, bd, n2, x, y);
+    relax_key(b, bd, n3, x, y);
+}
+
 // Per-block staging of next-pass list entries.  Groups reserve slots with
 // atomicAdd on *n; a group whose slots would run past STAGE goes to the global
 // list instead and lowers *cut to its first slot, so that only the prefix
@@ -121,7 +132,8 @@ struct Stage {
 };
 
 // Advance `cnt` (<= GROUP, warp-uniform) micro-tiles by one Jacobi pass and
-// list the micro-tiles pass t+1 must run.
+// list the micro-tiles pass t+1 must run.  KEYS: labels are owner keys.
+template <bool KEYS>
 __device__ __forceinline__ void advance(const int (&ids)[GROUP], int cnt, const int32_t* cur, int32_t* nxt,
                                         int pitch, int Wd, int Hd, int mt_x, int mt_y,
                                         const uint32_t* __restrict__ pos, uint32_t* bin, uint32_t* bout,
@@ -180,10 +192,18 @@ __device__ __forceinline__ void advance(const int (&ids)[GROUP], int cnt, const 
 
         // cells below UNDEF are walls between packed images: never updated
         int32_t b0 = a0[k], b1 = a1[k];
-        if (in0[k] && b0 >= UNDEF && (lf[k] != b0 || a1[k] != b0 || u0[k] != b0 || d0[k] != b0))
-            best_of4(b0, lf[k], a1[k], u0[k], d0[k], gx[k], gy[k], pos);
-        if (in1[k] && b1 >= UNDEF && (a0[k] != b1 || rt[k] != b1 || u1[k] != b1 || d1[k] != b1))
-            best_of4(b1, a0[k], rt[k], u1[k], d1[k], gx[k] + 1, gy[k], pos);
+        if (KEYS) {
+            int32_t c0 = b0, c1 = b1;
+            best_of4_keys(c0, lf[k], a1[k], u0[k], d0[k], gx[k], gy[k]);
+            best_of4_keys(c1, a0[k], rt[k], u1[k], d1[k], gx[k] + 1, gy[k]);
+            b0 = (in0[k] && b0 >= UNDEF) ? c0 : b0;
+            b1 = (in1[k] && b1 >= UNDEF) ? c1 : b1;
+        } else {
+            if (in0[k] && b0 >= UNDEF && (lf[k] != b0 || a1[k] != b0 || u0[k] != b0 || d0[k] != b0))
+                best_of4(b0, lf[k], a1[k], u0[k], d0[k], gx[k], gy[k], pos);
+            if (in1[k] && b1 >= UNDEF && (a0[k] != b1 || rt[k] != b1 || u1[k] != b1 || d1[k] != b1))
+                best_of4(b1, a0[k], rt[k], u1[k], d1[k], gx[k] + 1, gy[k], pos);
+        }
         const size_t o = (size_t)gy[k] * pitch + gx[k];
         if (in1[k]) *reinterpret_cast<int2*>(nxt + o) = make_int2(b0, b1);
         else if (in0[k]) nxt[o] = b0;
@@ -233,6 +253,7 @@ __device__ __forceinline__ void advance(const int (&ids)[GROUP], int cnt, const 
 
 // counts[t]: micro-tiles listed for pass t.  Pass t runs list t%2 and appends
 // pass t+1's micro-tiles to list (t+1)%2.
+template <bool KEYS>
 __global__ void __launch_bounds__(SJ_THREADS, 1)
 k_sparse_jacobi(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, const uint32_t* __restrict__ pos,
                 uint32_t* bits0, uint32_t* bits1, int32_t* list0, int32_t* list1, int32_t* counts, int max_steps,
@@ -264,8 +285,8 @@ k_sparse_jacobi(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, con
             const int cnt = min(GROUP, n - i0);
 #pragma unroll
             for (int k = 0; k < GROUP; ++k) ids[k] = k < cnt ? __ldcg(&lin[i0 + k]) : 0;
-            advance(ids, cnt, cur, nxt, pitch, Wd, Hd, mt_x, mt_y, pos, bin, bout, lout, counts + t + 1,
-                    Stage{s_list, &s_n, &s_cut}, lane);
+            advance<KEYS>(ids, cnt, cur, nxt, pitch, Wd, Hd, mt_x, mt_y, pos, bin, bout, lout, counts + t + 1,
+                          Stage{s_list, &s_n, &s_cut}, lane);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -375,21 +396,22 @@ void grid_barrier_selftest(Context& C, int missing_arrivals, unsigned spin_limit
 }
 
 int64_t propagate_sparse_from_tiles(Context& C, const Canvas& cv, const uint32_t* pos, const int32_t* big_list,
-                                    int n_big, int big_tiles_x, int big_w, int big_h)
+                                    int n_big, int big_tiles_x, int big_w, int big_h, bool keys)
 {
     if (big_w % MT != 0 || big_h % MT != 0) throw Error(IDL_ERR_INTERNAL, "tile sides must be micro-tile multiples");
-    return propagate_sparse_impl(C, cv, pos, nullptr, 0, big_list, n_big, big_tiles_x, big_w / MT, big_h / MT);
+    return propagate_sparse_impl(C, cv, pos, nullptr, 0, big_list, n_big, big_tiles_x, big_w / MT, big_h / MT,
+                                 keys);
 }
 
 int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
-                         int64_t n_new)
+                         int64_t n_new, bool keys)
 {
-    return propagate_sparse_impl(C, cv, pos, seed_pos, n_new, nullptr, 0, 0, 0, 0);
+    return propagate_sparse_impl(C, cv, pos, seed_pos, n_new, nullptr, 0, 0, 0, 0, keys);
 }
 
 int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
                               int64_t n_new, const int32_t* big_list, int n_big, int big_tiles_x, int sub_x,
-                              int sub_y)
+                              int sub_y, bool keys)
 {
     const int mt_x = ceil_div(cv.Wd, MT), mt_y = ceil_div(cv.Hd, MT);
     const int n_mt = mt_x * mt_y;
@@ -429,7 +451,8 @@ int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos,
     IDL_CUDA(cudaMemsetAsync(C.gsync.ptr, 0, sizeof(GridSync), C.stream));
 
     int per_sm = 0;
-    IDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sparse_jacobi, SJ_THREADS, 0));
+    const void* kernel = keys ? (const void*)k_sparse_jacobi<true> : (const void*)k_sparse_jacobi<false>;
+    IDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, SJ_THREADS, 0));
     if (per_sm < 1) throw Error(IDL_ERR_INTERNAL, "propagation kernel cannot be resident");
     const int grid = per_sm * C.num_sms;
     int32_t* p0 = C.lab[0].as<int32_t>();
@@ -445,8 +468,7 @@ int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos,
         // keeps each grid's co-residency independent of the other streams.
         static std::mutex device_locks[64];
         std::lock_guard<std::mutex> lock(device_locks[C.device & 63]);
-        IDL_CUDA(cudaLaunchCooperativeKernel((const void*)k_sparse_jacobi, dim3(grid), dim3(SJ_THREADS), args, 0,
-                                             C.stream));
+        IDL_CUDA(cudaLaunchCooperativeKernel(kernel, dim3(grid), dim3(SJ_THREADS), args, 0, C.stream));
         count_launch();
         IDL_CUDA(cudaMemcpyAsync(&h, gs, sizeof(GridSync), cudaMemcpyDeviceToHost, C.stream));
         IDL_CUDA(cudaStreamSynchronize(C.stream));

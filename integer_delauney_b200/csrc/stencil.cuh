@@ -26,3 +26,40 @@ __device__ __forceinline__ void relax(int32_t& bl, int32_t& bd, int32_t n, int x
 }
 
 }  // namespace idl
+
+namespace idl {
+
+// Owner keys.  During a from-scratch propagation in reference semantics the
+// label planes hold, instead of the owner's id, its position packed as
+// x << 15 | y (x, y < 32768, so keys are non-negative and below 2^30).  Seed
+// ids there are the seeds' (x, y)-sorted order (per image of a batch atlas,
+// and cells of different images never meet), so key order is id order and the
+// tie rule "equal distance, higher id wins" reads "higher key wins"; the
+// candidate's distance comes from its key with no seed-table load.  Negative
+// labels (UNDEF, OUTSIDE, batch walls) keep their meaning.
+__host__ __device__ inline int32_t key_from_pos(uint32_t p)
+{
+    return int32_t((uint32_t)pos_x(p) << 15 | (uint32_t)pos_y(p));
+}
+__host__ __device__ inline int key_x(int32_t k) { return k >> 15; }
+__host__ __device__ inline int key_y(int32_t k) { return k & 0x7FFF; }
+
+// Exact for a real key (below 2^31); for a negative label the value is
+// meaningless but defined (unsigned wrap-around), and callers mask it out.
+__device__ __forceinline__ int32_t key_dist2(int x, int y, int32_t k)
+{
+    const uint32_t dx = uint32_t(x - key_x(k)), dy = uint32_t(y - key_y(k));
+    return int32_t(dx * dx + dy * dy);
+}
+
+// relax() on keys, without branches: candidate n (negative = none) replaces
+// (bk, bd) if strictly closer, or equally close with a higher key.
+__device__ __forceinline__ void relax_key(int32_t& bk, int32_t& bd, int32_t n, int x, int y)
+{
+    const int32_t nd = key_dist2(x, y, n);
+    const bool better = n >= 0 && (nd < bd || (nd == bd && n > bk));
+    bk = better ? n : bk;
+    bd = better ? nd : bd;
+}
+
+}  // namespace idl

@@ -67,6 +67,8 @@ def lib():
     L.or_assign.argtypes = [i32, i32, _i32p, _i32p, i32, _i32p, i64, _i32p]
     L.or_assign_rows.restype = None
     L.or_assign_rows.argtypes = [i32, i32, _i32p, _i32p, i32, _i32p, i64, i32, i32, _i32p]
+    L.or_assign_bbox_rows.restype = None
+    L.or_assign_bbox_rows.argtypes = [i32, i32, _i32p, _i32p, _i32p, i64, i32, i32, _i32p]
     L.or_triangulate.restype = i64
     L.or_triangulate.argtypes = [i32, i32, _i32p, _i32p, i32, i32, i32, ctypes.c_void_p,
                                  _i32p, _i32p, i64, ctypes.POINTER(ctypes.c_int64)]
@@ -194,6 +196,18 @@ def assign_rows(W: int, H: int, xs, ys, tris: np.ndarray, y0: int, y1: int) -> n
     return out
 
 
+def assign_bbox(W: int, H: int, xs, ys, tris: np.ndarray, y0: int = 0, y1=None) -> np.ndarray:
+    """assign() evaluated per triangle over its bounding box (same result,
+    cost proportional to the triangles' box areas); rows [y0, y1)."""
+    y1 = H if y1 is None else y1
+    xs = np.ascontiguousarray(xs, dtype=np.int32)
+    ys = np.ascontiguousarray(ys, dtype=np.int32)
+    t = np.ascontiguousarray(tris, dtype=np.int32).reshape(-1, 5)
+    out = np.empty((y1 - y0, W), dtype=np.int32)
+    lib().or_assign_bbox_rows(W, H, xs, ys, t, len(t), int(y0), int(y1), out)
+    return out
+
+
 def triangulate(W: int, H: int, sorted_seeds, P: int = DEFAULT_BORDER_PADDING,
                 mode="reference", vgrid=None):
     """The batch pipeline of triangulation.cu:143-365.
@@ -262,7 +276,7 @@ def incremental(W: int, H: int, batches, P: int = DEFAULT_BORDER_PADDING):
         tris = tris[o]
         raw = raw[o]
     sx, sy = xs[order], ys[order]
-    tgrid = assign(W, H, sx, sy, tris) if n else np.full((H, W), -1, np.int32)
+    tgrid = assign_bbox(W, H, sx, sy, tris) if n else np.full((H, W), -1, np.int32)
     inner = lab[P:P + H, P:P + W]
     grid = np.empty((H, W, 3), dtype=np.int32)
     ok = inner >= 0

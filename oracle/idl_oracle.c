@@ -21,6 +21,7 @@
  *                          deterministic (smallest row-major block index)
  *   or_assign              src/cuda/triangulation.cu:79-137,355-368 and
  *                          src/cuda/geometry_device.cuh:68-86
+ *   or_assign_bbox_rows    the same rule per triangle over its bounding box
  *   or_triangulate         src/cuda/triangulation.cu:143-365
  *
  * Parity is pinned in tests/ against golden vectors generated from the
@@ -451,6 +452,55 @@ void or_assign(int W, int H, const int32_t* sx, const int32_t* sy, int n,
         }
     }
     free(ptr); free(idx); free(fill);
+}
+
+/* The same assignment as or_assign (src/cuda/triangulation.cu:101-137: the
+ * highest triangle index whose closed float test contains the pixel, -1 if
+ * none), evaluated per triangle over its bounding box instead of per pixel over
+ * the seed window.  A triangle containing a pixel has the pixel inside its
+ * bounding box, and the window of or_assign reaches every such triangle (its
+ * cap exceeds the longest side), so both loops find the same containing
+ * triangles with the same test; this one costs the triangles' box areas
+ * instead of pixels x seeds, which makes full-size checks feasible.  Rows
+ * [y0, y1) of the W x H grid into tgrid_rows. */
+void or_assign_bbox_rows(int W, int H, const int32_t* sx, const int32_t* sy, const int32_t* tris, int64_t ntri,
+                         int y0, int y1, int32_t* tgrid_rows)
+{
+    (void)H;
+    const size_t n_px = (size_t)(y1 - y0) * W;
+    for (size_t i = 0; i < n_px; ++i) tgrid_rows[i] = -1;
+    int nthreads = 1;
+#ifdef _OPENMP
+    nthreads = omp_get_max_threads();
+#endif
+    const int rows = y1 - y0;
+    const int chunk = (rows + nthreads - 1) / nthreads;
+#pragma omp parallel for schedule(static, 1)
+    for (int c = 0; c < nthreads; ++c) {
+        const int r0 = y0 + c * chunk, r1 = r0 + chunk < y1 ? r0 + chunk : y1;
+        if (r0 >= r1) continue;
+        for (int64_t t = 0; t < ntri; ++t) {     /* ascending: a later containing triangle wins */
+            const int32_t* v = tris + t * 5 + 2;
+            const int ax = sx[v[0]], ay = sy[v[0]], bx = sx[v[1]], by = sy[v[1]], cx = sx[v[2]], cy = sy[v[2]];
+            int lo_y = ay < by ? ay : by;
+            lo_y = lo_y < cy ? lo_y : cy;
+            int hi_y = ay > by ? ay : by;
+            hi_y = hi_y > cy ? hi_y : cy;
+            if (hi_y < r0 || lo_y >= r1) continue;
+            int lo_x = ax < bx ? ax : bx;
+            lo_x = lo_x < cx ? lo_x : cx;
+            int hi_x = ax > bx ? ax : bx;
+            hi_x = hi_x > cx ? hi_x : cx;
+            if (lo_x < 0) lo_x = 0;
+            if (hi_x > W - 1) hi_x = W - 1;
+            if (lo_y < r0) lo_y = r0;
+            if (hi_y > r1 - 1) hi_y = r1 - 1;
+            for (int y = lo_y; y <= hi_y; ++y)
+                for (int x = lo_x; x <= hi_x; ++x)
+                    if (pit_f((float)x, (float)y, (float)ax, (float)ay, (float)bx, (float)by, (float)cx, (float)cy))
+                        tgrid_rows[(size_t)(y - y0) * W + x] = (int32_t)t;
+        }
+    }
 }
 
 /* assignment restricted to rows [y0, y1), for bounded CPU-baseline samples */

@@ -241,23 +241,35 @@ def test_triangulate_4096_200k_vs_reference_cuda(kind):
 @pytest.mark.parametrize("kind", ["uniform", "clustered"])
 def test_propagation_schedules_agree(kind):
     """Tile rounds for the first passes and the persistent kernel for the
-    tail, switched at any round, give the Jacobi fixed point bit for bit."""
+    tail, switched at any round, under every tile shape, give the Jacobi
+    fixed point bit for bit; so does the Voronoi entry point, which has no
+    padding."""
     from integer_delauney_b200 import _capi, autotune
     W, H = 700, 500
     seeds = random_seeds(W, H, 3000, 31) if kind == "uniform" else clustered_seeds(W, H, 3000, 31, blobs=5,
                                                                                      sigma=15.0)
     s = oracle.sort_seeds(seeds, W, H)
     o_tris, o_grid, _ = oracle.triangulate(W, H, s, 16)
+    o_vor, _ = oracle.voronoi("reference", W, H, s)
     ctx = _capi.context_for(0)
     try:
-        for sched in (0, 1, 2, 5, -1):
+        n_shapes = ctx.set_tile(0)
+        assert n_shapes >= 4
+        for sched, shape in autotune.candidates(n_shapes, (0, 1, 2, 5, -1)):
             ctx.set_schedule(sched)
+            ctx.set_tile(shape)
             tm, grid = cu.triangulate(W, H, seeds, 16)
-            np.testing.assert_array_equal(grid, o_grid, err_msg=f"schedule {sched}")
-            np.testing.assert_array_equal(_tris_array(tm), o_tris, err_msg=f"schedule {sched}")
-        assert autotune.tune(W, H, seeds, 16, candidates=(0, 1, 2), repeats=1, context=ctx) in (0, 1, 2)
+            np.testing.assert_array_equal(grid, o_grid, err_msg=f"schedule {sched}, tile {shape}")
+            np.testing.assert_array_equal(_tris_array(tm), o_tris, err_msg=f"schedule {sched}, tile {shape}")
+            np.testing.assert_array_equal(cu.Voronoi().compute(W, H, seeds), o_vor,
+                                          err_msg=f"schedule {sched}, tile {shape}")
+        choice = autotune.tune(W, H, seeds, 16, schedules=(0, 1, -1), repeats=1, context=ctx)
+        assert choice in autotune.candidates(n_shapes, (0, 1, -1))
+        with pytest.raises(ValueError):
+            ctx.set_tile(n_shapes)
     finally:
         ctx.set_schedule(1)
+        ctx.set_tile(0)
 
 
 @pytest.mark.parametrize("kind", ["uniform", "clustered"])

@@ -263,3 +263,20 @@ def test_collinear_triangle_covers_its_line_within_the_window():
         if max(abs(k - 5), abs(k - 5)) <= wc or max(abs(k - 15), abs(k - 15)) <= wc:
             on_line[k, k] = True
     np.testing.assert_array_equal(t == 0, on_line)
+
+
+@pytest.mark.parametrize("W,H,n,kind", [(200, 150, 300, "uniform"), (512, 512, 2000, "uniform"),
+                                        (300, 300, 500, "clustered"), (97, 61, 40, "uniform")])
+def test_bounding_box_assignment_equals_windowed(W, H, n, kind):
+    """assign_bbox (per triangle over its bounding box) is the reference's
+    windowed per-pixel assignment (triangulation.cu:101-137) evaluated in
+    another order: same grid, whole and by row bands."""
+    from integer_delauney_b200.workloads import clustered, uniform
+    seeds = uniform(W, H, n, seed=n) if kind == "uniform" else clustered(W, H, n, seed=n, blobs=4, sigma=10.0)
+    s = oracle.sort_seeds(seeds, W, H)
+    tris, grid, _ = oracle.triangulate(W, H, s, 16)
+    want = oracle.assign(W, H, s[:, 0], s[:, 1], tris)
+    np.testing.assert_array_equal(want, grid[:, :, 2])
+    np.testing.assert_array_equal(oracle.assign_bbox(W, H, s[:, 0], s[:, 1], tris), want)
+    y0, y1 = H // 3, H // 3 + 7
+    np.testing.assert_array_equal(oracle.assign_bbox(W, H, s[:, 0], s[:, 1], tris, y0, y1), want[y0:y1])
