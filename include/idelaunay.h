@@ -370,6 +370,14 @@ IDL_API int idl_delaunay_insert_ordered(idl_delaunay* d, const int32_t* seeds_xy
  * copy; src may then run its next batch. */
 IDL_API int idl_delaunay_adopt(idl_delaunay* d, idl_context* src, int image);
 
+/* idl_delaunay_adopt for a group of n (1..16) distinct empty objects at once:
+ * objs[k] adopts image images[k] of the last batch on `src`.  One launch
+ * copies every image's labels and seeds, one host copy fills the host mirrors,
+ * and the call waits for its stream once, instead of once per object.  All
+ * objects must share one stream and device.  Each object ends in the state
+ * idl_delaunay_adopt would leave it in.  No counterpart in the reference. */
+IDL_API int idl_delaunay_adopt_group(idl_delaunay* const* objs, const int* images, int n, idl_context* src);
+
 /* Delaunay::finalise (src/cuda/delaunay.cu:325-347): assign pixels for the
  * pending changes and write the (height, width, 3) int32 grid (batch seed id,
  * squared distance, triangle id) to host grid_out (may be NULL).  Reports the

@@ -70,6 +70,7 @@ SIGNATURES = {
     "idl_delaunay_destroy": (_i32, [_vp]),
     "idl_delaunay_reset": (_i32, [_vp, _i32, _i32, _i64, _i32]),
     "idl_delaunay_set_workspace": (_i32, [_vp, _vp]),
+    "idl_delaunay_adopt_group": (_i32, [_vp, _vp, _i32, _vp]),
     "idl_delaunay_adopt": (_i32, [_vp, _vp, _i32]),
     "idl_delaunay_set_stream": (_i32, [_vp, _vp]),
     "idl_delaunay_insert": (_i32, [_vp, _vp, _i64, _vp, _vp]),

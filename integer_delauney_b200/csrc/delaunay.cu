@@ -270,6 +270,49 @@ __global__ void k_split(const int32_t* __restrict__ xy, int64_t k, int32_t* __re
     y[i] = xy[2 * i + 1];
 }
 
+// A group of objects adopting images of one batch: per image the label rows
+// (as k_adopt) and the seed coordinates and packed positions (as the copies
+// and k_pack_pos of idl_delaunay_adopt), all in one launch; blockIdx.y picks
+// the image.
+constexpr int ADOPT_GROUP_MAX = 16;
+struct AdoptItem {
+    const int32_t* atlas;
+    const int32_t* sxs;
+    const int32_t* sys;
+    int32_t* a;
+    int32_t* b;
+    int32_t* ix;
+    int32_t* iy;
+    uint32_t* pos;
+    long long seed_off, n;
+    int apitch, ox, oy, Wd, Hd, pitch, P;
+};
+struct AdoptGroup {
+    AdoptItem it[ADOPT_GROUP_MAX];
+};
+
+__global__ void k_adopt_group(AdoptGroup g)
+{
+    const AdoptItem& m = g.it[blockIdx.y];
+    for (int r = blockIdx.x; r < m.Hd; r += gridDim.x) {
+        const int32_t* src = m.atlas + (size_t)(m.oy + r) * m.apitch + m.ox;
+        const size_t o = (size_t)r * m.pitch;
+        for (int c = threadIdx.x; c < m.Wd; c += blockDim.x) {
+            const int32_t l = src[c];
+            const int32_t v = l >= 0 ? (int32_t)(l - m.seed_off) : UNDEF;
+            m.a[o + c] = v;
+            m.b[o + c] = v;
+        }
+    }
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < m.n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int32_t x = m.sxs[m.seed_off + i], y = m.sys[m.seed_off + i];
+        m.ix[i] = x;
+        m.iy[i] = y;
+        m.pos[i] = pack_pos(x + m.P, y + m.P);
+    }
+}
+
 __global__ void k_pack_pos(const int32_t* __restrict__ x, const int32_t* __restrict__ y, int64_t k, int P,
                            uint32_t* __restrict__ pos)
 {
@@ -979,6 +1022,81 @@ int idl_delaunay_adopt(idl_delaunay* d, idl_context* src, int image)
     d->N = n;
     d->rank_dirty = d->topo_dirty = d->raster_dirty = d->edges_dirty = true;
     d->pending = true;
+    IDL_API_END
+}
+
+int idl_delaunay_adopt_group(idl_delaunay* const* objs, const int* images, int n, idl_context* src)
+{
+    IDL_API_BEGIN
+    if (!objs || !images) invalid("arguments must not be NULL");
+    if (n < 1 || n > ADOPT_GROUP_MAX) invalid("a group holds 1 to 16 objects");
+    if (!src) invalid("context must not be NULL");
+    AdoptGroup g{};
+    int64_t lo = INT64_MAX, hi = 0;
+    int max_hd = 1;
+    std::vector<BatchImage> bis(n);
+    for (int k = 0; k < n; ++k) {
+        idl_delaunay* d = objs[k];
+        check_handle(d);
+        BatchImage& bi = bis[k];
+        if (!batch_image(*src, images[k], bi)) invalid("the context holds no batch with that image");
+        if (src->device != d->device) invalid("the batch was computed on another device");
+        if (bi.W != d->W || bi.H != d->H || bi.P != d->P)
+            invalid("the batch image's size or border padding differs from the object's");
+        if (d->N != 0) invalid("adopt needs an empty object (reset it first)");
+        if (d->mode != IDL_MODE_REFERENCE) invalid("adopt takes labels of reference semantics only");
+        if (bi.n > d->max_seeds) invalid("insert would exceed max_seeds capacity");
+        if (d->stream != objs[0]->stream || d->device != objs[0]->device)
+            invalid("the objects of a group must share one stream and device");
+        for (int j = 0; j < k; ++j)
+            if (objs[j] == d) invalid("an object appears twice in the group");
+        AdoptItem& m = g.it[k];
+        m.atlas = src->lab[0].as<int32_t>();
+        m.sxs = src->xs.as<int32_t>();
+        m.sys = src->ys.as<int32_t>();
+        m.a = d->planes;
+        m.b = d->planes + (size_t)d->pitch * d->Hd;
+        m.ix = d->ix;
+        m.iy = d->iy;
+        m.pos = d->pos;
+        m.seed_off = bi.seed_off;
+        m.n = bi.n;
+        m.apitch = bi.pitch;
+        m.ox = bi.ox;
+        m.oy = bi.oy;
+        m.Wd = d->Wd;
+        m.Hd = d->Hd;
+        m.pitch = d->pitch;
+        m.P = d->P;
+        max_hd = std::max(max_hd, d->Hd);
+        lo = std::min<int64_t>(lo, bi.seed_off);
+        hi = std::max<int64_t>(hi, bi.seed_off + bi.n);
+    }
+    idl_delaunay* d0 = objs[0];
+    DeviceGuard guard(d0->device);
+    const cudaStream_t st = d0->stream;
+    k_adopt_group<<<dim3((unsigned)std::min(max_hd, 1024), (unsigned)n), 256, 0, st>>>(g);
+    IDL_LAUNCH();
+    // host mirrors of every image's seeds: one copy of the group's range
+    std::vector<int32_t> hx((size_t)(hi - lo)), hy((size_t)(hi - lo));
+    if (hi > lo) {
+        IDL_CUDA(cudaMemcpyAsync(hx.data(), src->xs.as<int32_t>() + lo, (size_t)(hi - lo) * 4,
+                                 cudaMemcpyDeviceToHost, st));
+        IDL_CUDA(cudaMemcpyAsync(hy.data(), src->ys.as<int32_t>() + lo, (size_t)(hi - lo) * 4,
+                                 cudaMemcpyDeviceToHost, st));
+    }
+    IDL_CUDA(cudaStreamSynchronize(st));
+    for (int k = 0; k < n; ++k) {
+        idl_delaunay* d = objs[k];
+        const BatchImage& bi = bis[k];
+        d->hx.assign(hx.begin() + (bi.seed_off - lo), hx.begin() + (bi.seed_off - lo + bi.n));
+        d->hy.assign(hy.begin() + (bi.seed_off - lo), hy.begin() + (bi.seed_off - lo + bi.n));
+        ++d->generation;
+        d->N = bi.n;
+        d->rank_dirty = d->topo_dirty = d->raster_dirty = d->edges_dirty = true;
+        d->pending = true;
+        d->note_use();
+    }
     IDL_API_END
 }
 

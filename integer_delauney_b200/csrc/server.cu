@@ -25,6 +25,7 @@
 #include "context.cuh"
 #include "scheduler.h"
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <mutex>
@@ -182,6 +183,89 @@ void execute(idl_server& S, Slot& slot, const Item& it, int64_t batch_tris, int 
     o.done = true;
 }
 
+// A group of new diagrams whose batch succeeded: every object is made ready
+// (fresh or pooled, reset to its canvas), then all adopt their images at once
+// (idl_delaunay_adopt_group: one launch, one wait), and the fetched results
+// are copied from the batch with one more wait for the whole group.  A
+// request whose object cannot be made ready fails alone.
+void execute_group(idl_server& S, Slot& slot, const std::vector<Item>& work, const std::vector<int64_t>& batch_tris,
+                   int64_t start, std::vector<Outcome>& outs, std::vector<void*>& objs, std::vector<Capacity>& caps,
+                   std::vector<int64_t>& dev_bytes)
+{
+    const int P = S.sched.padding();
+    std::vector<idl_delaunay*> ready;
+    std::vector<int> images;
+    for (size_t k = 0; k < work.size(); ++k) {
+        const Request& r = work[k].req;
+        Outcome& o = outs[k];
+        o.kind = r.kind;
+        o.diagram = r.diagram;
+        o.arrival_ns = r.arrival_ns;
+        o.start_ns = start;
+        idl_delaunay* obj = static_cast<idl_delaunay*>(work[k].obj);
+        try {
+            const int64_t ms = r.n_seeds() + SEED_HEADROOM;
+            if (obj) {
+                caps[k] = work[k].cap;
+            } else {
+                const int Wc = class_dim(r.W), Hc = class_dim(r.H);
+                check_status(idl_delaunay_create(S.device, Wc, Hc, ms, P, S.mode, &obj));
+                caps[k] = capacity(Wc, Hc, ms, P);
+            }
+            objs[k] = obj;
+            check_status(idl_delaunay_set_stream(obj, slot.stream));
+            check_status(idl_delaunay_set_workspace(obj, slot.ws));
+            check_status(idl_delaunay_reset(obj, r.W, r.H, ms, P));
+            o.n_seeds = r.n_seeds();
+            ready.push_back(obj);
+            images.push_back((int)k);
+        } catch (const idl::Error& e) {
+            o.status = e.status;
+            o.error = e.what();
+            o.done_ns = clock_ns();
+            o.done = true;
+        } catch (const std::exception& e) {
+            o.status = IDL_ERR_INTERNAL;
+            o.error = e.what();
+            o.done_ns = clock_ns();
+            o.done = true;
+        }
+    }
+    if (ready.empty()) return;
+    int status = IDL_OK;
+    std::string error;
+    try {
+        check_status(idl_delaunay_adopt_group(ready.data(), images.data(), (int)ready.size(), slot.batch));
+        for (int k : images) {
+            outs[k].n_triangles = batch_tris[k];
+            if (work[k].req.fetch) {
+                outs[k].tris.resize((size_t)batch_tris[k] * 5);
+                idl::batch_fetch(*slot.batch, k, work[k].req.grid_out, outs[k].tris.data(),
+                                 (int64_t)outs[k].tris.size());
+            }
+        }
+        IDL_CUDA(cudaStreamSynchronize(slot.stream));
+        for (size_t j = 0; j < ready.size(); ++j) {
+            int64_t info[IDL_DI_COUNT];
+            check_status(idl_delaunay_info(ready[j], info, IDL_DI_COUNT));
+            dev_bytes[images[j]] = info[IDL_DI_DEVICE_BYTES];
+        }
+    } catch (const idl::Error& e) {
+        status = e.status;
+        error = e.what();
+    } catch (const std::exception& e) {
+        status = IDL_ERR_INTERNAL;
+        error = e.what();
+    }
+    const int64_t done = clock_ns();
+    for (int k : images) {
+        outs[k].status = status;
+        outs[k].error = error;
+        outs[k].done_ns = done;
+        outs[k].done = true;
+    }
+}
+
 void destroy_all(std::vector<void*>& objs)
 {
     for (void* p : objs) idl_delaunay_destroy(static_cast<idl_delaunay*>(p));
@@ -240,13 +324,28 @@ void worker_loop(idl_server* Sp, int index)
             std::lock_guard<std::mutex> lk(S.mu);
             S.sched.count_group((int)work.size());
         }
+        // a whole group that the batch took: adopt all of its images at once
+        const bool grouped = work[0].req.kind == NEW && S.mode == IDL_MODE_REFERENCE &&
+                             std::all_of(batch_tris.begin(), batch_tris.end(), [](int64_t t) { return t >= 0; });
+        std::vector<Outcome> outs(grouped ? work.size() : 0);
+        std::vector<void*> g_objs(outs.size(), nullptr);
+        std::vector<Capacity> g_caps(outs.size());
+        std::vector<int64_t> g_bytes(outs.size(), 0);
+        if (grouped) execute_group(S, slot, work, batch_tris, start, outs, g_objs, g_caps, g_bytes);
         for (size_t k = 0; k < work.size(); ++k) {
             const Item& it = work[k];
             Outcome o;
             void* obj = nullptr;
             Capacity cap;
             int64_t dev_bytes = 0;
-            execute(S, slot, it, batch_tris[k], (int)k, start, o, obj, cap, dev_bytes);
+            if (grouped) {
+                o = std::move(outs[k]);
+                obj = g_objs[k];
+                cap = g_caps[k];
+                dev_bytes = g_bytes[k];
+            } else {
+                execute(S, slot, it, batch_tris[k], (int)k, start, o, obj, cap, dev_bytes);
+            }
             void* drop = nullptr;
             {
                 std::lock_guard<std::mutex> lk(S.mu);

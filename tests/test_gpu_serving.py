@@ -140,6 +140,43 @@ def test_adopt_from_a_batch_equals_ordered_insert(cu):
         cu.Delaunay(7, 7, 10, 16)._adopt(ctx, 0)          # size differs from the batch image
 
 
+def test_adopt_group_equals_adopting_one_by_one(cu):
+    """idl_delaunay_adopt_group (every image of a group in one launch and one
+    wait) leaves each object exactly as idl_delaunay_adopt of its image does."""
+    import ctypes
+    import torch
+    from integer_delauney_b200 import _capi
+    news, _ = _requests(5, n_new=6)
+    ctx = _capi.Context(0)
+    lib = _capi.load()
+    stream = torch.cuda.current_stream().cuda_stream
+    ctx.set_stream(stream)
+    dims = np.array([(W, H) for W, H, _ in news], dtype=np.int32)
+    counts = np.array([len(p) for _, _, p in news], dtype=np.int64)
+    seeds = np.ascontiguousarray(np.concatenate([p for _, _, p in news]), dtype=np.int32)
+    _capi.check(lib.idl_voronoi_batch(ctx.handle, len(news), dims.ctypes.data, counts.ctypes.data,
+                                      seeds.ctypes.data, 16, 0))
+    group = [cu.Delaunay(W, H, len(p) + 50, 16) for W, H, p in news]
+    order = [4, 1, 5, 0, 3, 2]                      # any order of the group's images
+    for o in group:
+        _capi.check(lib.idl_delaunay_set_stream(o._h, stream))
+    handles = (ctypes.c_void_p * len(order))(*[group[k]._h.value for k in order])
+    images = (ctypes.c_int * len(order))(*order)
+    _capi.check(lib.idl_delaunay_adopt_group(handles, images, len(order), ctx.handle))
+    for k, (W, H, pts) in enumerate(news):
+        one = cu.Delaunay(W, H, len(pts) + 50, 16)
+        one._adopt(ctx, k)
+        np.testing.assert_array_equal(group[k].get_voronoi_grid(), one.get_voronoi_grid())
+        np.testing.assert_array_equal(group[k].get_seeds(), one.get_seeds())
+        va, ga = group[k].finalise(as_arrays=True)
+        vb, gb = one.finalise(as_arrays=True)
+        np.testing.assert_array_equal(va, vb)
+        np.testing.assert_array_equal(ga, gb)
+    twice = (ctypes.c_void_p * 2)(group[0]._h.value, group[0]._h.value)
+    assert lib.idl_delaunay_adopt_group(twice, (ctypes.c_int * 2)(0, 0), 2, ctx.handle) == _capi.IDL_ERR_INVALID
+    assert lib.idl_delaunay_adopt_group(handles, images, 17, ctx.handle) == _capi.IDL_ERR_INVALID
+
+
 def test_exact_mode_server_equals_exact_triangulate(cu):
     from integer_delauney_b200.serving import Server
     news, inserts = _requests(4, n_new=5)
