@@ -19,9 +19,10 @@
 // different columns at equal distance are ordered by column, i.e. by id.
 // Seed ids are (x asc, y asc) ranks, so "higher id" is a comparison of ids.
 //
-// Work is O(cells x distance to the nearest seed / 1 px) in the row phase:
-// dense seed sets (a few px apart) finish in a handful of column reads per
-// cell; cells in large empty regions scan further.
+// Work in the row phase: dense seed sets (a few px apart) finish in a handful
+// of column reads per cell; in large empty regions the scan jumps over whole
+// blocks of columns that cannot hold a candidate as near as the best so far,
+// so it tests about distance / 32 blocks instead of distance columns.
 #include "context.cuh"
 
 namespace idl {
@@ -83,29 +84,34 @@ __global__ void k_col_nearest(const uint32_t* __restrict__ pos, const int32_t* _
     }
 }
 
-// Phase 2: best column candidate of the row, scanning outward.
-__global__ void k_row_nearest(const int32_t* __restrict__ col, const int32_t* __restrict__ coldy, int Wd, int Hd,
-                              int pitch, int32_t* __restrict__ lab)
+// Phase 2: best column candidate of the row, scanning outward.  One block
+// per row.  The row's columns are grouped in blocks of RB; s_min[b] is the
+// smallest dy^2 among block b's candidates.  When the scan reaches a block's
+// nearest column at distance k, every candidate of the block costs at least
+// k^2 + s_min[b]; if that exceeds the best distance so far, nothing in the
+// block can beat or tie it and the scan jumps over it.  Cells far from every
+// seed (clustered inputs) thus test blocks instead of columns; the scan still
+// stops once k^2 exceeds the best distance.
+constexpr int RB = 32;
+constexpr int ROW_THREADS = 512;
+
+__device__ __forceinline__ void scan_side(const int32_t* __restrict__ row, const int32_t* __restrict__ rdy,
+                                          const int32_t* __restrict__ s_min, int x, int Wd, int dir, int32_t& bl,
+                                          long long& bd)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= Wd) return;
-    const int32_t* row = col + (size_t)y * pitch;
-    const int32_t* rdy = coldy + (size_t)y * pitch;
-    int32_t bl = row[x];
-    long long bd = 0x7FFFFFFFFFFFFFFFll;
-    if (bl >= 0) {
-        const long long dy = rdy[x];
-        bd = dy * dy;
-    }
-    for (int k = 1;; ++k) {
+    int k = 1;
+    for (;;) {
+        const int xx = x + dir * k;
+        if (xx < 0 || xx >= Wd) return;
         const long long kk = (long long)k * k;
-        if (kk > bd || (x - k < 0 && x + k >= Wd)) break;
-#pragma unroll
-        for (int side = 0; side < 2; ++side) {
-            const int xx = side ? x + k : x - k;
-            if (xx < 0 || xx >= Wd) continue;
-            const int32_t l = row[xx];
-            if (l < 0) continue;
+        if (kk > bd) return;
+        const bool entering = dir > 0 ? (xx % RB) == 0 : (xx % RB) == RB - 1;
+        if (entering && kk + s_min[xx / RB] > bd) {
+            k += RB;
+            continue;
+        }
+        const int32_t l = row[xx];
+        if (l >= 0) {
             const long long dy = rdy[xx];
             const long long d = kk + dy * dy;
             if (d < bd || (d == bd && l > bl)) {
@@ -113,8 +119,43 @@ __global__ void k_row_nearest(const int32_t* __restrict__ col, const int32_t* __
                 bl = l;
             }
         }
+        ++k;
     }
-    lab[(size_t)y * pitch + x] = bl;
+}
+
+__global__ void __launch_bounds__(ROW_THREADS)
+k_row_nearest(const int32_t* __restrict__ col, const int32_t* __restrict__ coldy, int Wd, int pitch,
+              int32_t* __restrict__ lab)
+{
+    extern __shared__ int32_t s_min[];   // ceil(Wd / RB) entries
+    const int y = blockIdx.x;
+    const int32_t* row = col + (size_t)y * pitch;
+    const int32_t* rdy = coldy + (size_t)y * pitch;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int nb = (Wd + RB - 1) / RB;
+    for (int b = warp; b < nb; b += nwarps) {
+        const int x = b * RB + lane;
+        int32_t v = 0x7FFFFFFF;
+        if (x < Wd && row[x] >= 0) {
+            const int32_t dy = rdy[x];
+            v = dy * dy;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+        if (lane == 0) s_min[b] = v;
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < Wd; x += blockDim.x) {
+        int32_t bl = row[x];
+        long long bd = 0x7FFFFFFFFFFFFFFFll;
+        if (bl >= 0) {
+            const long long dy = rdy[x];
+            bd = dy * dy;
+        }
+        scan_side(row, rdy, s_min, x, Wd, -1, bl, bd);
+        scan_side(row, rdy, s_min, x, Wd, +1, bl, bd);
+        lab[(size_t)y * pitch + x] = bl;
+    }
 }
 
 }  // namespace
@@ -128,14 +169,14 @@ void propagate_exact(Context& C, const Canvas& cv, const uint32_t* pos, int64_t 
     int32_t* cs = C.counts.as<int32_t>();
     k_col_start<<<(unsigned)((cv.Wd + 1 + 255) / 256), 256, 0, C.stream>>>(pos, n, cv.Wd, cs);
     IDL_LAUNCH();
-    const dim3 g((unsigned)ceil_div(cv.Wd, 256), (unsigned)cv.Hd);
     C.exact_dy.ensure(plane);
     const dim3 gc((unsigned)ceil_div(cv.Wd, 128), (unsigned)ceil_div(cv.Hd, CHUNK));
     k_col_nearest<<<gc, 128, 0, C.stream>>>(pos, cs, cv.Wd, cv.Hd, cv.pitch, C.lab[1].as<int32_t>(),
                                             C.exact_dy.as<int32_t>());
     IDL_LAUNCH();
-    k_row_nearest<<<g, 256, 0, C.stream>>>(C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>(), cv.Wd, cv.Hd,
-                                           cv.pitch, C.lab[0].as<int32_t>());
+    const size_t smem = (size_t)ceil_div(cv.Wd, RB) * 4;   // at most 4 KB (Wd <= 32767)
+    k_row_nearest<<<(unsigned)cv.Hd, ROW_THREADS, smem, C.stream>>>(C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>(),
+                                                                    cv.Wd, cv.pitch, C.lab[0].as<int32_t>());
     IDL_LAUNCH();
     if (C.prof.enabled) {
         C.prof.passes = 0;
