@@ -305,6 +305,7 @@ def incremental_case(cu, torch, rank, mode="reference"):
                         f"(30% in a 256x256 hotspot), P={PADDING}, {mode} mode",
             "insert_ms_mean": t_all * 1e3 / len(batches), "insert_ms_p50": lat_ms[len(lat_ms) // 2],
             "insert_ms_p99": lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))],
+            "slowest_inserts": [[int(i), round(lat[i] * 1e3, 2)] for i in np.argsort(lat)[::-1][:4]],
             "insert_mpix_s": Wi * Hi * len(batches) / t_all / 1e6,
             "deferred_total_ms": t_def * 1e3, "triangles_final": n_tri,
             "d2h_bytes_per_insert": Wi * Hi * 12}

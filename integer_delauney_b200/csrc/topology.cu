@@ -168,26 +168,58 @@ __device__ __forceinline__ void hash_insert(unsigned long long key, unsigned lon
     atomicOr(&sc->overflow, 1);
 }
 
+// One thread per column and strip of DETECT_STRIP block rows, a warp per 32
+// adjacent columns: each label row is loaded once (the block's right column
+// comes from the next lane) and becomes the next block's top row.  A key is
+// not inserted again when the same column's block one row up, or the block
+// one column left (the previous lane), emitted it: that block's row-major
+// index is smaller, so the atomicMin it did already keeps a smaller witness
+// than this one would.
+constexpr int DETECT_STRIP = 16;
+
 __global__ void __launch_bounds__(256)
 k_detect(const int32_t* __restrict__ lab, int pitch, int Wd, int Hd, const uint32_t* __restrict__ pos,
          const int32_t* __restrict__ rank, unsigned long long* __restrict__ keys,
          unsigned long long* __restrict__ vals, unsigned long long mask, Scalars* __restrict__ sc)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= Wd - 1 || y >= Hd - 1) return;
-    const int32_t a = lab[(size_t)y * pitch + x], b = lab[(size_t)y * pitch + x + 1];
-    const int32_t c = lab[(size_t)(y + 1) * pitch + x], d = lab[(size_t)(y + 1) * pitch + x + 1];
-    if (a == b && a == c && a == d) return;
-    if ((a == b && c == d) || (a == c && b == d)) return;   // two regions: no vertex
-    Emit e;
-    block_rule(a, b, c, d, pos, e);
-    const unsigned long long blk = (unsigned long long)y * Wd + x;
-    for (int k = 0; k < e.n; ++k) {
-        unsigned long long key;
-        unsigned code;
-        make_key(e.o[k], rank, key, code);
-        hash_insert(key, (blk << 4) | code, keys, vals, mask, sc);
+    const int lane = threadIdx.x;
+    const int x = blockIdx.x * 32 + lane;
+    const int y0 = (blockIdx.y * blockDim.y + threadIdx.y) * DETECT_STRIP;
+    if (y0 >= Hd - 1) return;   // uniform over the warp
+    const int y1 = min(y0 + DETECT_STRIP, Hd - 1);
+    const bool has_block = x < Wd - 1;
+    auto load_row = [&](int y, int32_t& l, int32_t& r) {
+        const int32_t* row = lab + (size_t)y * pitch;
+        l = x < Wd ? row[x] : -2;
+        r = __shfl_down_sync(0xffffffffu, l, 1);
+        if (lane == 31) r = x + 1 < Wd ? row[x + 1] : -2;
+    };
+    int32_t a, b;
+    load_row(y0, a, b);
+    const unsigned long long none = EMPTY_KEY;
+    unsigned long long up0 = none, up1 = none;   // keys this column's block emitted one row up
+    for (int y = y0; y < y1; ++y) {
+        int32_t c, d;
+        load_row(y + 1, c, d);
+        unsigned long long k0 = none, k1 = none;
+        unsigned code0 = 0, code1 = 0;
+        if (has_block && !(a == b && a == c && a == d) && !((a == b && c == d) || (a == c && b == d))) {
+            Emit e;
+            block_rule(a, b, c, d, pos, e);
+            if (e.n > 0) make_key(e.o[0], rank, k0, code0);
+            if (e.n > 1) make_key(e.o[1], rank, k1, code1);
+        }
+        const unsigned long long l0 = __shfl_up_sync(0xffffffffu, k0, 1), l1 = __shfl_up_sync(0xffffffffu, k1, 1);
+        const unsigned long long blk = (unsigned long long)y * Wd + x;
+        auto seen = [&](unsigned long long k) {
+            return k == up0 || k == up1 || (lane > 0 && (k == l0 || k == l1));
+        };
+        if (k0 != none && !seen(k0)) hash_insert(k0, (blk << 4) | code0, keys, vals, mask, sc);
+        if (k1 != none && !seen(k1)) hash_insert(k1, (blk << 4) | code1, keys, vals, mask, sc);
+        up0 = k0;
+        up1 = k1;
+        a = c;
+        b = d;
     }
 }
 
@@ -287,7 +319,7 @@ void detect_triangles(Context& C, const Canvas& cv, const int32_t* labels, const
         IDL_CUDA(cudaMemsetAsync(C.cnt.ptr, 0, (size_t)(n + 1) * 4, C.stream));
 
         dim3 blk(32, 8);
-        dim3 grd(ceil_div(std::max(cv.Wd - 1, 1), 32), ceil_div(std::max(cv.Hd - 1, 1), 8));
+        dim3 grd(ceil_div(std::max(cv.Wd - 1, 1), 32), ceil_div(std::max(cv.Hd - 1, 1), 8 * DETECT_STRIP));
         k_detect<<<grd, blk, 0, C.stream>>>(labels, cv.pitch, cv.Wd, cv.Hd, pos, rank, C.hkeys.as<unsigned long long>(),
                                             C.hvals.as<unsigned long long>(), (unsigned long long)(cap - 1), C.sc());
         IDL_LAUNCH();
