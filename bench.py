@@ -627,7 +627,11 @@ def run_ours(args, rank, world):
     # propagation schedule for this input class, picked by timing the
     # candidates (untimed; every schedule gives the same result)
     from integer_delauney_b200 import autotune
-    schedule = autotune.tune(W, H, seeds_u, PADDING, context=ctx)
+    if args.schedule is not None:
+        schedule = (args.schedule, args.tile)
+        autotune.apply(ctx, schedule)
+    else:
+        schedule = autotune.tune(W, H, seeds_u, PADDING, context=ctx)
     ctx.set_stream(stream.cuda_stream)
     # headline: K plain steps; the per-stage events are recorded in a second
     # timed run, since profiling reads counters back between stages
@@ -654,11 +658,22 @@ def run_ours(args, rank, world):
     dom_kernel = dominant if dominant in roof else "propagate_ms"
     achieved = roof[dom_kernel]
 
-    # clustered variant (same size), device path
+    if args.device_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "Mpixel/s", "ms_per_step": ms / args.steps,
+                              "stages_ms": {k[:-3]: round(v, 4) for k, v in stage.items()},
+                              "schedule": schedule, "passes": p0["passes"], "gpu_launches": int(launches),
+                              "roofline_achieved_gbs": achieved, "clocks": clocks}), flush=True)
+        return
+
+    # clustered variant (same size), device path, with its own tuned schedule
     seeds_c = clustered(W, H, N_SEEDS, seed=rank)
+    schedule_c = schedule if args.schedule is not None else autotune.tune(W, H, seeds_c, PADDING, context=ctx)
+    ctx.set_stream(stream.cuda_stream)
     c_steps = max(1, args.steps // 2)
     ms_c, profs_c, _, _ = time_device(seeds_c, c_steps, 1, profile=True)
     value_c = world * W * H * c_steps / (ms_c / 1e3) / 1e6
+    autotune.apply(ctx, schedule)
 
     # end to end through the public drop-in call, pinned host seeds
     pinned = torch.from_numpy(seeds_u).pin_memory()
@@ -741,7 +756,7 @@ def run_ours(args, rank, world):
                      "traffic": TRAFFIC_PER_LAUNCH.get(dom_kernel),
                      "per_stage_gbs": {k[:-3]: v for k, v in roof.items()}},
         "clustered": {"value": value_c, "unit": "Mpixel/s", "ms_per_step": ms_c / c_steps,
-                      "passes": profs_c[-1]["passes"], "rounds": profs_c[-1]["rounds"],
+                      "schedule": schedule_c, "passes": profs_c[-1]["passes"], "rounds": profs_c[-1]["rounds"],
                       "stages_ms": {k[:-3]: round(statistics.mean(p[k] for p in profs_c), 4) for k in keys}},
         "e2e": {"value": e2e, "unit": "Mpixel/s", "ms_per_step": ms_e / e_steps,
                 "h2d_bytes_per_step": int(seeds_u.nbytes),
@@ -767,6 +782,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--ref-rows", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--device-only", action="store_true",
+                    help="time only the device-resident 4096 x 4096 step (for profiler captures)")
+    ap.add_argument("--schedule", type=int, default=None,
+                    help="propagation schedule instead of the autotuned one (idl_context_set_schedule)")
+    ap.add_argument("--tile", type=int, default=0, help="tile shape with --schedule (idl_context_set_tile)")
     ap.add_argument("--serve-seconds", type=float, default=10.0,
                     help="length of the real-time serving trace (0 skips the serving measurement)")
     args = ap.parse_args()

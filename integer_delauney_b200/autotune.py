@@ -17,9 +17,9 @@ Where each pays depends on the seed density and layout: dense, uniform seed
 sets change most of the canvas for the first few passes, clustered ones leave
 long thin fronts.  ``tune`` times one representative input under every
 candidate (schedule, shape) on the device and keeps the fastest for that
-input's class (canvas size and density, both on a log scale), so a stream of
-similar inputs is tuned once.  Every candidate gives the same result bit for
-bit; only the time differs.
+input's class (canvas size and density on a log scale, and how much of the
+canvas the seeds occupy), so a stream of similar inputs is tuned once.  Every
+candidate gives the same result bit for bit; only the time differs.
 """
 from __future__ import annotations
 
@@ -34,11 +34,24 @@ SCHEDULES = (0, 1, 2, 3, -1)
 _cache: dict[tuple, tuple[int, int]] = {}
 
 
-def input_class(width: int, height: int, n_seeds: int) -> tuple:
+def occupancy(width: int, height: int, seeds) -> float:
+    """Share of the canvas's 64 x 64 cells that hold at least one seed: near 1
+    for uniform seed sets, small for clustered ones (long fronts through empty
+    space), which favour other schedules at the same size and density."""
+    s = np.asarray(seeds, dtype=np.int64).reshape(-1, 2)
+    cw = (int(width) + 63) // 64
+    ch = (int(height) + 63) // 64
+    if len(s) == 0:
+        return 0.0
+    cells = np.unique((s[:, 1] // 64) * cw + s[:, 0] // 64)
+    return len(cells) / float(cw * ch)
+
+
+def input_class(width: int, height: int, n_seeds: int, occ: float = 1.0) -> tuple:
     """Inputs in one class share a tuned schedule: canvas pixels and seeds per
-    pixel, each bucketed by powers of two."""
+    pixel, each bucketed by powers of two, and the seed occupancy in quarters."""
     px = max(1, int(width) * int(height))
-    return (int(math.log2(px)), int(math.log2(max(1, int(n_seeds)) / px * 1e6 + 1)))
+    return (int(math.log2(px)), int(math.log2(max(1, int(n_seeds)) / px * 1e6 + 1)), min(4, int(occ * 4)))
 
 
 def candidates(n_shapes: int, schedules: Iterable[int] = SCHEDULES) -> list[tuple[int, int]]:
@@ -64,7 +77,7 @@ def tune(width: int, height: int, seeds, border_padding: int = _capi.AUTO_BORDER
     it.  Times idl_triangulate_device with CUDA events on the current stream."""
     import torch
     s = np.ascontiguousarray(np.asarray(seeds, dtype=np.int32).reshape(-1, 2))
-    key = input_class(width, height, len(s))
+    key = input_class(width, height, len(s), occupancy(width, height, s))
     ctx = context or _capi.context_for(torch.cuda.current_device())
     if key in _cache and not force:
         apply(ctx, _cache[key])
