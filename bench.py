@@ -624,6 +624,8 @@ def run_ours(args, rank, world):
         return ms, profs, clk.summary(), launches
 
     seeds_u = uniform(W, H, N_SEEDS, seed=rank)
+    if args.device_only and args.seeds == "clustered":
+        seeds_u = clustered(W, H, N_SEEDS, seed=rank)
     # propagation schedule for this input class, picked by timing the
     # candidates (untimed; every schedule gives the same result)
     from integer_delauney_b200 import autotune
@@ -632,6 +634,7 @@ def run_ours(args, rank, world):
         autotune.apply(ctx, schedule)
     else:
         schedule = autotune.tune(W, H, seeds_u, PADDING, context=ctx)
+    tuned_u = {f"{s},{t}": round(v, 3) for (s, t), v in autotune.last_report.items()}
     ctx.set_stream(stream.cuda_stream)
     # headline: K plain steps; the per-stage events are recorded in a second
     # timed run, since profiling reads counters back between stages
@@ -662,13 +665,15 @@ def run_ours(args, rank, world):
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "Mpixel/s", "ms_per_step": ms / args.steps,
                               "stages_ms": {k[:-3]: round(v, 4) for k, v in stage.items()},
-                              "schedule": schedule, "passes": p0["passes"], "gpu_launches": int(launches),
+                              "schedule": schedule, "autotune_ms": tuned_u, "passes": p0["passes"],
+                              "gpu_launches": int(launches),
                               "roofline_achieved_gbs": achieved, "clocks": clocks}), flush=True)
         return
 
     # clustered variant (same size), device path, with its own tuned schedule
     seeds_c = clustered(W, H, N_SEEDS, seed=rank)
     schedule_c = schedule if args.schedule is not None else autotune.tune(W, H, seeds_c, PADDING, context=ctx)
+    tuned_c = {f"{s},{t}": round(v, 3) for (s, t), v in autotune.last_report.items()}
     ctx.set_stream(stream.cuda_stream)
     c_steps = max(1, args.steps // 2)
     ms_c, profs_c, _, _ = time_device(seeds_c, c_steps, 1, profile=True)
@@ -747,7 +752,8 @@ def run_ours(args, rank, world):
                    "global_batch": world, "parallelism": f"replicas x{world}",
                    "l2": "working set > L2 (label planes 2 x 68 MB, output 201 MB); no flush"},
         "stages_ms": {k[:-3]: round(v, 4) for k, v in stage.items()},
-        "propagation": {"schedule_dense_rounds": schedule[0], "tile_shape": schedule[1], "passes": p0["passes"],
+        "propagation": {"schedule_dense_rounds": schedule[0], "tile_shape": schedule[1], "autotune_ms": tuned_u,
+                        "passes": p0["passes"],
                         "rounds": p0["rounds"],
                         "tiles": p0["tiles"],
                         "tile": [p0["tile_w"], p0["tile_h"]], "steps_per_round": p0["steps_per_round"]},
@@ -756,7 +762,8 @@ def run_ours(args, rank, world):
                      "traffic": TRAFFIC_PER_LAUNCH.get(dom_kernel),
                      "per_stage_gbs": {k[:-3]: v for k, v in roof.items()}},
         "clustered": {"value": value_c, "unit": "Mpixel/s", "ms_per_step": ms_c / c_steps,
-                      "schedule": schedule_c, "passes": profs_c[-1]["passes"], "rounds": profs_c[-1]["rounds"],
+                      "schedule": schedule_c, "autotune_ms": tuned_c, "passes": profs_c[-1]["passes"],
+                      "rounds": profs_c[-1]["rounds"],
                       "stages_ms": {k[:-3]: round(statistics.mean(p[k] for p in profs_c), 4) for k in keys}},
         "e2e": {"value": e2e, "unit": "Mpixel/s", "ms_per_step": ms_e / e_steps,
                 "h2d_bytes_per_step": int(seeds_u.nbytes),
@@ -787,6 +794,8 @@ def main():
     ap.add_argument("--schedule", type=int, default=None,
                     help="propagation schedule instead of the autotuned one (idl_context_set_schedule)")
     ap.add_argument("--tile", type=int, default=0, help="tile shape with --schedule (idl_context_set_tile)")
+    ap.add_argument("--seeds", choices=["uniform", "clustered"], default="uniform",
+                    help="seed layout of the --device-only step")
     ap.add_argument("--serve-seconds", type=float, default=10.0,
                     help="length of the real-time serving trace (0 skips the serving measurement)")
     args = ap.parse_args()

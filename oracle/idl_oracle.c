@@ -456,11 +456,15 @@ void or_assign(int W, int H, const int32_t* sx, const int32_t* sy, int n,
 
 /* The same assignment as or_assign (src/cuda/triangulation.cu:101-137: the
  * highest triangle index whose closed float test contains the pixel, -1 if
- * none), evaluated per triangle over its bounding box instead of per pixel over
- * the seed window.  A triangle containing a pixel has the pixel inside its
- * bounding box, and the window of or_assign reaches every such triangle (its
- * cap exceeds the longest side), so both loops find the same containing
- * triangles with the same test; this one costs the triangles' box areas
+ * none), evaluated per triangle instead of per pixel over the seed window.
+ * A proper triangle containing a pixel has the pixel inside its bounding box,
+ * within its longest side of every vertex and so inside the window or_assign
+ * searches; its bounding box is scanned.  A degenerate (collinear) triangle
+ * passes the closed test at every pixel of its supporting line, and or_assign
+ * finds it wherever one of its vertices lies within the window cap
+ * (Chebyshev distance); the union of those windows is scanned with that
+ * condition.  Both loops thus test the same (pixel, triangle) pairs that can
+ * succeed, with the same test; this one costs the triangles' box areas
  * instead of pixels x seeds, which makes full-size checks feasible.  Rows
  * [y0, y1) of the W x H grid into tgrid_rows. */
 void or_assign_bbox_rows(int W, int H, const int32_t* sx, const int32_t* sy, const int32_t* tris, int64_t ntri,
@@ -469,6 +473,8 @@ void or_assign_bbox_rows(int W, int H, const int32_t* sx, const int32_t* sy, con
     (void)H;
     const size_t n_px = (size_t)(y1 - y0) * W;
     for (size_t i = 0; i < n_px; ++i) tgrid_rows[i] = -1;
+    if (ntri == 0) return;
+    const int wc = or_window_cap(tris, ntri, sx, sy);
     int nthreads = 1;
 #ifdef _OPENMP
     nthreads = omp_get_max_threads();
@@ -482,23 +488,29 @@ void or_assign_bbox_rows(int W, int H, const int32_t* sx, const int32_t* sy, con
         for (int64_t t = 0; t < ntri; ++t) {     /* ascending: a later containing triangle wins */
             const int32_t* v = tris + t * 5 + 2;
             const int ax = sx[v[0]], ay = sy[v[0]], bx = sx[v[1]], by = sy[v[1]], cx = sx[v[2]], cy = sy[v[2]];
+            const int64_t area2 = (int64_t)(bx - ax) * (cy - ay) - (int64_t)(by - ay) * (cx - ax);
+            const int pad = area2 == 0 ? wc : 0;
             int lo_y = ay < by ? ay : by;
-            lo_y = lo_y < cy ? lo_y : cy;
+            lo_y = (lo_y < cy ? lo_y : cy) - pad;
             int hi_y = ay > by ? ay : by;
-            hi_y = hi_y > cy ? hi_y : cy;
+            hi_y = (hi_y > cy ? hi_y : cy) + pad;
             if (hi_y < r0 || lo_y >= r1) continue;
             int lo_x = ax < bx ? ax : bx;
-            lo_x = lo_x < cx ? lo_x : cx;
+            lo_x = (lo_x < cx ? lo_x : cx) - pad;
             int hi_x = ax > bx ? ax : bx;
-            hi_x = hi_x > cx ? hi_x : cx;
+            hi_x = (hi_x > cx ? hi_x : cx) + pad;
             if (lo_x < 0) lo_x = 0;
             if (hi_x > W - 1) hi_x = W - 1;
             if (lo_y < r0) lo_y = r0;
             if (hi_y > r1 - 1) hi_y = r1 - 1;
             for (int y = lo_y; y <= hi_y; ++y)
-                for (int x = lo_x; x <= hi_x; ++x)
+                for (int x = lo_x; x <= hi_x; ++x) {
+                    if (pad && !((abs(ax - x) <= wc && abs(ay - y) <= wc) || (abs(bx - x) <= wc && abs(by - y) <= wc) ||
+                                 (abs(cx - x) <= wc && abs(cy - y) <= wc)))
+                        continue;
                     if (pit_f((float)x, (float)y, (float)ax, (float)ay, (float)bx, (float)by, (float)cx, (float)cy))
                         tgrid_rows[(size_t)(y - y0) * W + x] = (int32_t)t;
+                }
         }
     }
 }

@@ -280,3 +280,22 @@ def test_bounding_box_assignment_equals_windowed(W, H, n, kind):
     np.testing.assert_array_equal(oracle.assign_bbox(W, H, s[:, 0], s[:, 1], tris), want)
     y0, y1 = H // 3, H // 3 + 7
     np.testing.assert_array_equal(oracle.assign_bbox(W, H, s[:, 0], s[:, 1], tris, y0, y1), want[y0:y1])
+
+
+def test_bounding_box_assignment_covers_collinear_triangles_like_the_window():
+    """A collinear triangle passes the reference's closed test along its whole
+    supporting line, within the seed window (triangulation.cu:101-137); the
+    bounding-box form must give it the same pixels.  This incremental case
+    holds such a triangle (seeds (220, 38), (221, 39), (222, 40))."""
+    from integer_delauney_b200.workloads import uniform
+    W, H, P = 300, 200, 16
+    seeds = uniform(W, H, 2000, seed=2016)
+    o = oracle.incremental(W, H, [seeds[i:i + 500] for i in range(0, 2000, 500)], P)
+    order = np.lexsort((o["ys"], o["xs"]))
+    sx, sy = o["xs"][order], o["ys"][order]
+    t = o["tris"]
+    v = t[:, 2:5]
+    area = (sx[v[:, 1]] - sx[v[:, 0]]).astype(np.int64) * (sy[v[:, 2]] - sy[v[:, 0]]) - \
+        (sy[v[:, 1]] - sy[v[:, 0]]).astype(np.int64) * (sx[v[:, 2]] - sx[v[:, 0]])
+    assert (area == 0).any()
+    np.testing.assert_array_equal(oracle.assign_bbox(W, H, sx, sy, t), oracle.assign(W, H, sx, sy, t))
