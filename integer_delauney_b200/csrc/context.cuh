@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <memory>
+#include <mutex>
 #include <string>
 
 #include "common.cuh"
@@ -147,6 +148,9 @@ struct Context {
     int32_t stamp_epoch = 0;
     int dense_rounds = 1;  // propagation schedule from scratch (propagate.cu; idl_context_set_schedule)
     int key_tile = 0;      // tile shape of the owner-key tile round (propagate.cu; idl_context_set_tile)
+    // Owner-key tile rounds as one cooperative launch (propagate.cu); off for
+    // contexts whose work must overlap other streams' (a server's workers).
+    bool persistent_rounds = true;
 
     // topology
     DevBuf hkeys, hvals;  // hash table of triangle keys -> first witness
@@ -280,6 +284,11 @@ int64_t propagate_sparse_from_tiles(Context& C, const Canvas& cv, const uint32_t
 int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
                               int64_t n_new, const int32_t* big_list, int n_big, int big_tiles_x, int sub_x,
                               int sub_y, bool keys);
+
+// Held from launch to completion of a device-filling persistent kernel, one
+// per device: such grids run one at a time, so each one's co-residency does
+// not depend on other streams' grids (sparse_jacobi.cu).
+std::mutex& persistent_grid_lock(int device);
 
 // Run the persistent kernel's grid barrier alone (sparse_jacobi.cu) on one
 // block per SM, waiting for `missing_arrivals` more blocks than the grid has,

@@ -35,6 +35,7 @@
 // holds the same state in both planes, so reads of the frozen neighbours of an
 // active tile are always current, and at convergence the planes agree.
 #include "context.cuh"
+#include "gridsync.cuh"
 #include "stencil.cuh"
 
 #include <vector>
@@ -336,6 +337,148 @@ __device__ __forceinline__ void key_cell(int32_t& k, int32_t& d, int32_t a, int3
     d = fixed ? d : bd;
 }
 
+// The inner-cell mask of a thread (bit 2r + c: row r, column c of its cells).
+template <int NW, int KS>
+__device__ __forceinline__ uint32_t key_inner_mask(int cx0, int cy0)
+{
+    using T = KeyTile<NW, KS>;
+    uint32_t inner = 0;
+#pragma unroll
+    for (int r = 0; r < T::ROWS; ++r)
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+            if (cx0 + c >= KS && cx0 + c < KS + T::TW && cy0 + r >= KS && cy0 + r < KS + T::TH)
+                inner |= 1u << (2 * r + c);
+    return inner;
+}
+
+// Advance tile t by KS Jacobi steps (src -> dst, inner cells written) and, if
+// an inner cell changed, list the tile and its 8 neighbours for the next round.
+// L2: load the plane through L2 only (ld.global.cg), for a persistent kernel
+// whose other blocks rewrite the planes between rounds.
+template <int NW, int KS, bool L2>
+__device__ __forceinline__ void key_tile(KeyEdges<NW>& E, const int32_t* src, int32_t* dst, int pitch, int Wd, int Hd,
+                                         int t, int tiles_x, int tiles_y, int32_t* list_out, int32_t* count_out,
+                                         int32_t* stamp, int32_t stamp_next, long long step_base,
+                                         long long* last_change, uint32_t inner)
+{
+    using T = KeyTile<NW, KS>;
+    constexpr int ROWS = T::ROWS;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int cx0 = 2 * lane;
+    const int tx = t % tiles_x, ty = t / tiles_x;
+    const int gx = tx * T::TW - KS + cx0;
+    const int gyb = ty * T::TH - KS + warp * ROWS;
+
+    int32_t L[ROWS][2], D[ROWS][2];
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r) {
+        const int gy = gyb + r;
+        const bool row_in = gy >= 0 && gy < Hd;
+        int32_t l0 = OUTSIDE, l1 = OUTSIDE;
+        if (row_in) {
+            const int32_t* row = src + (size_t)gy * pitch;
+            if (gx >= 0 && gx + 1 < Wd) {
+                const int2 v = L2 ? __ldcg(reinterpret_cast<const int2*>(row + gx))
+                                  : *reinterpret_cast<const int2*>(row + gx);
+                l0 = v.x;
+                l1 = v.y;
+            } else {
+                if (gx >= 0 && gx < Wd) l0 = L2 ? __ldcg(row + gx) : row[gx];
+                if (gx + 1 >= 0 && gx + 1 < Wd) l1 = L2 ? __ldcg(row + gx + 1) : row[gx + 1];
+            }
+        }
+        L[r][0] = l0;
+        L[r][1] = l1;
+        D[r][0] = l0 >= 0 ? key_dist2(gx, gy, l0) : FAR;
+        D[r][1] = l1 >= 0 ? key_dist2(gx + 1, gy, l1) : FAR;
+    }
+    key_publish<NW>(E, 1, warp, lane, L, 0xFFFFFFFFu);
+    __syncthreads();
+
+    uint32_t chg = 0;
+    int last_step = -1;
+    int par = 1;
+#pragma unroll 1
+    for (int s = 0; s < KS; ++s) {
+        uint32_t new_chg = 0;
+        const int pp = par;
+        int32_t up0 = warp > 0 ? E.lab[pp][warp - 1][1][cx0] : OUTSIDE;
+        int32_t up1 = warp > 0 ? E.lab[pp][warp - 1][1][cx0 + 1] : OUTSIDE;
+        const int32_t dn0 = warp < NW - 1 ? E.lab[pp][warp + 1][0][cx0] : OUTSIDE;
+        const int32_t dn1 = warp < NW - 1 ? E.lab[pp][warp + 1][0][cx0 + 1] : OUTSIDE;
+        uint32_t dirty;
+        if (s == 0) {
+            dirty = 0xFFFFu;
+        } else {
+            dirty = chg | (chg << 2) | (chg >> 2) | ((chg & 0x5555u) << 1) | ((chg & 0xAAAAu) >> 1);
+            const uint32_t lc = __shfl_up_sync(FULL, chg, 1), rc = __shfl_down_sync(FULL, chg, 1);
+            if (lane > 0) dirty |= (lc & 0xAAAAu) >> 1;
+            if (lane < 31) dirty |= (rc & 0x5555u) << 1;
+            if (warp > 0) {
+                dirty |= (E.chg[pp][warp - 1][1][0] >> lane) & 1u;
+                dirty |= ((E.chg[pp][warp - 1][1][1] >> lane) & 1u) << 1;
+            }
+            if (warp < NW - 1) {
+                dirty |= ((E.chg[pp][warp + 1][0][0] >> lane) & 1u) << 14;
+                dirty |= ((E.chg[pp][warp + 1][0][1] >> lane) & 1u) << 15;
+            }
+            dirty &= 0xFFFFu;
+        }
+        if (__any_sync(FULL, dirty != 0)) {
+#pragma unroll
+            for (int r = 0; r < ROWS; ++r) {
+                const int32_t o0 = L[r][0], o1 = L[r][1];
+                int32_t left = __shfl_up_sync(FULL, o1, 1);
+                int32_t right = __shfl_down_sync(FULL, o0, 1);
+                if (lane == 0) left = OUTSIDE;
+                if (lane == 31) right = OUTSIDE;
+                const int32_t b0 = r + 1 < ROWS ? L[r + 1][0] : dn0;
+                const int32_t b1 = r + 1 < ROWS ? L[r + 1][1] : dn1;
+                const int gy = gyb + r;
+                key_cell(L[r][0], D[r][0], left, o1, up0, b0, gx, gy);
+                key_cell(L[r][1], D[r][1], o0, right, up1, b1, gx + 1, gy);
+                new_chg |= (uint32_t(L[r][0] != o0) << (2 * r)) | (uint32_t(L[r][1] != o1) << (2 * r + 1));
+                up0 = o0;
+                up1 = o1;
+            }
+        }
+        par ^= 1;
+        key_publish<NW>(E, par, warp, lane, L, new_chg);
+        chg = new_chg;
+        if (__syncthreads_or((new_chg & inner) != 0u)) last_step = s;
+    }
+
+    // inner cells only: a lane's two columns are both inner or both not
+#pragma unroll
+    for (int r = 0; r < ROWS; ++r) {
+        const int gy = gyb + r;
+        if (!((inner >> (2 * r)) & 1u) || gy >= Hd) continue;
+        int32_t* row = dst + (size_t)gy * pitch;
+        if (gx + 1 < Wd) {
+            *reinterpret_cast<int2*>(row + gx) = make_int2(L[r][0], L[r][1]);
+        } else if (gx < Wd) {
+            row[gx] = L[r][0];
+        }
+    }
+
+    if (last_step >= 0) {
+        if (threadIdx.x == 0) atomicMax(last_change, step_base + last_step);
+        if (threadIdx.x < 9) {
+            const int nx = tx + int(threadIdx.x % 3) - 1, ny = ty + int(threadIdx.x / 3) - 1;
+            if (nx >= 0 && nx < tiles_x && ny >= 0 && ny < tiles_y) {
+                const int nt = ny * tiles_x + nx;
+                if (atomicExch(&stamp[nt], stamp_next) != stamp_next) {
+                    const int slot = atomicAdd(count_out, 1);
+                    list_out[slot] = nt;
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// One tile round: every tile of list_in advanced KS steps.
 template <int NW, int KS>
 __global__ void __launch_bounds__(NW * 32, (NW <= 8 ? 3 : 2))
 k_round_keys(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pitch, int Wd, int Hd,
@@ -343,133 +486,42 @@ k_round_keys(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pit
              int32_t* __restrict__ list_out, int32_t* __restrict__ count_out, int32_t* __restrict__ stamp,
              int32_t stamp_next, int tiles_x, int tiles_y, long long step_base, long long* __restrict__ last_change)
 {
-    using T = KeyTile<NW, KS>;
-    constexpr int ROWS = T::ROWS;
     __shared__ KeyEdges<NW> E;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int cx0 = 2 * lane, cy0 = warp * ROWS;
-
-    uint32_t inner = 0;
-#pragma unroll
-    for (int r = 0; r < ROWS; ++r)
-#pragma unroll
-        for (int c = 0; c < 2; ++c)
-            if (cx0 + c >= KS && cx0 + c < KS + T::TW && cy0 + r >= KS && cy0 + r < KS + T::TH)
-                inner |= 1u << (2 * r + c);
-
+    const uint32_t inner = key_inner_mask<NW, KS>(2 * (threadIdx.x & 31), (threadIdx.x >> 5) * 8);
     const int n_items = *count_in;
-    for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-        const int t = list_in[item];
-        const int tx = t % tiles_x, ty = t / tiles_x;
-        const int gx = tx * T::TW - KS + cx0;
-        const int gyb = ty * T::TH - KS + cy0;
+    for (int item = blockIdx.x; item < n_items; item += gridDim.x)
+        key_tile<NW, KS, false>(E, src, dst, pitch, Wd, Hd, list_in[item], tiles_x, tiles_y, list_out, count_out,
+                                stamp, stamp_next, step_base, last_change, inner);
+}
 
-        int32_t L[ROWS][2], D[ROWS][2];
-#pragma unroll
-        for (int r = 0; r < ROWS; ++r) {
-            const int gy = gyb + r;
-            const bool row_in = gy >= 0 && gy < Hd;
-            int32_t l0 = OUTSIDE, l1 = OUTSIDE;
-            if (row_in) {
-                const int32_t* row = src + (size_t)gy * pitch;
-                if (gx >= 0 && gx + 1 < Wd) {
-                    const int2 v = *reinterpret_cast<const int2*>(row + gx);
-                    l0 = v.x;
-                    l1 = v.y;
-                } else {
-                    if (gx >= 0 && gx < Wd) l0 = row[gx];
-                    if (gx + 1 >= 0 && gx + 1 < Wd) l1 = row[gx + 1];
-                }
-            }
-            L[r][0] = l0;
-            L[r][1] = l1;
-            D[r][0] = l0 >= 0 ? key_dist2(gx, gy, l0) : FAR;
-            D[r][1] = l1 >= 0 ? key_dist2(gx + 1, gy, l1) : FAR;
-        }
-        key_publish<NW>(E, 1, warp, lane, L, 0xFFFFFFFFu);
-        __syncthreads();
-
-        uint32_t chg = 0;
-        int last_step = -1;
-        int par = 1;
-#pragma unroll 1
-        for (int s = 0; s < KS; ++s) {
-            uint32_t new_chg = 0;
-            const int pp = par;
-            int32_t up0 = warp > 0 ? E.lab[pp][warp - 1][1][cx0] : OUTSIDE;
-            int32_t up1 = warp > 0 ? E.lab[pp][warp - 1][1][cx0 + 1] : OUTSIDE;
-            const int32_t dn0 = warp < NW - 1 ? E.lab[pp][warp + 1][0][cx0] : OUTSIDE;
-            const int32_t dn1 = warp < NW - 1 ? E.lab[pp][warp + 1][0][cx0 + 1] : OUTSIDE;
-            uint32_t dirty;
-            if (s == 0) {
-                dirty = 0xFFFFu;
-            } else {
-                dirty = chg | (chg << 2) | (chg >> 2) | ((chg & 0x5555u) << 1) | ((chg & 0xAAAAu) >> 1);
-                const uint32_t lc = __shfl_up_sync(FULL, chg, 1), rc = __shfl_down_sync(FULL, chg, 1);
-                if (lane > 0) dirty |= (lc & 0xAAAAu) >> 1;
-                if (lane < 31) dirty |= (rc & 0x5555u) << 1;
-                if (warp > 0) {
-                    dirty |= (E.chg[pp][warp - 1][1][0] >> lane) & 1u;
-                    dirty |= ((E.chg[pp][warp - 1][1][1] >> lane) & 1u) << 1;
-                }
-                if (warp < NW - 1) {
-                    dirty |= ((E.chg[pp][warp + 1][0][0] >> lane) & 1u) << 14;
-                    dirty |= ((E.chg[pp][warp + 1][0][1] >> lane) & 1u) << 15;
-                }
-                dirty &= 0xFFFFu;
-            }
-            if (__any_sync(FULL, dirty != 0)) {
-#pragma unroll
-                for (int r = 0; r < ROWS; ++r) {
-                    const int32_t o0 = L[r][0], o1 = L[r][1];
-                    int32_t left = __shfl_up_sync(FULL, o1, 1);
-                    int32_t right = __shfl_down_sync(FULL, o0, 1);
-                    if (lane == 0) left = OUTSIDE;
-                    if (lane == 31) right = OUTSIDE;
-                    const int32_t b0 = r + 1 < ROWS ? L[r + 1][0] : dn0;
-                    const int32_t b1 = r + 1 < ROWS ? L[r + 1][1] : dn1;
-                    const int gy = gyb + r;
-                    key_cell(L[r][0], D[r][0], left, o1, up0, b0, gx, gy);
-                    key_cell(L[r][1], D[r][1], o0, right, up1, b1, gx + 1, gy);
-                    new_chg |= (uint32_t(L[r][0] != o0) << (2 * r)) | (uint32_t(L[r][1] != o1) << (2 * r + 1));
-                    up0 = o0;
-                    up1 = o1;
-                }
-            }
-            par ^= 1;
-            key_publish<NW>(E, par, warp, lane, L, new_chg);
-            chg = new_chg;
-            if (__syncthreads_or((new_chg & inner) != 0u)) last_step = s;
-        }
-
-        // inner cells only: a lane's two columns are both inner or both not
-#pragma unroll
-        for (int r = 0; r < ROWS; ++r) {
-            const int gy = gyb + r;
-            if (!((inner >> (2 * r)) & 1u) || gy >= Hd) continue;
-            int32_t* row = dst + (size_t)gy * pitch;
-            if (gx + 1 < Wd) {
-                *reinterpret_cast<int2*>(row + gx) = make_int2(L[r][0], L[r][1]);
-            } else if (gx < Wd) {
-                row[gx] = L[r][0];
-            }
-        }
-
-        if (last_step >= 0) {
-            if (threadIdx.x == 0) atomicMax(last_change, step_base + last_step);
-            if (threadIdx.x < 9) {
-                const int nx = tx + int(threadIdx.x % 3) - 1, ny = ty + int(threadIdx.x / 3) - 1;
-                if (nx >= 0 && nx < tiles_x && ny >= 0 && ny < tiles_y) {
-                    const int nt = ny * tiles_x + nx;
-                    if (atomicExch(&stamp[nt], stamp_next) != stamp_next) {
-                        const int slot = atomicAdd(count_out, 1);
-                        list_out[slot] = nt;
-                    }
-                }
-            }
-        }
-        __syncthreads();
+// Up to max_rounds tile rounds in one cooperative launch, separated by the
+// bounded grid barrier: round r runs list r%2 from plane r%2 into plane
+// (r+1)%2 and builds list (r+1)%2, exactly as successive k_round_keys
+// launches would.  Stops when a round's list is empty; gs->passes receives
+// the rounds run.
+template <int NW, int KS>
+__global__ void __launch_bounds__(NW * 32, (NW <= 8 ? 3 : 2))
+k_rounds_keys(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, int32_t* list0, int32_t* list1,
+              int32_t* counts, int32_t* stamp, int32_t epoch, int tiles_x, int tiles_y, int max_rounds,
+              long long* last_change, GridSync* gs)
+{
+    __shared__ KeyEdges<NW> E;
+    const uint32_t inner = key_inner_mask<NW, KS>(2 * (threadIdx.x & 31), (threadIdx.x >> 5) * 8);
+    unsigned gen_local = 0;
+    int r = 0;
+    for (; r < max_rounds; ++r) {
+        const int n = __ldcg(&counts[r]);
+        if (n == 0) break;
+        const int32_t* src = (r & 1) ? plane1 : plane0;
+        int32_t* dst = (r & 1) ? plane0 : plane1;
+        const int32_t* lin = (r & 1) ? list1 : list0;
+        int32_t* lout = (r & 1) ? list0 : list1;
+        for (int item = blockIdx.x; item < n; item += gridDim.x)
+            key_tile<NW, KS, true>(E, src, dst, pitch, Wd, Hd, __ldcg(&lin[item]), tiles_x, tiles_y, lout,
+                                   counts + r + 1, stamp, epoch + r + 1, (long long)r * KS, last_change, inner);
+        if (!grid_sync(gs, gridDim.x, gen_local)) return;
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) gs->passes = r;
 }
 
 // Seed cells of both planes take their seeds' keys (the rest of the planes
@@ -616,6 +668,40 @@ void launch_round_keys(Context& C, int per_sm, const int32_t* src, int32_t* dst,
 int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
                          int64_t n_new, bool keys);
 
+// Up to `rounds_cap` owner-key tile rounds in one cooperative launch (the
+// first work list already in C.tiles[0] and counts[0]); returns the rounds run.
+template <int NW, int KS>
+int64_t run_rounds_keys(Context& C, const Canvas& cv, int32_t* counts, int32_t epoch, int tiles_x, int tiles_y,
+                        int64_t rounds_cap, long long* last)
+{
+    int per_sm = 0;
+    IDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rounds_keys<NW, KS>, NW * 32, 0));
+    if (per_sm < 1) throw Error(IDL_ERR_INTERNAL, "tile round kernel cannot be resident");
+    const int grid = std::max(1, std::min(tiles_x * tiles_y, per_sm * C.num_sms));
+    C.gsync.ensure(sizeof(GridSync));
+    IDL_CUDA(cudaMemsetAsync(C.gsync.ptr, 0, sizeof(GridSync), C.stream));
+    int32_t* p0 = C.lab[0].as<int32_t>();
+    int32_t* p1 = C.lab[1].as<int32_t>();
+    int32_t* l0 = C.tiles[0].as<int32_t>();
+    int32_t* l1 = C.tiles[1].as<int32_t>();
+    int32_t* stamp = C.stamps.as<int32_t>();
+    GridSync* gs = C.gsync.as<GridSync>();
+    int pitch = cv.pitch, Wd = cv.Wd, Hd = cv.Hd, tx = tiles_x, ty = tiles_y;
+    int cap = (int)std::min<int64_t>(rounds_cap, 1 << 30);
+    void* args[] = {&p0, &p1, &pitch, &Wd, &Hd, &l0, &l1, &counts, &stamp, &epoch, &tx, &ty, &cap, &last, &gs};
+    GridSync h{};
+    {
+        std::lock_guard<std::mutex> lock(persistent_grid_lock(C.device));
+        IDL_CUDA(cudaLaunchCooperativeKernel((const void*)k_rounds_keys<NW, KS>, dim3(grid), dim3(NW * 32), args, 0,
+                                             C.stream));
+        count_launch();
+        IDL_CUDA(cudaMemcpyAsync(&h, gs, sizeof(GridSync), cudaMemcpyDeviceToHost, C.stream));
+        IDL_CUDA(cudaStreamSynchronize(C.stream));
+    }
+    if (h.error) throw Error(IDL_ERR_INTERNAL, "Voronoi propagation: grid barrier timed out");
+    return h.passes;
+}
+
 }  // namespace
 
 int key_tile_shapes() { return N_KEY_SHAPES; }
@@ -701,7 +787,19 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
     int64_t r = 0;
     int group = 2;
     int32_t remaining = 0;
-    for (;;) {
+    if (keys && C.persistent_rounds) {
+        // every round in one cooperative launch, rounds separated by the grid barrier
+        const int64_t cap = round_limit >= 0 ? round_limit : max_rounds;
+        switch (C.key_tile) {
+        case 1: r = run_rounds_keys<16, 8>(C, cv, counts, epoch, tiles_x, tiles_y, cap, last); break;
+        case 2: r = run_rounds_keys<8, 4>(C, cv, counts, epoch, tiles_x, tiles_y, cap, last); break;
+        case 3: r = run_rounds_keys<16, 12>(C, cv, counts, epoch, tiles_x, tiles_y, cap, last); break;
+        default: r = run_rounds_keys<8, 8>(C, cv, counts, epoch, tiles_x, tiles_y, cap, last);
+        }
+        IDL_CUDA(cudaMemcpy(&remaining, counts + r, 4, cudaMemcpyDeviceToHost));
+        if (round_limit < 0 && remaining != 0) throw Error(IDL_ERR_INTERNAL, "Voronoi propagation did not converge");
+    }
+    for (; !(keys && C.persistent_rounds);) {
         for (int g = 0; g < group && r < max_rounds && (round_limit < 0 || r < round_limit); ++g, ++r) {
             const int32_t* srcp = C.lab[r & 1].as<int32_t>();
             int32_t* dstp = C.lab[(r + 1) & 1].as<int32_t>();

@@ -419,6 +419,9 @@ int idl_server_create(int device, int64_t budget_bytes, int slots, int border_pa
             check_status(idl_context_create(dev, &sl.batch));
             check_status(idl_context_set_stream(sl.ws, sl.stream));
             check_status(idl_context_set_stream(sl.batch, sl.stream));
+            // workers overlap: tile rounds as plain launches, not a device-filling grid
+            sl.ws->persistent_rounds = false;
+            sl.batch->persistent_rounds = false;
             // inserts as tile rounds: plain launches that overlap the other
             // workers' work, where the persistent kernel would hold the whole
             // device (measured: twice the insert throughput with 8 workers)

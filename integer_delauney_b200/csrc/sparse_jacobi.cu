@@ -27,6 +27,7 @@
 // passes, so they are read with ld.global.cg (L2), never through L1 or the
 // read-only path; barrier arrival and departure are release/acquire.
 #include "context.cuh"
+#include "gridsync.cuh"
 #include "stencil.cuh"
 
 #include <cuda/atomic>
@@ -40,50 +41,7 @@ constexpr int MT = 8;                       // micro-tile side
 constexpr int SJ_THREADS = 1024;
 constexpr int SJ_WARPS = SJ_THREADS / 32;
 constexpr int GROUP = 2;                    // micro-tiles a warp advances together
-constexpr unsigned SPIN_LIMIT = 1u << 24;   // barrier polls before giving up
 constexpr int STAGE = 6144;                 // per-block staging of next-pass list entries
-
-struct GridSync {
-    unsigned count;
-    unsigned gen;
-    int error;
-    int passes;   // passes run (the last one changed nothing)
-};
-
-// Grid-wide barrier with a bounded wait: at most `spin_limit` polls per
-// block.  On timeout the error flag is raised and every block leaves the
-// kernel, so a bug cannot hang the GPU.
-__device__ __forceinline__ bool grid_sync(GridSync* gs, unsigned nblocks, unsigned& gen_local,
-                                          unsigned spin_limit = SPIN_LIMIT)
-{
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(gs->count), gen(gs->gen);
-        cuda::atomic_ref<int, cuda::thread_scope_device> err(gs->error);
-        const unsigned target = gen_local + 1;
-        int ok = 1;
-        if (cnt.fetch_add(1u, cuda::memory_order_acq_rel) == nblocks - 1) {
-            cnt.store(0u, cuda::memory_order_relaxed);
-            gen.store(target, cuda::memory_order_release);
-        } else {
-            unsigned spins = 0;
-            while (gen.load(cuda::memory_order_acquire) != target) {
-                if (++spins > spin_limit) {
-                    err.fetch_or(1, cuda::memory_order_relaxed);
-                    ok = 0;
-                    break;
-                }
-                if (spins > 32) __nanosleep(20);
-            }
-        }
-        if (err.load(cuda::memory_order_relaxed)) ok = 0;
-        s_ok = ok;
-    }
-    __syncthreads();
-    ++gen_local;
-    return s_ok != 0;
-}
 
 // The Jacobi update of one cell owned by `b` from its four neighbours' owners
 // (geometry_device.cuh:40-66).  The owner's and the candidates' distances are
@@ -374,6 +332,12 @@ __global__ void k_expand_tiles(const int32_t* __restrict__ big, int big_tiles_x,
 
 }  // namespace
 
+std::mutex& persistent_grid_lock(int device)
+{
+    static std::mutex locks[64];
+    return locks[device & 63];
+}
+
 void grid_barrier_selftest(Context& C, int missing_arrivals, unsigned spin_limit)
 {
     if (missing_arrivals < 0 || missing_arrivals > 1024) invalid("missing_arrivals must be in [0, 1024]");
@@ -466,8 +430,7 @@ int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos,
         // so two contexts' launches on different streams could not run side by
         // side anyway, and holding the device lock from launch to completion
         // keeps each grid's co-residency independent of the other streams.
-        static std::mutex device_locks[64];
-        std::lock_guard<std::mutex> lock(device_locks[C.device & 63]);
+        std::lock_guard<std::mutex> lock(persistent_grid_lock(C.device));
         IDL_CUDA(cudaLaunchCooperativeKernel(kernel, dim3(grid), dim3(SJ_THREADS), args, 0, C.stream));
         count_launch();
         IDL_CUDA(cudaMemcpyAsync(&h, gs, sizeof(GridSync), cudaMemcpyDeviceToHost, C.stream));
