@@ -435,10 +435,17 @@ __device__ __forceinline__ void key_tile(KeyEdges<NW>& E, const int32_t* src, in
                 if (lane == 31) right = OUTSIDE;
                 const int32_t b0 = r + 1 < ROWS ? L[r + 1][0] : dn0;
                 const int32_t b1 = r + 1 < ROWS ? L[r + 1][1] : dn1;
-                const int gy = gyb + r;
-                key_cell(L[r][0], D[r][0], left, o1, up0, b0, gx, gy);
-                key_cell(L[r][1], D[r][1], o0, right, up1, b1, gx + 1, gy);
-                new_chg |= (uint32_t(L[r][0] != o0) << (2 * r)) | (uint32_t(L[r][1] != o1) << (2 * r + 1));
+                // a cell can change only if its neighbourhood changed in the
+                // last step (dirty) and a neighbour has another owner; the warp
+                // skips a row none of whose cells can
+                const bool need0 = ((dirty >> (2 * r)) & 1u) && (left != o0 || o1 != o0 || up0 != o0 || b0 != o0);
+                const bool need1 = ((dirty >> (2 * r + 1)) & 1u) && (o0 != o1 || right != o1 || up1 != o1 || b1 != o1);
+                if (__any_sync(FULL, need0 || need1)) {
+                    const int gy = gyb + r;
+                    key_cell(L[r][0], D[r][0], left, o1, up0, b0, gx, gy);
+                    key_cell(L[r][1], D[r][1], o0, right, up1, b1, gx + 1, gy);
+                    new_chg |= (uint32_t(L[r][0] != o0) << (2 * r)) | (uint32_t(L[r][1] != o1) << (2 * r + 1));
+                }
                 up0 = o0;
                 up1 = o1;
             }

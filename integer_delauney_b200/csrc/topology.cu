@@ -169,13 +169,13 @@ __device__ __forceinline__ void hash_insert(unsigned long long key, unsigned lon
 }
 
 // One thread per column and strip of DETECT_STRIP block rows, a warp per 32
-// adjacent columns: each label row is loaded once (the block's right column
-// comes from the next lane) and becomes the next block's top row.  A key is
-// not inserted again when the same column's block one row up, or the block
-// one column left (the previous lane), emitted it: that block's row-major
-// index is smaller, so the atomicMin it did already keeps a smaller witness
-// than this one would.
-constexpr int DETECT_STRIP = 16;
+// adjacent columns: the strip's DETECT_STRIP + 1 label rows are loaded once,
+// all at the start (independent loads in flight together), and each block's
+// right column comes from the next lane.  A key is not inserted again when the
+// same column's block one row up, or the block one column left (the previous
+// lane), emitted it: that block's row-major index is smaller, so the
+// atomicMin it did already keeps a smaller witness than this one would.
+constexpr int DETECT_STRIP = 8;
 
 __global__ void __launch_bounds__(256)
 k_detect(const int32_t* __restrict__ lab, int pitch, int Wd, int Hd, const uint32_t* __restrict__ pos,
@@ -186,21 +186,27 @@ k_detect(const int32_t* __restrict__ lab, int pitch, int Wd, int Hd, const uint3
     const int x = blockIdx.x * 32 + lane;
     const int y0 = (blockIdx.y * blockDim.y + threadIdx.y) * DETECT_STRIP;
     if (y0 >= Hd - 1) return;   // uniform over the warp
-    const int y1 = min(y0 + DETECT_STRIP, Hd - 1);
+    const int rows = min(DETECT_STRIP, Hd - 1 - y0);   // blocks in this strip
     const bool has_block = x < Wd - 1;
-    auto load_row = [&](int y, int32_t& l, int32_t& r) {
-        const int32_t* row = lab + (size_t)y * pitch;
-        l = x < Wd ? row[x] : -2;
-        r = __shfl_down_sync(0xffffffffu, l, 1);
-        if (lane == 31) r = x + 1 < Wd ? row[x + 1] : -2;
-    };
-    int32_t a, b;
-    load_row(y0, a, b);
+    int32_t L[DETECT_STRIP + 1], R[DETECT_STRIP + 1];
+#pragma unroll
+    for (int i = 0; i <= DETECT_STRIP; ++i) {
+        L[i] = -2;
+        if (i <= rows && x < Wd) L[i] = lab[(size_t)(y0 + i) * pitch + x];
+    }
+    const int32_t* last_col = lab + x + 1;
+    const bool edge = lane == 31 && x + 1 < Wd;
+#pragma unroll
+    for (int i = 0; i <= DETECT_STRIP; ++i) {
+        R[i] = __shfl_down_sync(0xffffffffu, L[i], 1);
+        if (lane == 31) R[i] = (edge && i <= rows) ? last_col[(size_t)(y0 + i) * pitch] : -2;
+    }
     const unsigned long long none = EMPTY_KEY;
     unsigned long long up0 = none, up1 = none;   // keys this column's block emitted one row up
-    for (int y = y0; y < y1; ++y) {
-        int32_t c, d;
-        load_row(y + 1, c, d);
+#pragma unroll
+    for (int i = 0; i < DETECT_STRIP; ++i) {
+        if (i >= rows) break;   // uniform over the warp
+        const int32_t a = L[i], b = R[i], c = L[i + 1], d = R[i + 1];
         unsigned long long k0 = none, k1 = none;
         unsigned code0 = 0, code1 = 0;
         if (has_block && !(a == b && a == c && a == d) && !((a == b && c == d) || (a == c && b == d))) {
@@ -210,7 +216,7 @@ k_detect(const int32_t* __restrict__ lab, int pitch, int Wd, int Hd, const uint3
             if (e.n > 1) make_key(e.o[1], rank, k1, code1);
         }
         const unsigned long long l0 = __shfl_up_sync(0xffffffffu, k0, 1), l1 = __shfl_up_sync(0xffffffffu, k1, 1);
-        const unsigned long long blk = (unsigned long long)y * Wd + x;
+        const unsigned long long blk = (unsigned long long)(y0 + i) * Wd + x;
         auto seen = [&](unsigned long long k) {
             return k == up0 || k == up1 || (lane > 0 && (k == l0 || k == l1));
         };
@@ -218,8 +224,6 @@ k_detect(const int32_t* __restrict__ lab, int pitch, int Wd, int Hd, const uint3
         if (k1 != none && !seen(k1)) hash_insert(k1, (blk << 4) | code1, keys, vals, mask, sc);
         up0 = k0;
         up1 = k1;
-        a = c;
-        b = d;
     }
 }
 
