@@ -44,17 +44,20 @@ __global__ void k_max_side(const int32_t* __restrict__ tris, const Scalars* __re
     if ((threadIdx.x & 31) == 0 && best > 0) atomicMax(&sc->max_side, best);
 }
 
-// One warp per triangle; lanes take rows.
+// A group of RASTER_GROUP lanes per triangle (four triangles per warp: a
+// Delaunay triangle of a dense seed set spans a few rows); lanes take rows.
+constexpr int RASTER_GROUP = 8;
+
 __global__ void __launch_bounds__(256)
 k_raster(const int32_t* __restrict__ tris, const Scalars* __restrict__ sc, const int32_t* __restrict__ xs,
          const int32_t* __restrict__ ys, int W, int H, int32_t* __restrict__ tgrid)
 {
     const long long nt = sc->n_triangles;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x % RASTER_GROUP;
     const int wc = max(20, sc->max_side + 3);
-    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nt; t += warps)
-        raster_one(tris + t * 5 + 2, (int32_t)t, xs, ys, W, H, wc, tgrid, lane);
+    const long long groups = (long long)gridDim.x * (blockDim.x / RASTER_GROUP);
+    for (long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / RASTER_GROUP; t < nt; t += groups)
+        raster_one<RASTER_GROUP>(tris + t * 5 + 2, (int32_t)t, xs, ys, W, H, wc, tgrid, lane);
 }
 
 }  // namespace
@@ -67,7 +70,8 @@ void assign_pixels(Context& C, int W, int H, const int32_t* xs, const int32_t* y
     const int g = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(max_tri, 256), C.num_sms * 8));
     k_max_side<<<g, 256, 0, C.stream>>>(C.tris.as<int32_t>(), C.sc(), xs, ys, C.sc());
     IDL_LAUNCH();
-    const int gr = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(max_tri, 8), C.num_sms * 16));
+    const int gr = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(max_tri, 256 / RASTER_GROUP),
+                                                                C.num_sms * 16));
     k_raster<<<gr, 256, 0, C.stream>>>(C.tris.as<int32_t>(), C.sc(), xs, ys, W, H, tgrid);
     IDL_LAUNCH();
 }

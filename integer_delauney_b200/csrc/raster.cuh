@@ -31,8 +31,10 @@ __device__ __forceinline__ int tri_max_side(const int32_t* v, const int32_t* __r
 }
 
 // Rasterise one triangle (vertex ids v, coordinates xs/ys) into a W x H grid
-// of triangle ids with atomicMax; the calling warp's 32 lanes share the rows.
-// wc: the degenerate-case seed window (max(20, max_side + 3)).
+// of triangle ids with atomicMax; a group of G lanes shares the rows (`lane`
+// is the caller's index in its group).  wc: the degenerate-case seed window
+// (max(20, max_side + 3)).
+template <int G = 32>
 __device__ __forceinline__ void raster_one(const int32_t* v, int32_t tid, const int32_t* __restrict__ xs,
                                            const int32_t* __restrict__ ys, int W, int H, int wc,
                                            int32_t* __restrict__ tgrid, int lane)
@@ -72,7 +74,7 @@ __device__ __forceinline__ void raster_one(const int32_t* v, int32_t tid, const 
     const long long C0[3] = {sgn * (ax * by - ay * bx), sgn * (bx * cy - by * cx), sgn * (cx * ay - cy * ax)};
     const long long y0 = max(0ll, min(ay, min(by, cy)));
     const long long y1 = min((long long)H - 1, max(ay, max(by, cy)));
-    for (long long y = y0 + lane; y <= y1; y += 32) {
+    for (long long y = y0 + lane; y <= y1; y += G) {
         long long xl = 0, xr = W - 1;
         bool empty = false;
 #pragma unroll
