@@ -125,7 +125,9 @@ IDL_API int idl_context_set_schedule(idl_context* ctx, int dense_rounds);
 /* Tile shape of a from-scratch propagation's tile rounds (reference
  * semantics), as an index: 0 = 48 x 48 cells advanced 8 passes per round
  * (default), 1 = 48 x 112 / 8 passes, 2 = 56 x 56 / 4 passes,
- * 3 = 40 x 104 / 12 passes.  Results do not depend on it, only the time does.
+ * 3 = 40 x 104 / 12 passes, one launch per round; 4..7 = the same shapes with
+ * all rounds in one cooperative launch separated by a bounded grid barrier.
+ * Results do not depend on it, only the time does.
  * *n_shapes_out (may be NULL) receives the number of shapes; an index outside
  * [0, n) is IDL_ERR_INVALID.  No counterpart in the reference (fixed 16 x 16
  * blocks, one pass per launch, src/cuda/voronoi.cu:97-98). */

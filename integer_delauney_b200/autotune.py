@@ -10,8 +10,9 @@ its speed, never its result:
   convergence);
 * the tile shape (idl_context_set_tile): the inner tile of a round and the
   passes it advances per round trip (48 x 48 / 8, 48 x 112 / 8, 56 x 56 / 4,
-  40 x 104 / 12).  Larger tiles waste less work on halos, more passes per round
-  trip suit thin fronts crossing empty space, fewer suit dense seed sets.
+  40 x 104 / 12), with the rounds as separate launches or all in one
+  cooperative launch.  Larger tiles waste less work on halos, more passes per
+  round trip suit thin fronts crossing empty space, fewer suit dense seed sets.
 
 Where each pays depends on the seed density and layout: dense, uniform seed
 sets change most of the canvas for the first few passes, clustered ones leave

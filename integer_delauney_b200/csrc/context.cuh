@@ -148,12 +148,13 @@ struct Context {
     int32_t stamp_epoch = 0;
     int dense_rounds = 1;  // propagation schedule from scratch (propagate.cu; idl_context_set_schedule)
     int key_tile = 0;      // tile shape of the owner-key tile round (propagate.cu; idl_context_set_tile)
-    // Owner-key tile rounds as one cooperative launch (propagate.cu); off for
+    // Whether the persistent tile shapes (key_tile >= 4) may run their rounds
+    // as one device-filling cooperative launch (propagate.cu); off for
     // contexts whose work must overlap other streams' (a server's workers).
     bool persistent_rounds = true;
 
     // topology
-    DevBuf hkeys, hvals;  // hash table of triangle keys -> first witness
+    DevBuf hkeys;         // hash table of triangle keys -> first witness (key, value interleaved)
     DevBuf ukeys, uvals;  // compacted unique keys
     DevBuf cnt, off, fill, grp;  // group-by-smallest-vertex ranking
     DevBuf tris;          // n_tri x 5 int32 (x, y, a, b, c)
@@ -200,7 +201,7 @@ struct Context {
     {
         DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
                          &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &big_tiles, &exact_dy, &hkeys,
-                         &hvals, &ukeys, &uvals, &cnt, &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded,
+                         &ukeys, &uvals, &cnt, &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded,
                          &batch_img, &batch_seed_img, &batch_rows, &batch_sid, &batch_stats, &batch_bad,
                          &batch_ximg, &batch_colimg, &batch_rowimg, &scalars};
         for (DevBuf* b : all) f(*b);

@@ -711,7 +711,9 @@ int64_t run_rounds_keys(Context& C, const Canvas& cv, int32_t* counts, int32_t e
 
 }  // namespace
 
-int key_tile_shapes() { return N_KEY_SHAPES; }
+// Indices N_KEY_SHAPES .. 2 N_KEY_SHAPES - 1 are the same shapes with the
+// rounds run as one cooperative launch (run_rounds_keys).
+int key_tile_shapes() { return 2 * N_KEY_SHAPES; }
 
 int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, int64_t n_seeds,
                   const uint32_t* seed_pos, int64_t n_new)
@@ -760,7 +762,10 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
         return propagate_sparse(C, cv, pos, seed_pos, n_new, keys);
     if (seed_pos && n_new == 0) return 0;
     const int64_t round_limit = hybrid && C.dense_rounds > 0 ? C.dense_rounds : -1;
-    const KeyShape shape = KEY_SHAPES[std::min(std::max(C.key_tile, 0), N_KEY_SHAPES - 1)];
+    const int tile = std::min(std::max(C.key_tile, 0), 2 * N_KEY_SHAPES - 1);
+    const int base_shape = tile % N_KEY_SHAPES;
+    const bool persistent = keys && C.persistent_rounds && tile >= N_KEY_SHAPES;
+    const KeyShape shape = KEY_SHAPES[base_shape];
     const int tw = keys ? shape.tw : TW, th = keys ? shape.th : TH, steps = keys ? shape.ks : KSTEPS;
     const int tiles_x = ceil_div(cv.Wd, tw), tiles_y = ceil_div(cv.Hd, th);
     const int n_tiles = tiles_x * tiles_y;
@@ -794,10 +799,10 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
     int64_t r = 0;
     int group = 2;
     int32_t remaining = 0;
-    if (keys && C.persistent_rounds) {
+    if (persistent) {
         // every round in one cooperative launch, rounds separated by the grid barrier
         const int64_t cap = round_limit >= 0 ? round_limit : max_rounds;
-        switch (C.key_tile) {
+        switch (base_shape) {
         case 1: r = run_rounds_keys<16, 8>(C, cv, counts, epoch, tiles_x, tiles_y, cap, last); break;
         case 2: r = run_rounds_keys<8, 4>(C, cv, counts, epoch, tiles_x, tiles_y, cap, last); break;
         case 3: r = run_rounds_keys<16, 12>(C, cv, counts, epoch, tiles_x, tiles_y, cap, last); break;
@@ -806,7 +811,7 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
         IDL_CUDA(cudaMemcpy(&remaining, counts + r, 4, cudaMemcpyDeviceToHost));
         if (round_limit < 0 && remaining != 0) throw Error(IDL_ERR_INTERNAL, "Voronoi propagation did not converge");
     }
-    for (; !(keys && C.persistent_rounds);) {
+    for (; !persistent;) {
         for (int g = 0; g < group && r < max_rounds && (round_limit < 0 || r < round_limit); ++g, ++r) {
             const int32_t* srcp = C.lab[r & 1].as<int32_t>();
             int32_t* dstp = C.lab[(r + 1) & 1].as<int32_t>();
@@ -816,7 +821,7 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
             const int32_t stamp_next = epoch + int32_t(r) + 1;
             int32_t* stamp = C.stamps.as<int32_t>();
             if (keys) {
-                switch (C.key_tile) {
+                switch (base_shape) {
                 case 1:
                     launch_round_keys<16, 8>(C, 2, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
                                              stamp_next, tiles_x, tiles_y, base, last);

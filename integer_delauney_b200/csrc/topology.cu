@@ -151,16 +151,17 @@ __device__ __forceinline__ void make_key(const int32_t in[3], const int32_t* __r
     code = i0 * 3u + i1;
 }
 
+// The table interleaves each slot's key and value (table[2s], table[2s + 1]),
+// so an insert touches one 16-byte pair in one memory sector.
 __device__ __forceinline__ void hash_insert(unsigned long long key, unsigned long long val,
-                                            unsigned long long* __restrict__ keys,
-                                            unsigned long long* __restrict__ vals, unsigned long long mask,
+                                            unsigned long long* __restrict__ table, unsigned long long mask,
                                             Scalars* __restrict__ sc)
 {
     unsigned long long slot = mix64(key) & mask;
     for (int probe = 0; probe < MAX_PROBES; ++probe) {
-        const unsigned long long prev = atomicCAS(&keys[slot], EMPTY_KEY, key);
+        const unsigned long long prev = atomicCAS(&table[2 * slot], EMPTY_KEY, key);
         if (prev == EMPTY_KEY || prev == key) {
-            atomicMin(&vals[slot], val);
+            atomicMin(&table[2 * slot + 1], val);
             return;
         }
         slot = (slot + 1) & mask;
@@ -168,63 +169,35 @@ __device__ __forceinline__ void hash_insert(unsigned long long key, unsigned lon
     atomicOr(&sc->overflow, 1);
 }
 
-// One thread per column and strip of DETECT_STRIP block rows, a warp per 32
-// adjacent columns: the strip's DETECT_STRIP + 1 label rows are loaded once,
-// all at the start (independent loads in flight together), and each block's
-// right column comes from the next lane.  A key is not inserted again when the
-// same column's block one row up, or the block one column left (the previous
-// lane), emitted it: that block's row-major index is smaller, so the
-// atomicMin it did already keeps a smaller witness than this one would.
-constexpr int DETECT_STRIP = 8;
-
+// One thread per 2 x 2 block; a warp covers 32 adjacent blocks of a row.  A
+// key the block one column left (the previous lane) emitted as well is not
+// inserted again: that block's row-major index is smaller, so its atomicMin
+// already keeps a smaller witness than this one would.
 __global__ void __launch_bounds__(256)
 k_detect(const int32_t* __restrict__ lab, int pitch, int Wd, int Hd, const uint32_t* __restrict__ pos,
-         const int32_t* __restrict__ rank, unsigned long long* __restrict__ keys,
-         unsigned long long* __restrict__ vals, unsigned long long mask, Scalars* __restrict__ sc)
+         const int32_t* __restrict__ rank, unsigned long long* __restrict__ table, unsigned long long mask,
+         Scalars* __restrict__ sc)
 {
-    const int lane = threadIdx.x;
-    const int x = blockIdx.x * 32 + lane;
-    const int y0 = (blockIdx.y * blockDim.y + threadIdx.y) * DETECT_STRIP;
-    if (y0 >= Hd - 1) return;   // uniform over the warp
-    const int rows = min(DETECT_STRIP, Hd - 1 - y0);   // blocks in this strip
-    const bool has_block = x < Wd - 1;
-    int32_t L[DETECT_STRIP + 1], R[DETECT_STRIP + 1];
-#pragma unroll
-    for (int i = 0; i <= DETECT_STRIP; ++i) {
-        L[i] = -2;
-        if (i <= rows && x < Wd) L[i] = lab[(size_t)(y0 + i) * pitch + x];
-    }
-    const int32_t* last_col = lab + x + 1;
-    const bool edge = lane == 31 && x + 1 < Wd;
-#pragma unroll
-    for (int i = 0; i <= DETECT_STRIP; ++i) {
-        R[i] = __shfl_down_sync(0xffffffffu, L[i], 1);
-        if (lane == 31) R[i] = (edge && i <= rows) ? last_col[(size_t)(y0 + i) * pitch] : -2;
-    }
-    const unsigned long long none = EMPTY_KEY;
-    unsigned long long up0 = none, up1 = none;   // keys this column's block emitted one row up
-#pragma unroll
-    for (int i = 0; i < DETECT_STRIP; ++i) {
-        if (i >= rows) break;   // uniform over the warp
-        const int32_t a = L[i], b = R[i], c = L[i + 1], d = R[i + 1];
-        unsigned long long k0 = none, k1 = none;
-        unsigned code0 = 0, code1 = 0;
-        if (has_block && !(a == b && a == c && a == d) && !((a == b && c == d) || (a == c && b == d))) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (y >= Hd - 1) return;   // uniform over the warp (blockDim.x = 32)
+    unsigned long long k0 = EMPTY_KEY, k1 = EMPTY_KEY;
+    unsigned code0 = 0, code1 = 0;
+    if (x < Wd - 1) {
+        const int32_t a = lab[(size_t)y * pitch + x], b = lab[(size_t)y * pitch + x + 1];
+        const int32_t c = lab[(size_t)(y + 1) * pitch + x], d = lab[(size_t)(y + 1) * pitch + x + 1];
+        if (!(a == b && a == c && a == d) && !((a == b && c == d) || (a == c && b == d))) {
             Emit e;
             block_rule(a, b, c, d, pos, e);
             if (e.n > 0) make_key(e.o[0], rank, k0, code0);
             if (e.n > 1) make_key(e.o[1], rank, k1, code1);
         }
-        const unsigned long long l0 = __shfl_up_sync(0xffffffffu, k0, 1), l1 = __shfl_up_sync(0xffffffffu, k1, 1);
-        const unsigned long long blk = (unsigned long long)(y0 + i) * Wd + x;
-        auto seen = [&](unsigned long long k) {
-            return k == up0 || k == up1 || (lane > 0 && (k == l0 || k == l1));
-        };
-        if (k0 != none && !seen(k0)) hash_insert(k0, (blk << 4) | code0, keys, vals, mask, sc);
-        if (k1 != none && !seen(k1)) hash_insert(k1, (blk << 4) | code1, keys, vals, mask, sc);
-        up0 = k0;
-        up1 = k1;
     }
+    const unsigned long long l0 = __shfl_up_sync(0xffffffffu, k0, 1), l1 = __shfl_up_sync(0xffffffffu, k1, 1);
+    const bool first = threadIdx.x == 0;
+    const unsigned long long blk = (unsigned long long)y * Wd + x;
+    if (k0 != EMPTY_KEY && (first || (k0 != l0 && k0 != l1))) hash_insert(k0, (blk << 4) | code0, table, mask, sc);
+    if (k1 != EMPTY_KEY && (first || (k1 != l0 && k1 != l1))) hash_insert(k1, (blk << 4) | code1, table, mask, sc);
 }
 
 // Warp-aggregated append: one atomic per warp.
@@ -240,19 +213,18 @@ __device__ __forceinline__ long long warp_append(bool pred, unsigned long long* 
     return pred ? (long long)(base + __popc(ballot & ((1u << lane) - 1u))) : -1;
 }
 
-__global__ void k_enumerate(const unsigned long long* __restrict__ keys, const unsigned long long* __restrict__ vals,
-                            long long cap, unsigned long long* __restrict__ ukeys,
+__global__ void k_enumerate(const unsigned long long* __restrict__ table, long long cap, unsigned long long* __restrict__ ukeys,
                             unsigned long long* __restrict__ uvals, int32_t* __restrict__ cnt,
                             Scalars* __restrict__ sc)
 {
     for (long long s0 = (long long)blockIdx.x * blockDim.x; s0 < cap; s0 += (long long)gridDim.x * blockDim.x) {
         const long long s = s0 + threadIdx.x;
-        const unsigned long long k = s < cap ? keys[s] : EMPTY_KEY;
+        const unsigned long long k = s < cap ? table[2 * s] : EMPTY_KEY;
         const bool occ = k != EMPTY_KEY;
         const long long u = warp_append(occ, reinterpret_cast<unsigned long long*>(&sc->n_triangles));
         if (occ) {
             ukeys[u] = k;
-            uvals[u] = vals[s];
+            uvals[u] = table[2 * s + 1];
             atomicAdd(&cnt[(int)(k >> 42)], 1);
         }
     }
@@ -312,26 +284,24 @@ void detect_triangles(Context& C, const Canvas& cv, const int32_t* labels, const
     C.off.ensure((size_t)(n + 2) * 4);
     C.fill.ensure((size_t)(n + 1) * 4);
     for (int attempt = 0;; ++attempt) {
-        C.hkeys.ensure((size_t)cap * 8);
-        C.hvals.ensure((size_t)cap * 8);
+        C.hkeys.ensure((size_t)cap * 16);
         C.ukeys.ensure((size_t)cap * 8);
         C.uvals.ensure((size_t)cap * 8);
-        IDL_CUDA(cudaMemsetAsync(C.hkeys.ptr, 0xFF, (size_t)cap * 8, C.stream));
-        IDL_CUDA(cudaMemsetAsync(C.hvals.ptr, 0xFF, (size_t)cap * 8, C.stream));
+        IDL_CUDA(cudaMemsetAsync(C.hkeys.ptr, 0xFF, (size_t)cap * 16, C.stream));
         IDL_CUDA(cudaMemsetAsync(&C.sc()->overflow, 0, sizeof(int32_t), C.stream));
         IDL_CUDA(cudaMemsetAsync(&C.sc()->n_triangles, 0, sizeof(int64_t), C.stream));
         IDL_CUDA(cudaMemsetAsync(C.cnt.ptr, 0, (size_t)(n + 1) * 4, C.stream));
 
         dim3 blk(32, 8);
-        dim3 grd(ceil_div(std::max(cv.Wd - 1, 1), 32), ceil_div(std::max(cv.Hd - 1, 1), 8 * DETECT_STRIP));
+        dim3 grd(ceil_div(std::max(cv.Wd - 1, 1), 32), ceil_div(std::max(cv.Hd - 1, 1), 8));
         k_detect<<<grd, blk, 0, C.stream>>>(labels, cv.pitch, cv.Wd, cv.Hd, pos, rank, C.hkeys.as<unsigned long long>(),
-                                            C.hvals.as<unsigned long long>(), (unsigned long long)(cap - 1), C.sc());
+                                            (unsigned long long)(cap - 1), C.sc());
         IDL_LAUNCH();
         if (mid) IDL_CUDA(cudaEventRecord(mid, C.stream));
         C.mark(PM_DETECT);
         const int g1 = (int)std::min<int64_t>(ceil_div(cap, 256), C.num_sms * 16);
-        k_enumerate<<<g1, 256, 0, C.stream>>>(C.hkeys.as<unsigned long long>(), C.hvals.as<unsigned long long>(),
-                                              cap, C.ukeys.as<unsigned long long>(),
+        k_enumerate<<<g1, 256, 0, C.stream>>>(C.hkeys.as<unsigned long long>(), cap,
+                                              C.ukeys.as<unsigned long long>(),
                                               C.uvals.as<unsigned long long>(), C.cnt.as<int32_t>(), C.sc());
         IDL_LAUNCH();
         C.fetch_scalars();
