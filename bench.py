@@ -666,6 +666,7 @@ def run_ours(args, rank, world):
             print(json.dumps({"metric": METRIC, "value": value, "unit": "Mpixel/s", "ms_per_step": ms / args.steps,
                               "stages_ms": {k[:-3]: round(v, 4) for k, v in stage.items()},
                               "schedule": schedule, "autotune_ms": tuned_u, "passes": p0["passes"],
+                              "sparse_pass_trace": ctx.pass_trace(),
                               "gpu_launches": int(launches),
                               "roofline_achieved_gbs": achieved, "clocks": clocks}), flush=True)
         return

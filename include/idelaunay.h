@@ -157,6 +157,12 @@ IDL_API int idl_context_set_profiling(idl_context* ctx, int enable);
 #define IDL_PROF_PROP_BYTES 15  /* algorithmic HBM bytes of stage (a): 8 per cell update */
 #define IDL_PROF_COUNT 16
 IDL_API int idl_context_last_profile(idl_context* ctx, double* out, int n);
+/* Per-pass trace of the persistent propagation kernel in the last profiled
+ * run: *n_out passes; up to `capacity` of them, each pass's duration in ns
+ * (GPU global timer) into ns_out and its work-list length in 8 x 8 micro-tiles
+ * into tiles_out (either may be NULL).  Empty when the run did not use it.
+ * No counterpart in the reference. */
+IDL_API int idl_context_pass_trace(idl_context* ctx, int64_t* ns_out, int32_t* tiles_out, int capacity, int* n_out);
 
 /* ---- stage (a): Voronoi().compute ----------------------------------- */
 /* Replaces cuda_compute_voronoi (src/cuda/voronoi.cuh:32-35,

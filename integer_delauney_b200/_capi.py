@@ -52,6 +52,7 @@ SIGNATURES = {
     "idl_context_synchronize": (_i32, [_vp]),
     "idl_context_set_schedule": (_i32, [_vp, _i32]),
     "idl_context_set_tile": (_i32, [_vp, _i32, ctypes.POINTER(_i32)]),
+    "idl_context_pass_trace": (_i32, [_vp, _vp, _vp, _i32, ctypes.POINTER(_i32)]),
     "idl_context_workspace_bytes": (_i32, [_vp, _pi64]),
     "idl_context_set_profiling": (_i32, [_vp, _i32]),
     "idl_context_last_profile": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _i32]),
@@ -212,6 +213,17 @@ class Context:
         buf = (ctypes.c_double * len(self.PROFILE_KEYS))()
         check(self._lib.idl_context_last_profile(self.handle, buf, len(self.PROFILE_KEYS)))
         return {k: float(buf[i]) for i, k in enumerate(self.PROFILE_KEYS)}
+
+    def pass_trace(self) -> list[tuple[int, float]]:
+        """(work-list micro-tiles, microseconds) of each pass of the persistent
+        kernel in the last profiled run (idl_context_pass_trace)."""
+        n = _i32(0)
+        check(self._lib.idl_context_pass_trace(self.handle, None, None, 0, ctypes.byref(n)))
+        ns = np.zeros(n.value, dtype=np.int64)
+        tiles = np.zeros(n.value, dtype=np.int32)
+        check(self._lib.idl_context_pass_trace(self.handle, ns.ctypes.data, tiles.ctypes.data, n.value,
+                                               ctypes.byref(n)))
+        return [(int(t), round(float(v) / 1e3, 2)) for t, v in zip(tiles, ns)]
 
     def workspace_bytes(self) -> int:
         v = ctypes.c_int64(0)

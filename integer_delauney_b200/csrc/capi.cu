@@ -385,6 +385,19 @@ int idl_context_set_profiling(idl_context* ctx, int enable)
     IDL_API_END
 }
 
+int idl_context_pass_trace(idl_context* ctx, int64_t* ns_out, int32_t* tiles_out, int capacity, int* n_out)
+{
+    IDL_API_BEGIN
+    if (!ctx || !n_out) invalid("arguments must not be NULL");
+    const Profile& P = ctx->prof;
+    *n_out = (int)P.pass_ns.size();
+    for (int i = 0; i < capacity && i < (int)P.pass_ns.size(); ++i) {
+        if (ns_out) ns_out[i] = P.pass_ns[i];
+        if (tiles_out) tiles_out[i] = P.pass_tiles[i];
+    }
+    IDL_API_END
+}
+
 int idl_context_last_profile(idl_context* ctx, double* out, int n)
 {
     IDL_API_BEGIN

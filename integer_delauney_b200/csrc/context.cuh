@@ -14,6 +14,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 
@@ -122,6 +123,9 @@ struct Profile {
     int64_t image_px = 0;         // output pixels
     int64_t n_triangles = 0;
     int tile_w = 0, tile_h = 0, steps_per_round = 0;
+    // persistent sparse kernel: duration (ns) and work-list length of each pass
+    std::vector<int64_t> pass_ns;
+    std::vector<int32_t> pass_tiles;
 };
 
 struct Context {
@@ -142,6 +146,7 @@ struct Context {
     DevBuf stamps;        // per-tile "already listed for round r" marks
     DevBuf counts;        // per-round list lengths
     DevBuf gsync;         // grid barrier state of the persistent propagation kernel
+    DevBuf trace;         // per-pass timestamps of the persistent kernel (profiling only)
     DevBuf bits;          // work-list dedup bitmaps of the persistent propagation kernel
     DevBuf big_tiles;     // tile rounds' last work list, handed to the persistent kernel
     DevBuf exact_dy;      // exact mode: row distance to each cell's column-nearest seed
@@ -200,7 +205,7 @@ struct Context {
     void each_buf(F&& f)
     {
         DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
-                         &tiles[0], &tiles[1], &stamps, &counts, &gsync, &bits, &big_tiles, &exact_dy, &hkeys,
+                         &tiles[0], &tiles[1], &stamps, &counts, &gsync, &trace, &bits, &big_tiles, &exact_dy, &hkeys,
                          &ukeys, &uvals, &cnt, &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded,
                          &batch_img, &batch_seed_img, &batch_rows, &batch_sid, &batch_stats, &batch_bad,
                          &batch_ximg, &batch_colimg, &batch_rowimg, &scalars};

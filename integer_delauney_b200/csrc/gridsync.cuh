@@ -11,6 +11,14 @@ namespace idl {
 
 constexpr unsigned SPIN_LIMIT = 1u << 24;   // barrier polls before giving up
 
+// Nanoseconds of the GPU's global timer (for per-pass profiling traces).
+__device__ __forceinline__ unsigned long long global_timer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 struct GridSync {
     unsigned count;
     unsigned gen;

@@ -720,6 +720,8 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, i
 {
     C.prof.tiles = C.prof.rounds = C.prof.passes = 0;
     C.prof.prop_bytes = 0.0;
+    C.prof.pass_ns.clear();
+    C.prof.pass_tiles.clear();
     if (mode != IDL_MODE_REFERENCE || seed_pos) return propagate_rounds(C, mode, cv, pos, seed_pos, n_new, false);
     // From scratch in reference semantics: run on owner keys, then map every
     // owned cell back to its owner's id.

@@ -215,8 +215,10 @@ template <bool KEYS>
 __global__ void __launch_bounds__(SJ_THREADS, 1)
 k_sparse_jacobi(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, const uint32_t* __restrict__ pos,
                 uint32_t* bits0, uint32_t* bits1, int32_t* list0, int32_t* list1, int32_t* counts, int max_steps,
-                int mt_x, int mt_y, GridSync* gs)
+                int mt_x, int mt_y, GridSync* gs, unsigned long long* trace)
 {
+    // trace (profiling only): the global timer at the start and after each pass
+    if (trace && blockIdx.x == 0 && threadIdx.x == 0) trace[0] = global_timer_ns();
     __shared__ int32_t s_list[STAGE];
     __shared__ int s_n, s_cut, s_base, s_m;
     const int lane = threadIdx.x & 31;
@@ -255,6 +257,7 @@ k_sparse_jacobi(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, con
         __syncthreads();
         for (int i = threadIdx.x; i < s_m; i += blockDim.x) lout[s_base + i] = s_list[i];
         if (!grid_sync(gs, gridDim.x, gen_local)) return;
+        if (trace && blockIdx.x == 0 && threadIdx.x == 0) trace[t + 1] = global_timer_ns();
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) gs->passes = t;
 }
@@ -423,7 +426,12 @@ int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos,
     int32_t* p1 = C.lab[1].as<int32_t>();
     GridSync* gs = C.gsync.as<GridSync>();
     int pitch = cv.pitch, Wd = cv.Wd, Hd = cv.Hd, ms = max_steps, mx = mt_x, my = mt_y;
-    void* args[] = {&p0, &p1, &pitch, &Wd, &Hd, (void*)&pos, &b0, &b1, &l0, &l1, &counts, &ms, &mx, &my, &gs};
+    unsigned long long* trace = nullptr;
+    if (C.prof.enabled) {
+        C.trace.ensure(((size_t)max_steps + 2) * 8);
+        trace = C.trace.as<unsigned long long>();
+    }
+    void* args[] = {&p0, &p1, &pitch, &Wd, &Hd, (void*)&pos, &b0, &b1, &l0, &l1, &counts, &ms, &mx, &my, &gs, &trace};
     GridSync h{};
     {
         // One persistent grid per device at a time: the kernel fills every SM,
@@ -442,6 +450,14 @@ int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos,
     if (C.prof.enabled) {
         std::vector<int32_t> hc((size_t)passes + 1);
         IDL_CUDA(cudaMemcpy(hc.data(), counts, hc.size() * 4, cudaMemcpyDeviceToHost));
+        std::vector<unsigned long long> ht((size_t)passes + 1);
+        IDL_CUDA(cudaMemcpy(ht.data(), trace, ht.size() * 8, cudaMemcpyDeviceToHost));
+        C.prof.pass_ns.clear();
+        C.prof.pass_tiles.clear();
+        for (int64_t i = 0; i < passes; ++i) {
+            C.prof.pass_ns.push_back((int64_t)(ht[i + 1] - ht[i]));
+            C.prof.pass_tiles.push_back(hc[i]);
+        }
         int64_t tiles = 0;
         for (int32_t c : hc) tiles += c;
         // accumulated: a hybrid run has counted its tile rounds already
