@@ -98,7 +98,7 @@ struct Scalars {
     int32_t err_label;        // a caller-supplied label was outside [-1, n)
     int32_t overflow;         // hash table over its load limit or probe bound
     int32_t max_side;         // longest triangle side, float-truncated (triangulation.cu:355-368)
-    int32_t pad_;
+    int32_t n_big;            // tall triangles the raster hands to its block-per-triangle pass
 };
 
 struct Timing {
@@ -147,6 +147,7 @@ struct Context {
     DevBuf counts;        // per-round list lengths
     DevBuf gsync;         // grid barrier state of the persistent propagation kernel
     DevBuf trace;         // per-pass timestamps of the persistent kernel (profiling only)
+    DevBuf rbig;          // raster: ids of tall triangles
     DevBuf bits;          // work-list dedup bitmaps of the persistent propagation kernel
     DevBuf big_tiles;     // tile rounds' last work list, handed to the persistent kernel
     DevBuf exact_dy;      // exact mode: row distance to each cell's column-nearest seed
@@ -205,7 +206,7 @@ struct Context {
     void each_buf(F&& f)
     {
         DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
-                         &tiles[0], &tiles[1], &stamps, &counts, &gsync, &trace, &bits, &big_tiles, &exact_dy, &hkeys,
+                         &tiles[0], &tiles[1], &stamps, &counts, &gsync, &trace, &rbig, &bits, &big_tiles, &exact_dy, &hkeys,
                          &ukeys, &uvals, &cnt, &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded,
                          &batch_img, &batch_seed_img, &batch_rows, &batch_sid, &batch_stats, &batch_bad,
                          &batch_ximg, &batch_colimg, &batch_rowimg, &scalars};

@@ -531,6 +531,180 @@ k_rounds_keys(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, int32
     if (blockIdx.x == 0 && threadIdx.x == 0) gs->passes = r;
 }
 
+// ---------------------------------------------------------------------------
+// Owner-key tile round on cell lists.  The RW x RH region (inner tile plus a
+// KS-cell halo on every side) lives in shared memory in two buffers, A (the
+// state after the last step) and B (the one before), and each step
+// evaluates only the cells of its list: the cells whose closed neighbourhood
+// changed in the step before (for the round's first step, every cell with a
+// neighbour owned by another seed -- a superset of the cells that can change,
+// since a cell whose four neighbours share its owner keeps it).  A listed
+// cell writes its new value to B, and a cell that changed lists itself and
+// its four neighbours for the next step.  A cell not listed did not change in
+// the last step, so it already holds the same value in both buffers; the
+// buffers then swap.  Work per step is proportional to the active cells, not
+// to the region, which is what thin fronts and the settling tail need.
+// ---------------------------------------------------------------------------
+template <int RW, int RH, int KS>
+struct CellTile {
+    static constexpr int TW = RW - 2 * KS, TH = RH - 2 * KS;
+    static constexpr int N = RW * RH;
+    static constexpr int WORDS = N / 32;
+    static constexpr int THREADS = 256;
+    static_assert(RW % 32 == 0 && N % 32 == 0, "rows of whole words");
+    static_assert(KS >= 1 && KS <= TW && KS <= TH, "a round's light cone must stay within the neighbour tiles");
+    static_assert(TW % 8 == 0 && TH % 8 == 0, "tiles must be whole 8 x 8 micro-tiles for the sparse hand-off");
+    static_assert(N <= 65536, "cell indices are 16 bits");
+    // dynamic shared memory: two label buffers, two lists, two bitmaps, counters
+    static constexpr size_t SMEM = 2 * N * 4 + 2 * N * 2 + 2 * WORDS * 4 + 16;
+};
+
+template <int RW, int RH>
+__device__ __forceinline__ void cell_mark(int c, uint32_t* bits, uint16_t* list, int* n)
+{
+    const uint32_t bit = 1u << (c & 31);
+    if (!(atomicOr(&bits[c >> 5], bit) & bit)) list[atomicAdd(n, 1)] = (uint16_t)c;
+}
+
+template <int RW, int RH, int KS, bool L2>
+__device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* src, int32_t* dst, int pitch, int Wd,
+                                          int Hd, int t, int tiles_x, int tiles_y, int32_t* list_out,
+                                          int32_t* count_out, int32_t* stamp, int32_t stamp_next, long long step_base,
+                                          long long* last_change)
+{
+    using T = CellTile<RW, RH, KS>;
+    constexpr int N = T::N;
+    int32_t* bufA = reinterpret_cast<int32_t*>(smem);
+    int32_t* bufB = bufA + N;
+    uint16_t* listA = reinterpret_cast<uint16_t*>(bufB + N);
+    uint16_t* listB = listA + N;
+    uint32_t* bitsA = reinterpret_cast<uint32_t*>(listB + N);
+    uint32_t* bitsB = bitsA + T::WORDS;
+    int* cnt = reinterpret_cast<int*>(bitsB + T::WORDS);   // [0], [1]: list lengths; [2]: inner change
+    const int tid = threadIdx.x;
+    const int tx = t % tiles_x, ty = t / tiles_x;
+    const int ox = tx * T::TW - KS, oy = ty * T::TH - KS;
+
+    for (int i = tid; i < N; i += blockDim.x) {
+        const int cx = i % RW, cy = i / RW;
+        const int gx = ox + cx, gy = oy + cy;
+        int32_t v = OUTSIDE;
+        if (gx >= 0 && gx < Wd && gy >= 0 && gy < Hd) {
+            const int32_t* p = src + (size_t)gy * pitch + gx;
+            v = L2 ? __ldcg(p) : *p;
+        }
+        bufA[i] = v;
+        bufB[i] = v;
+    }
+    for (int w = tid; w < T::WORDS; w += blockDim.x) {
+        bitsA[w] = 0;
+        bitsB[w] = 0;
+    }
+    if (tid < 3) cnt[tid] = 0;
+    __syncthreads();
+    // first list: cells with a neighbour owned by another seed
+    for (int i = tid; i < N; i += blockDim.x) {
+        const int32_t o = bufA[i];
+        if (o < UNDEF) continue;
+        const int cx = i % RW, cy = i / RW;
+        const bool diff = (cx > 0 && bufA[i - 1] != o) || (cx < RW - 1 && bufA[i + 1] != o) ||
+                          (cy > 0 && bufA[i - RW] != o) || (cy < RH - 1 && bufA[i + RW] != o);
+        if (diff) listA[atomicAdd(&cnt[0], 1)] = (uint16_t)i;
+    }
+    __syncthreads();
+
+    int32_t* cur = bufA;
+    int32_t* nxt = bufB;
+    uint16_t* lc = listA;
+    uint16_t* ln = listB;
+    uint32_t* bn = bitsB;   // marks of the next list
+    uint32_t* bc = bitsA;   // marks of the current list (cleared before reuse)
+    int ic = 0;             // cnt index of the current list
+    int last_step = -1;
+#pragma unroll 1
+    for (int s = 0; s < KS; ++s) {
+        const int n = cnt[ic];
+        for (int i = tid; i < n; i += blockDim.x) {
+            const int c = lc[i];
+            const int32_t own = cur[c];
+            if (own < UNDEF) continue;
+            const int cx = c % RW, cy = c / RW;
+            const int32_t l = cx > 0 ? cur[c - 1] : OUTSIDE;
+            const int32_t r = cx < RW - 1 ? cur[c + 1] : OUTSIDE;
+            const int32_t u = cy > 0 ? cur[c - RW] : OUTSIDE;
+            const int32_t d = cy < RH - 1 ? cur[c + RW] : OUTSIDE;
+            const int gx = ox + cx, gy = oy + cy;
+            int32_t k = own;
+            int32_t dd = own >= 0 ? key_dist2(gx, gy, own) : FAR;
+            relax_key(k, dd, l, gx, gy);
+            relax_key(k, dd, r, gx, gy);
+            relax_key(k, dd, u, gx, gy);
+            relax_key(k, dd, d, gx, gy);
+            nxt[c] = k;
+            if (k != own) {
+                int* nn = &cnt[ic ^ 1];
+                cell_mark<RW, RH>(c, bn, ln, nn);
+                if (cx > 0) cell_mark<RW, RH>(c - 1, bn, ln, nn);
+                if (cx < RW - 1) cell_mark<RW, RH>(c + 1, bn, ln, nn);
+                if (cy > 0) cell_mark<RW, RH>(c - RW, bn, ln, nn);
+                if (cy < RH - 1) cell_mark<RW, RH>(c + RW, bn, ln, nn);
+                if (cx >= KS && cx < KS + T::TW && cy >= KS && cy < KS + T::TH) cnt[2] = 1;
+            }
+        }
+        __syncthreads();
+        if (cnt[2]) last_step = s;
+        // the current list's marks and length are spent; clear them for reuse
+        for (int w = tid; w < T::WORDS; w += blockDim.x) bc[w] = 0;
+        __syncthreads();
+        if (tid == 0) {
+            cnt[ic] = 0;
+            cnt[2] = 0;
+        }
+        int32_t* tb = cur; cur = nxt; nxt = tb;
+        uint16_t* tl = lc; lc = ln; ln = tl;
+        uint32_t* tw = bc; bc = bn; bn = tw;
+        ic ^= 1;
+        __syncthreads();
+        if (cnt[ic] == 0) break;   // nothing can change any more in this round
+    }
+
+    // inner cells of the latest state
+    for (int i = tid; i < T::TW * T::TH; i += blockDim.x) {
+        const int cx = KS + i % T::TW, cy = KS + i / T::TW;
+        const int gx = ox + cx, gy = oy + cy;
+        if (gx < Wd && gy < Hd) dst[(size_t)gy * pitch + gx] = cur[cy * RW + cx];
+    }
+
+    if (last_step >= 0) {
+        if (tid == 0) atomicMax(last_change, step_base + last_step);
+        if (tid < 9) {
+            const int nx = tx + int(tid % 3) - 1, ny = ty + int(tid / 3) - 1;
+            if (nx >= 0 && nx < tiles_x && ny >= 0 && ny < tiles_y) {
+                const int nt = ny * tiles_x + nx;
+                if (atomicExch(&stamp[nt], stamp_next) != stamp_next) {
+                    const int slot = atomicAdd(count_out, 1);
+                    list_out[slot] = nt;
+                }
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <int RW, int RH, int KS>
+__global__ void __launch_bounds__(256)
+k_round_cells(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pitch, int Wd, int Hd,
+              const int32_t* __restrict__ list_in, const int32_t* __restrict__ count_in,
+              int32_t* __restrict__ list_out, int32_t* __restrict__ count_out, int32_t* __restrict__ stamp,
+              int32_t stamp_next, int tiles_x, int tiles_y, long long step_base, long long* __restrict__ last_change)
+{
+    extern __shared__ __align__(16) unsigned char cell_smem[];
+    const int n_items = *count_in;
+    for (int item = blockIdx.x; item < n_items; item += gridDim.x)
+        cell_tile<RW, RH, KS, false>(cell_smem, src, dst, pitch, Wd, Hd, list_in[item], tiles_x, tiles_y, list_out,
+                                     count_out, stamp, stamp_next, step_base, last_change);
+}
+
 // Seed cells of both planes take their seeds' keys (the rest of the planes
 // already holds UNDEF, or walls for a batch atlas).
 __global__ void k_seed_keys(int32_t* __restrict__ a, int32_t* __restrict__ b, int pitch,
@@ -662,6 +836,38 @@ constexpr KeyShape KEY_SHAPES[] = {
 };
 constexpr int N_KEY_SHAPES = int(sizeof(KEY_SHAPES) / sizeof(KEY_SHAPES[0]));
 
+// Cell-list tile round shapes (k_round_cells): region width x height and steps.
+struct CellShape {
+    int rw, rh, ks, tw, th;
+};
+constexpr CellShape CELL_SHAPES[] = {
+    {64, 64, 8, CellTile<64, 64, 8>::TW, CellTile<64, 64, 8>::TH},          // 48 x 48, 8 passes
+    {64, 64, 4, CellTile<64, 64, 4>::TW, CellTile<64, 64, 4>::TH},          // 56 x 56, 4 passes
+    {128, 64, 8, CellTile<128, 64, 8>::TW, CellTile<128, 64, 8>::TH},       // 112 x 48, 8 passes
+    {128, 128, 16, CellTile<128, 128, 16>::TW, CellTile<128, 128, 16>::TH},  // 96 x 96, 16 passes
+};
+constexpr int N_CELL_SHAPES = int(sizeof(CELL_SHAPES) / sizeof(CELL_SHAPES[0]));
+
+template <int RW, int RH, int KS>
+void launch_round_cells(Context& C, const int32_t* src, int32_t* dst, const Canvas& cv, const int32_t* lin,
+                        const int32_t* cin, int32_t* lout, int32_t* cout, int32_t* stamp, int32_t stamp_next,
+                        int tiles_x, int tiles_y, long long base, long long* last)
+{
+    using T = CellTile<RW, RH, KS>;
+    static bool attr = false;   // the opt-in is per function, set once per process (device-independent)
+    if (!attr) {
+        IDL_CUDA(cudaFuncSetAttribute((const void*)k_round_cells<RW, RH, KS>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
+        attr = true;
+    }
+    int per_sm = 0;
+    IDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_round_cells<RW, RH, KS>, T::THREADS, T::SMEM));
+    const int grid = std::max(1, std::min(tiles_x * tiles_y, std::max(per_sm, 1) * C.num_sms));
+    k_round_cells<RW, RH, KS><<<grid, T::THREADS, T::SMEM, C.stream>>>(src, dst, cv.pitch, cv.Wd, cv.Hd, lin, cin,
+                                                                      lout, cout, stamp, stamp_next, tiles_x,
+                                                                      tiles_y, base, last);
+}
+
 template <int NW, int KS>
 void launch_round_keys(Context& C, int per_sm, const int32_t* src, int32_t* dst, const Canvas& cv, const int32_t* lin,
                        const int32_t* cin, int32_t* lout, int32_t* cout, int32_t* stamp, int32_t stamp_next,
@@ -712,8 +918,9 @@ int64_t run_rounds_keys(Context& C, const Canvas& cv, int32_t* counts, int32_t e
 }  // namespace
 
 // Indices N_KEY_SHAPES .. 2 N_KEY_SHAPES - 1 are the same shapes with the
-// rounds run as one cooperative launch (run_rounds_keys).
-int key_tile_shapes() { return 2 * N_KEY_SHAPES; }
+// rounds run as one cooperative launch (run_rounds_keys); the next
+// N_CELL_SHAPES are the cell-list tile rounds (k_round_cells).
+int key_tile_shapes() { return 2 * N_KEY_SHAPES + N_CELL_SHAPES; }
 
 int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, int64_t n_seeds,
                   const uint32_t* seed_pos, int64_t n_new)
@@ -764,11 +971,15 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
         return propagate_sparse(C, cv, pos, seed_pos, n_new, keys);
     if (seed_pos && n_new == 0) return 0;
     const int64_t round_limit = hybrid && C.dense_rounds > 0 ? C.dense_rounds : -1;
-    const int tile = std::min(std::max(C.key_tile, 0), 2 * N_KEY_SHAPES - 1);
-    const int base_shape = tile % N_KEY_SHAPES;
-    const bool persistent = keys && C.persistent_rounds && tile >= N_KEY_SHAPES;
+    const int tile = std::min(std::max(C.key_tile, 0), key_tile_shapes() - 1);
+    const bool cells = keys && tile >= 2 * N_KEY_SHAPES;
+    const int base_shape = cells ? 0 : tile % N_KEY_SHAPES;
+    const bool persistent = keys && C.persistent_rounds && !cells && tile >= N_KEY_SHAPES;
     const KeyShape shape = KEY_SHAPES[base_shape];
-    const int tw = keys ? shape.tw : TW, th = keys ? shape.th : TH, steps = keys ? shape.ks : KSTEPS;
+    const CellShape cshape = CELL_SHAPES[cells ? tile - 2 * N_KEY_SHAPES : 0];
+    const int tw = cells ? cshape.tw : keys ? shape.tw : TW;
+    const int th = cells ? cshape.th : keys ? shape.th : TH;
+    const int steps = cells ? cshape.ks : keys ? shape.ks : KSTEPS;
     const int tiles_x = ceil_div(cv.Wd, tw), tiles_y = ceil_div(cv.Hd, th);
     const int n_tiles = tiles_x * tiles_y;
     // Bound on rounds: far above any real run (a pass count beyond the canvas
@@ -822,7 +1033,25 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
             const long long base = (long long)r * steps;
             const int32_t stamp_next = epoch + int32_t(r) + 1;
             int32_t* stamp = C.stamps.as<int32_t>();
-            if (keys) {
+            if (cells) {
+                switch (tile - 2 * N_KEY_SHAPES) {
+                case 1:
+                    launch_round_cells<64, 64, 4>(C, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
+                                                  stamp_next, tiles_x, tiles_y, base, last);
+                    break;
+                case 2:
+                    launch_round_cells<128, 64, 8>(C, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
+                                                   stamp_next, tiles_x, tiles_y, base, last);
+                    break;
+                case 3:
+                    launch_round_cells<128, 128, 16>(C, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
+                                                     stamp_next, tiles_x, tiles_y, base, last);
+                    break;
+                default:
+                    launch_round_cells<64, 64, 8>(C, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
+                                                  stamp_next, tiles_x, tiles_y, base, last);
+                }
+            } else if (keys) {
                 switch (base_shape) {
                 case 1:
                     launch_round_keys<16, 8>(C, 2, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,

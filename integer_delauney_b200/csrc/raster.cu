@@ -49,15 +49,28 @@ __global__ void k_max_side(const int32_t* __restrict__ tris, const Scalars* __re
 constexpr int RASTER_GROUP = 8;
 
 __global__ void __launch_bounds__(256)
-k_raster(const int32_t* __restrict__ tris, const Scalars* __restrict__ sc, const int32_t* __restrict__ xs,
-         const int32_t* __restrict__ ys, int W, int H, int32_t* __restrict__ tgrid)
+k_raster(const int32_t* __restrict__ tris, Scalars* __restrict__ sc, const int32_t* __restrict__ xs,
+         const int32_t* __restrict__ ys, int W, int H, int32_t* __restrict__ tgrid, int32_t* __restrict__ big)
 {
     const long long nt = sc->n_triangles;
     const int lane = threadIdx.x % RASTER_GROUP;
     const int wc = max(20, sc->max_side + 3);
     const long long groups = (long long)gridDim.x * (blockDim.x / RASTER_GROUP);
     for (long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / RASTER_GROUP; t < nt; t += groups)
-        raster_one<RASTER_GROUP>(tris + t * 5 + 2, (int32_t)t, xs, ys, W, H, wc, tgrid, lane);
+        raster_one<RASTER_GROUP>(tris + t * 5 + 2, (int32_t)t, xs, ys, W, H, wc, tgrid, lane, big, &sc->n_big);
+}
+
+// The tall triangles k_raster set aside: one block per triangle.
+__global__ void __launch_bounds__(256)
+k_raster_big(const int32_t* __restrict__ tris, const Scalars* __restrict__ sc, const int32_t* __restrict__ xs,
+             const int32_t* __restrict__ ys, int W, int H, int32_t* __restrict__ tgrid,
+             const int32_t* __restrict__ big)
+{
+    const int nb = sc->n_big;
+    for (int i = blockIdx.x; i < nb; i += gridDim.x) {
+        const int32_t t = big[i];
+        raster_rows_block(tris + (size_t)t * 5 + 2, t, xs, ys, W, H, tgrid);
+    }
 }
 
 }  // namespace
@@ -66,13 +79,17 @@ void assign_pixels(Context& C, int W, int H, const int32_t* xs, const int32_t* y
 {
     IDL_CUDA(cudaMemsetAsync(tgrid, 0xFF, (size_t)W * H * sizeof(int32_t), C.stream));
     if (max_tri <= 0) return;
-    IDL_CUDA(cudaMemsetAsync(&C.sc()->max_side, 0, sizeof(int32_t), C.stream));
+    IDL_CUDA(cudaMemsetAsync(&C.sc()->max_side, 0, 2 * sizeof(int32_t), C.stream));   // max_side, n_big
+    C.rbig.ensure((size_t)max_tri * 4);
     const int g = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(max_tri, 256), C.num_sms * 8));
     k_max_side<<<g, 256, 0, C.stream>>>(C.tris.as<int32_t>(), C.sc(), xs, ys, C.sc());
     IDL_LAUNCH();
     const int gr = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(max_tri, 256 / RASTER_GROUP),
                                                                 C.num_sms * 16));
-    k_raster<<<gr, 256, 0, C.stream>>>(C.tris.as<int32_t>(), C.sc(), xs, ys, W, H, tgrid);
+    k_raster<<<gr, 256, 0, C.stream>>>(C.tris.as<int32_t>(), C.sc(), xs, ys, W, H, tgrid, C.rbig.as<int32_t>());
+    IDL_LAUNCH();
+    k_raster_big<<<C.num_sms * 4, 256, 0, C.stream>>>(C.tris.as<int32_t>(), C.sc(), xs, ys, W, H, tgrid,
+                                                      C.rbig.as<int32_t>());
     IDL_LAUNCH();
 }
 

@@ -30,14 +30,41 @@ __device__ __forceinline__ int tri_max_side(const int32_t* v, const int32_t* __r
     return best;
 }
 
+constexpr int BIG_ROWS = 64;
+
+// The x-interval [xl, xr] of row y inside the closed triangle (a, b, c), in
+// exact integers; false if the row misses it.
+__device__ __forceinline__ bool tri_row_span(long long ax, long long ay, long long bx, long long by, long long cx,
+                                             long long cy, long long y, int W, long long& xl, long long& xr)
+{
+    const long long area2 = (bx - ax) * (cy - ay) - (by - ay) * (cx - ax);
+    const long long sgn = area2 > 0 ? 1 : -1;
+    const long long A[3] = {sgn * (ay - by), sgn * (by - cy), sgn * (cy - ay)};
+    const long long B[3] = {sgn * (bx - ax), sgn * (cx - bx), sgn * (ax - cx)};
+    const long long C0[3] = {sgn * (ax * by - ay * bx), sgn * (bx * cy - by * cx), sgn * (cx * ay - cy * ax)};
+    xl = 0;
+    xr = W - 1;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+        const long long c = B[e] * y + C0[e];   // need A*x + c >= 0
+        if (A[e] > 0) xl = max(xl, ceil_div_ll(-c, A[e]));
+        else if (A[e] < 0) xr = min(xr, floor_div(c, -A[e]));
+        else if (c < 0) return false;
+    }
+    return xl <= xr;
+}
+
 // Rasterise one triangle (vertex ids v, coordinates xs/ys) into a W x H grid
 // of triangle ids with atomicMax; a group of G lanes shares the rows (`lane`
 // is the caller's index in its group).  wc: the degenerate-case seed window
-// (max(20, max_side + 3)).
+// (max(20, max_side + 3)).  With `big` set, a proper triangle spanning
+// BIG_ROWS rows or more is appended to big (count *n_big) instead, for
+// raster_rows_block.
 template <int G = 32>
 __device__ __forceinline__ void raster_one(const int32_t* v, int32_t tid, const int32_t* __restrict__ xs,
                                            const int32_t* __restrict__ ys, int W, int H, int wc,
-                                           int32_t* __restrict__ tgrid, int lane)
+                                           int32_t* __restrict__ tgrid, int lane, int32_t* big = nullptr,
+                                           int32_t* n_big = nullptr)
 {
     const long long ax = xs[v[0]], ay = ys[v[0]], bx = xs[v[1]], by = ys[v[1]], cx = xs[v[2]], cy = ys[v[2]];
     const long long area2 = (bx - ax) * (cy - ay) - (by - ay) * (cx - ax);
@@ -67,13 +94,17 @@ __device__ __forceinline__ void raster_one(const int32_t* v, int32_t tid, const 
         return;
     }
     const long long sgn = area2 > 0 ? 1 : -1;
+    const long long y0 = max(0ll, min(ay, min(by, cy)));
+    const long long y1 = min((long long)H - 1, max(ay, max(by, cy)));
+    if (big && y1 - y0 >= BIG_ROWS) {   // tall: its rows go to a whole block, lanes along each row
+        if (lane == 0) big[atomicAdd(n_big, 1)] = tid;
+        return;
+    }
     // d_i(x, y) = A_i * x + B_i * y + C_i for edges (a,b), (b,c), (c,a):
     // cross(u - p, w - p) = (uy - wy) * px + (wx - ux) * py + (ux*wy - uy*wx)
     const long long A[3] = {sgn * (ay - by), sgn * (by - cy), sgn * (cy - ay)};
     const long long B[3] = {sgn * (bx - ax), sgn * (cx - bx), sgn * (ax - cx)};
     const long long C0[3] = {sgn * (ax * by - ay * bx), sgn * (bx * cy - by * cx), sgn * (cx * ay - cy * ax)};
-    const long long y0 = max(0ll, min(ay, min(by, cy)));
-    const long long y1 = min((long long)H - 1, max(ay, max(by, cy)));
     for (long long y = y0 + lane; y <= y1; y += G) {
         long long xl = 0, xr = W - 1;
         bool empty = false;
@@ -87,6 +118,24 @@ __device__ __forceinline__ void raster_one(const int32_t* v, int32_t tid, const 
         if (empty) continue;
         int32_t* row = tgrid + (size_t)y * W;
         for (long long x = xl; x <= xr; ++x) atomicMax(&row[x], tid);
+    }
+}
+
+// The rows of one proper triangle split over a whole block: each warp takes a
+// row, its lanes the row's pixels.
+__device__ __forceinline__ void raster_rows_block(const int32_t* v, int32_t tid, const int32_t* __restrict__ xs,
+                                                  const int32_t* __restrict__ ys, int W, int H,
+                                                  int32_t* __restrict__ tgrid)
+{
+    const long long ax = xs[v[0]], ay = ys[v[0]], bx = xs[v[1]], by = ys[v[1]], cx = xs[v[2]], cy = ys[v[2]];
+    const long long y0 = max(0ll, min(ay, min(by, cy)));
+    const long long y1 = min((long long)H - 1, max(ay, max(by, cy)));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (long long y = y0 + warp; y <= y1; y += nwarps) {
+        long long xl, xr;
+        if (!tri_row_span(ax, ay, bx, by, cx, cy, y, W, xl, xr)) continue;
+        int32_t* row = tgrid + (size_t)y * W;
+        for (long long x = xl + lane; x <= xr; x += 32) atomicMax(&row[x], tid);
     }
 }
 
