@@ -151,6 +151,7 @@ struct Context {
     DevBuf bits;          // work-list dedup bitmaps of the persistent propagation kernel
     DevBuf big_tiles;     // tile rounds' last work list, handed to the persistent kernel
     DevBuf exact_dy;      // exact mode: row distance to each cell's column-nearest seed
+    DevBuf exact_rmin;    // exact mode: per row, smallest squared row distance of each 32-column block
     int32_t stamp_epoch = 0;
     int dense_rounds = 1;  // propagation schedule from scratch (propagate.cu; idl_context_set_schedule)
     int key_tile = 0;      // tile shape of the owner-key tile round (propagate.cu; idl_context_set_tile)
@@ -206,7 +207,7 @@ struct Context {
     void each_buf(F&& f)
     {
         DevBuf* all[] = {&seeds_in, &xs, &ys, &pos, &bitmap, &scan_a, &scan_b, &scan_c, &lab[0], &lab[1],
-                         &tiles[0], &tiles[1], &stamps, &counts, &gsync, &trace, &rbig, &bits, &big_tiles, &exact_dy, &hkeys,
+                         &tiles[0], &tiles[1], &stamps, &counts, &gsync, &trace, &rbig, &bits, &big_tiles, &exact_dy, &exact_rmin, &hkeys,
                          &ukeys, &uvals, &cnt, &off, &fill, &grp, &tris, &tgrid, &vgrid, &outgrid, &padded,
                          &batch_img, &batch_seed_img, &batch_rows, &batch_sid, &batch_stats, &batch_bad,
                          &batch_ximg, &batch_colimg, &batch_rowimg, &scalars};

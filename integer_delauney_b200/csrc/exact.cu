@@ -46,23 +46,21 @@ __global__ void k_col_start(const uint32_t* __restrict__ pos, int64_t n, int Wd,
 // row distance |dy| (so the row phase reads distances instead of gathering
 // seed positions).  One thread walks one column through a band of CHUNK rows,
 // advancing through the column's seeds as the row advances (one binary search
-// per band), so a warp of adjacent columns writes each row coalesced.
+// per band), so a warp of adjacent columns writes each row coalesced.  The
+// warp also reduces, per row, the smallest dy^2 over its 32 columns into
+// rmin[y][x / 32] (INT_MAX where none of them has a seed) for the row phase.
 constexpr int CHUNK = 64;
+constexpr int RB = 32;   // columns per row block of the row phase
 
 __global__ void k_col_nearest(const uint32_t* __restrict__ pos, const int32_t* __restrict__ cs, int Wd, int Hd,
-                              int pitch, int32_t* __restrict__ col, int32_t* __restrict__ coldy)
+                              int pitch, int32_t* __restrict__ col, int32_t* __restrict__ coldy,
+                              int32_t* __restrict__ rmin, int nb)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    if (x >= Wd) return;
+    const int lane = threadIdx.x & 31;
     const int y0 = blockIdx.y * CHUNK, y1 = min(Hd, y0 + CHUNK);
-    const int32_t lo = __ldg(&cs[x]), hi = __ldg(&cs[x + 1]);
-    if (lo == hi) {
-        for (int y = y0; y < y1; ++y) {
-            col[(size_t)y * pitch + x] = UNDEF;
-            coldy[(size_t)y * pitch + x] = 0;
-        }
-        return;
-    }
+    const bool in = x < Wd;
+    const int32_t lo = in ? __ldg(&cs[x]) : 0, hi = in ? __ldg(&cs[x + 1]) : 0;
     int32_t a = lo, b = hi;   // first seed of the column with y >= y0
     while (a < b) {
         const int32_t m = (a + b) >> 1;
@@ -72,31 +70,40 @@ __global__ void k_col_nearest(const uint32_t* __restrict__ pos, const int32_t* _
     int next_y = a < hi ? (int)pos_y(__ldg(&pos[a])) : 0x7FFFFFFF;     // seed at or below
     int prev_y = a > lo ? (int)pos_y(__ldg(&pos[a - 1])) : -0x3FFFFFFF; // seed above
     for (int y = y0; y < y1; ++y) {
-        while (next_y < y) {   // the seed below was passed: it becomes the one above
-            prev_y = next_y;
-            ++a;
-            next_y = a < hi ? (int)pos_y(__ldg(&pos[a])) : 0x7FFFFFFF;
+        int32_t v = 0x7FFFFFFF;
+        if (in) {
+            if (lo == hi) {
+                col[(size_t)y * pitch + x] = UNDEF;
+                coldy[(size_t)y * pitch + x] = 0;
+            } else {
+                while (next_y < y) {   // the seed below was passed: it becomes the one above
+                    prev_y = next_y;
+                    ++a;
+                    next_y = a < hi ? (int)pos_y(__ldg(&pos[a])) : 0x7FFFFFFF;
+                }
+                const int below = next_y - y, above = y - prev_y;   // tie: the larger y, the higher id
+                const bool take_below = a < hi && (a == lo || below <= above);
+                const int dy = take_below ? below : above;
+                col[(size_t)y * pitch + x] = take_below ? a : a - 1;
+                coldy[(size_t)y * pitch + x] = dy;
+                v = dy * dy;
+            }
         }
-        const int below = next_y - y, above = y - prev_y;   // tie: the larger y, the higher id
-        const bool take_below = a < hi && (a == lo || below <= above);
-        col[(size_t)y * pitch + x] = take_below ? a : a - 1;
-        coldy[(size_t)y * pitch + x] = take_below ? below : above;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+        if (lane == 0 && x < Wd) rmin[(size_t)y * nb + x / RB] = v;
     }
 }
 
-// Phase 2: best column candidate of the row, scanning outward.  One block
-// per row.  The row's columns are grouped in blocks of RB; s_min[b] is the
-// smallest dy^2 among block b's candidates.  When the scan reaches a block's
-// nearest column at distance k, every candidate of the block costs at least
-// k^2 + s_min[b]; if that exceeds the best distance so far, nothing in the
-// block can beat or tie it and the scan jumps over it.  Cells far from every
-// seed (clustered inputs) thus test blocks instead of columns; the scan still
-// stops once k^2 exceeds the best distance.
-constexpr int RB = 32;
-constexpr int ROW_THREADS = 512;
-
+// Phase 2: best column candidate of the row, scanning outward from each cell.
+// When the scan reaches a block's nearest column at distance k, every
+// candidate of the block costs at least k^2 + rmin[y][block]; if that exceeds
+// the best distance so far, nothing in the block can beat or tie it and the
+// scan jumps over it.  Cells far from every seed (clustered inputs) thus test
+// blocks instead of columns; the scan still stops once k^2 exceeds the best
+// distance.
 __device__ __forceinline__ void scan_side(const int32_t* __restrict__ row, const int32_t* __restrict__ rdy,
-                                          const int32_t* __restrict__ s_min, int x, int Wd, int dir, int32_t& bl,
+                                          const int32_t* __restrict__ bmin, int x, int Wd, int dir, int32_t& bl,
                                           long long& bd)
 {
     int k = 1;
@@ -106,7 +113,7 @@ __device__ __forceinline__ void scan_side(const int32_t* __restrict__ row, const
         const long long kk = (long long)k * k;
         if (kk > bd) return;
         const bool entering = dir > 0 ? (xx % RB) == 0 : (xx % RB) == RB - 1;
-        if (entering && kk + s_min[xx / RB] > bd) {
+        if (entering && kk + __ldg(&bmin[xx / RB]) > bd) {
             k += RB;
             continue;
         }
@@ -123,39 +130,23 @@ __device__ __forceinline__ void scan_side(const int32_t* __restrict__ row, const
     }
 }
 
-__global__ void __launch_bounds__(ROW_THREADS)
-k_row_nearest(const int32_t* __restrict__ col, const int32_t* __restrict__ coldy, int Wd, int pitch,
-              int32_t* __restrict__ lab)
+__global__ void k_row_nearest(const int32_t* __restrict__ col, const int32_t* __restrict__ coldy,
+                              const int32_t* __restrict__ rmin, int nb, int Wd, int pitch, int32_t* __restrict__ lab)
 {
-    extern __shared__ int32_t s_min[];   // ceil(Wd / RB) entries
-    const int y = blockIdx.x;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= Wd) return;
     const int32_t* row = col + (size_t)y * pitch;
     const int32_t* rdy = coldy + (size_t)y * pitch;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int nb = (Wd + RB - 1) / RB;
-    for (int b = warp; b < nb; b += nwarps) {
-        const int x = b * RB + lane;
-        int32_t v = 0x7FFFFFFF;
-        if (x < Wd && row[x] >= 0) {
-            const int32_t dy = rdy[x];
-            v = dy * dy;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
-        if (lane == 0) s_min[b] = v;
+    const int32_t* bmin = rmin + (size_t)y * nb;
+    int32_t bl = row[x];
+    long long bd = 0x7FFFFFFFFFFFFFFFll;
+    if (bl >= 0) {
+        const long long dy = rdy[x];
+        bd = dy * dy;
     }
-    __syncthreads();
-    for (int x = threadIdx.x; x < Wd; x += blockDim.x) {
-        int32_t bl = row[x];
-        long long bd = 0x7FFFFFFFFFFFFFFFll;
-        if (bl >= 0) {
-            const long long dy = rdy[x];
-            bd = dy * dy;
-        }
-        scan_side(row, rdy, s_min, x, Wd, -1, bl, bd);
-        scan_side(row, rdy, s_min, x, Wd, +1, bl, bd);
-        lab[(size_t)y * pitch + x] = bl;
-    }
+    scan_side(row, rdy, bmin, x, Wd, -1, bl, bd);
+    scan_side(row, rdy, bmin, x, Wd, +1, bl, bd);
+    lab[(size_t)y * pitch + x] = bl;
 }
 
 }  // namespace
@@ -171,12 +162,14 @@ void propagate_exact(Context& C, const Canvas& cv, const uint32_t* pos, int64_t 
     IDL_LAUNCH();
     C.exact_dy.ensure(plane);
     const dim3 gc((unsigned)ceil_div(cv.Wd, 128), (unsigned)ceil_div(cv.Hd, CHUNK));
+    const int nb = ceil_div(cv.Wd, RB);
+    C.exact_rmin.ensure((size_t)nb * cv.Hd * 4);
     k_col_nearest<<<gc, 128, 0, C.stream>>>(pos, cs, cv.Wd, cv.Hd, cv.pitch, C.lab[1].as<int32_t>(),
-                                            C.exact_dy.as<int32_t>());
+                                            C.exact_dy.as<int32_t>(), C.exact_rmin.as<int32_t>(), nb);
     IDL_LAUNCH();
-    const size_t smem = (size_t)ceil_div(cv.Wd, RB) * 4;   // at most 4 KB (Wd <= 32767)
-    k_row_nearest<<<(unsigned)cv.Hd, ROW_THREADS, smem, C.stream>>>(C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>(),
-                                                                    cv.Wd, cv.pitch, C.lab[0].as<int32_t>());
+    const dim3 g((unsigned)ceil_div(cv.Wd, 256), (unsigned)cv.Hd);
+    k_row_nearest<<<g, 256, 0, C.stream>>>(C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>(), C.exact_rmin.as<int32_t>(),
+                                           nb, cv.Wd, cv.pitch, C.lab[0].as<int32_t>());
     IDL_LAUNCH();
     if (C.prof.enabled) {
         C.prof.passes = 0;
