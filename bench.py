@@ -528,11 +528,13 @@ def serving_case(torch, rank, seconds, slots=8):
             meta[j] = (W, H, np.sort(np.concatenate([k, keys_of(W, pts)])))
             meta.append(None)              # meta stays index-aligned with reqs
             reqs.append(("insert", j, pts))
-    def saturate(n_slots, schedule=None):
+    def saturate(n_slots, schedule=None, tile=None):
         torch.cuda.synchronize()
         srv = Server(budget_bytes=budget, slots=n_slots, border_padding=PADDING)
         if schedule is not None:
             srv.set_schedule(*schedule)
+        if tile is not None:
+            srv.set_tile(tile)
         t1 = time.perf_counter()
         fut_of = {}
         sfuts = []
@@ -553,6 +555,13 @@ def serving_case(torch, rank, seconds, slots=8):
         return dt, ok
 
     saturate(slots)                         # warm-up, untimed: the device memory pool grows once
+    # group propagation as tile rounds to convergence on cell lists (plain
+    # launches, so workers overlap) against the default hybrid schedule
+    variants = {}
+    for name, sched, tile in (("groups_cells8", (-1, -1), 8), ("groups_cells9", (-1, -1), 9),
+                              ("groups_tiles0", (-1, -1), 0)):
+        t_v, ok_v = saturate(slots, sched, tile)
+        variants[name] = ok_v / t_v
     t_srv, srv_ok = saturate(slots)
     t_one, one_ok = saturate(1)
     t_pk, pk_ok = saturate(slots, (1, 1))      # inserts in the persistent kernel instead of tile rounds
@@ -568,7 +577,8 @@ def serving_case(torch, rank, seconds, slots=8):
                  "server_insert_persistent_kernel_req_s": pk_ok / t_pk,
                  "serial_s": t_ser, "serial_req_s": ser_ok / t_ser, "serial_ok": ser_ok,
                  "speedup_vs_serial": (srv_ok / t_srv) / (ser_ok / t_ser),
-                 "speedup_vs_1slot": (srv_ok / t_srv) / (one_ok / t_one)}
+                 "speedup_vs_1slot": (srv_ok / t_srv) / (one_ok / t_one),
+                 "group_schedule_variants_req_s": variants}
     rt = [realtime(1000.0), realtime(500.0)]
     return {"workload": f"Poisson 1000 req/s for {seconds:g} s: 70% new (side log-U 128..4096, density "
                         f"0.05..1%), 30% inserts of 100..5000 seeds into resident diagrams; 40 GB budget; "

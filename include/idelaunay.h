@@ -514,6 +514,10 @@ IDL_API int idl_server_create(int device, int64_t budget_bytes, int slots, int b
  * overlap other slots' work; 0 or more: the device-wide persistent kernel).
  * Before the first request; IDL_ERR_STATE after it. */
 IDL_API int idl_server_set_schedule(idl_server* s, int group_rounds, int insert_rounds);
+/* Tile shape (idl_context_set_tile) of every slot's grouped propagation of new
+ * diagrams; shapes that run as one cooperative launch run as separate
+ * launches here, so that workers overlap.  Set before the first request. */
+IDL_API int idl_server_set_tile(idl_server* s, int shape);
 /* Runs what is queued, stops the workers and frees every object. */
 IDL_API int idl_server_destroy(idl_server* s);
 /* Queue a new diagram (seeds copied; n <= 200000).  fetch != 0: grid_out

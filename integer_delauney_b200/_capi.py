@@ -94,6 +94,7 @@ SIGNATURES = {
     "idl_server_create": (_i32, [_i32, _i64, _i32, _i32, _i32, ctypes.POINTER(_vp)]),
     "idl_server_destroy": (_i32, [_vp]),
     "idl_server_set_schedule": (_i32, [_vp, _i32, _i32]),
+    "idl_server_set_tile": (_i32, [_vp, _i32]),
     "idl_server_submit_new": (_i32, [_vp, _i32, _i32, _vp, _i64, _i32, _vp, _i64, _pi64, _pi64]),
     "idl_server_submit_insert": (_i32, [_vp, _i64, _vp, _i64, _i32, _vp, _i64, _pi64]),
     "idl_server_wait": (_i32, [_vp, _i64, ctypes.c_double, _pi64, _vp, _i64]),

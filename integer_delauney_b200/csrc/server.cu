@@ -450,6 +450,16 @@ int idl_server_set_schedule(idl_server* s, int group_rounds, int insert_rounds)
     IDL_API_END
 }
 
+int idl_server_set_tile(idl_server* s, int shape)
+{
+    IDL_API_BEGIN
+    check_server(s);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->submitted) throw idl::Error(IDL_ERR_STATE, "the tile shape is set before the first request");
+    for (auto& sl : s->slots) check_status(idl_context_set_tile(sl.batch, shape, nullptr));
+    IDL_API_END
+}
+
 int idl_server_destroy(idl_server* s)
 {
     IDL_API_BEGIN

@@ -191,6 +191,11 @@ class Server:
                                                 _capi.mode_id(mode), ctypes.byref(h)))
         self._h = h.value
 
+    def set_tile(self, shape: int) -> None:
+        """Tile shape (Context.set_tile) of the grouped new diagrams'
+        propagation; set before the first request (idl_server_set_tile)."""
+        _capi.check(self._lib.idl_server_set_tile(self._handle(), int(shape)))
+
     def set_schedule(self, group_rounds: int, insert_rounds: int) -> None:
         """Propagation schedules (Context.set_schedule) of the grouped new
         diagrams and of inserts (-1 for inserts: tile rounds from the new
