@@ -558,7 +558,7 @@ def serving_case(torch, rank, seconds, slots=8):
     # group propagation as tile rounds to convergence on cell lists (plain
     # launches, so workers overlap) against the default hybrid schedule
     variants = {}
-    for name, sched, tile in (("groups_cells8", (-1, -1), 8), ("groups_cells9", (-1, -1), 9),
+    for name, sched, tile in (("groups_hybrid_tiles0", (1, -1), 0), ("groups_cells9", (-1, -1), 9),
                               ("groups_tiles0", (-1, -1), 0)):
         t_v, ok_v = saturate(slots, sched, tile)
         variants[name] = ok_v / t_v
@@ -737,6 +737,19 @@ def run_ours(args, rank, world):
     ms_x = reduce_max(e0.elapsed_time(e1), world) / args.steps
     exact = {"workload": f"triangulate {W}x{H}, {N_SEEDS} uniform seeds, P={PADDING}, voronoi_mode=exact",
              "ms_per_step": ms_x, "mpix_s": world * W * H / (ms_x / 1e3) / 1e6}
+    d_seeds = torch.from_numpy(seeds_c).cuda()       # the clustered seed set, exact semantics
+    for _ in range(args.warmup):
+        exact_step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(c_steps):
+        exact_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_xc = reduce_max(e0.elapsed_time(e1), world) / c_steps
+    exact["clustered_ms_per_step"] = ms_xc
+    exact["clustered_mpix_s"] = world * W * H / (ms_xc / 1e3) / 1e6
     bat = batched_case(torch, lib, ctx, stream, rank)
     srv = serving_case(torch, rank, args.serve_seconds) if args.serve_seconds > 0 else None
 
