@@ -285,11 +285,16 @@ def incremental_case(cu, torch, rank, mode="reference"):
     gc.collect()
     gc.disable()                             # no collector pauses inside the timed loops
     lat = []
+    allocs = []
+    from integer_delauney_b200 import _capi
+    lib = _capi.load()
     t_all = time.perf_counter()
     for b in batches:
+        a0 = lib.idl_alloc_count()
         t0 = time.perf_counter()
         m, g = d.insert(b, as_arrays=True)
         lat.append(time.perf_counter() - t0)
+        allocs.append(lib.idl_alloc_count() - a0)
     t_all = time.perf_counter() - t_all
     n_tri = len(m)
     d2 = fresh()
@@ -305,7 +310,8 @@ def incremental_case(cu, torch, rank, mode="reference"):
                         f"(30% in a 256x256 hotspot), P={PADDING}, {mode} mode",
             "insert_ms_mean": t_all * 1e3 / len(batches), "insert_ms_p50": lat_ms[len(lat_ms) // 2],
             "insert_ms_p99": lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))],
-            "slowest_inserts": [[int(i), round(lat[i] * 1e3, 2)] for i in np.argsort(lat)[::-1][:4]],
+            "slowest_inserts": [[int(i), round(lat[i] * 1e3, 2), int(allocs[i])] for i in np.argsort(lat)[::-1][:4]],
+            "inserts_that_allocated": [int(i) for i in np.flatnonzero(np.array(allocs) > 0)][:10],
             "insert_mpix_s": Wi * Hi * len(batches) / t_all / 1e6,
             "deferred_total_ms": t_def * 1e3, "triangles_final": n_tri,
             "d2h_bytes_per_insert": Wi * Hi * 12}
