@@ -551,19 +551,65 @@ struct CellTile {
     static constexpr int N = RW * RH;
     static constexpr int WORDS = N / 32;
     static constexpr int THREADS = 256;
+    static constexpr int WPT = (WORDS + THREADS - 1) / THREADS;   // bitmap words per thread in a compaction
     static_assert(RW % 32 == 0 && N % 32 == 0, "rows of whole words");
     static_assert(KS >= 1 && KS <= TW && KS <= TH, "a round's light cone must stay within the neighbour tiles");
     static_assert(TW % 8 == 0 && TH % 8 == 0, "tiles must be whole 8 x 8 micro-tiles for the sparse hand-off");
     static_assert(N <= 65536, "cell indices are 16 bits");
-    // dynamic shared memory: two label buffers, two lists, two bitmaps, counters
-    static constexpr size_t SMEM = 2 * N * 4 + 2 * N * 2 + 2 * WORDS * 4 + 16;
+    static_assert(WPT <= 2, "a compaction handles at most two bitmap words per thread");
+    // dynamic shared memory: two label buffers, two lists, the mark bitmap, scan scratch and counters
+    static constexpr size_t SMEM = 2 * N * 4 + 2 * N * 2 + WORDS * 4 + 32 * 4 + 16;
 };
 
-template <int RW, int RH>
-__device__ __forceinline__ void cell_mark(int c, uint32_t* bits, uint16_t* list, int* n)
+// The marked cells of `bits` (one bit per cell) into `list` in ascending order;
+// the bitmap is cleared on the way.  Returns the list length (every thread).
+template <int WORDS, int WPT>
+__device__ __forceinline__ int cell_compact(uint32_t* bits, uint16_t* list, int* warp_sums)
 {
-    const uint32_t bit = 1u << (c & 31);
-    if (!(atomicOr(&bits[c >> 5], bit) & bit)) list[atomicAdd(n, 1)] = (uint16_t)c;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    uint32_t w[WPT];
+    int cnt = 0;
+#pragma unroll
+    for (int j = 0; j < WPT; ++j) {
+        const int i = tid * WPT + j;
+        w[j] = i < WORDS ? bits[i] : 0u;
+        cnt += __popc(w[j]);
+    }
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int v = lane < nwarps ? warp_sums[lane] : 0;
+        int inc = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += u;
+        }
+        if (lane < nwarps) warp_sums[lane] = inc - v;   // exclusive warp offsets
+        if (lane == nwarps - 1) warp_sums[31] = inc;    // total
+    }
+    __syncthreads();
+    int pos = warp_sums[warp] + incl - cnt;
+#pragma unroll
+    for (int j = 0; j < WPT; ++j) {
+        const int i = tid * WPT + j;
+        uint32_t m = w[j];
+        while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            list[pos++] = (uint16_t)(i * 32 + b);
+        }
+        if (i < WORDS) bits[i] = 0u;
+    }
+    const int total = warp_sums[31];
+    __syncthreads();   // warp_sums and the list are read or rewritten by the next use
+    return total;
 }
 
 template <int RW, int RH, int KS, bool L2>
@@ -578,9 +624,9 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
     int32_t* bufB = bufA + N;
     uint16_t* listA = reinterpret_cast<uint16_t*>(bufB + N);
     uint16_t* listB = listA + N;
-    uint32_t* bitsA = reinterpret_cast<uint32_t*>(listB + N);
-    uint32_t* bitsB = bitsA + T::WORDS;
-    int* cnt = reinterpret_cast<int*>(bitsB + T::WORDS);   // [0], [1]: list lengths; [2]: inner change
+    uint32_t* bits = reinterpret_cast<uint32_t*>(listB + N);
+    int* warp_sums = reinterpret_cast<int*>(bits + T::WORDS);   // 32 entries
+    int* flag = warp_sums + 32;                                 // an inner cell changed in this step
     const int tid = threadIdx.x;
     const int tx = t % tiles_x, ty = t / tiles_x;
     const int ox = tx * T::TW - KS, oy = ty * T::TH - KS;
@@ -596,11 +642,8 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
         bufA[i] = v;
         bufB[i] = v;
     }
-    for (int w = tid; w < T::WORDS; w += blockDim.x) {
-        bitsA[w] = 0;
-        bitsB[w] = 0;
-    }
-    if (tid < 3) cnt[tid] = 0;
+    for (int w = tid; w < T::WORDS; w += blockDim.x) bits[w] = 0;
+    if (tid == 0) *flag = 0;
     __syncthreads();
     // first list: cells with a neighbour owned by another seed
     for (int i = tid; i < N; i += blockDim.x) {
@@ -609,21 +652,18 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
         const int cx = i % RW, cy = i / RW;
         const bool diff = (cx > 0 && bufA[i - 1] != o) || (cx < RW - 1 && bufA[i + 1] != o) ||
                           (cy > 0 && bufA[i - RW] != o) || (cy < RH - 1 && bufA[i + RW] != o);
-        if (diff) listA[atomicAdd(&cnt[0], 1)] = (uint16_t)i;
+        if (diff) atomicOr(&bits[i >> 5], 1u << (i & 31));
     }
     __syncthreads();
+    int n = cell_compact<T::WORDS, T::WPT>(bits, listA, warp_sums);
 
     int32_t* cur = bufA;
     int32_t* nxt = bufB;
     uint16_t* lc = listA;
     uint16_t* ln = listB;
-    uint32_t* bn = bitsB;   // marks of the next list
-    uint32_t* bc = bitsA;   // marks of the current list (cleared before reuse)
-    int ic = 0;             // cnt index of the current list
     int last_step = -1;
 #pragma unroll 1
-    for (int s = 0; s < KS; ++s) {
-        const int n = cnt[ic];
+    for (int s = 0; s < KS && n > 0; ++s) {
         for (int i = tid; i < n; i += blockDim.x) {
             const int c = lc[i];
             const int32_t own = cur[c];
@@ -642,30 +682,22 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
             relax_key(k, dd, d, gx, gy);
             nxt[c] = k;
             if (k != own) {
-                int* nn = &cnt[ic ^ 1];
-                cell_mark<RW, RH>(c, bn, ln, nn);
-                if (cx > 0) cell_mark<RW, RH>(c - 1, bn, ln, nn);
-                if (cx < RW - 1) cell_mark<RW, RH>(c + 1, bn, ln, nn);
-                if (cy > 0) cell_mark<RW, RH>(c - RW, bn, ln, nn);
-                if (cy < RH - 1) cell_mark<RW, RH>(c + RW, bn, ln, nn);
-                if (cx >= KS && cx < KS + T::TW && cy >= KS && cy < KS + T::TH) cnt[2] = 1;
+                // this cell and its four neighbours may change in the next step
+                atomicOr(&bits[c >> 5], 1u << (c & 31));
+                if (cx > 0) atomicOr(&bits[(c - 1) >> 5], 1u << ((c - 1) & 31));
+                if (cx < RW - 1) atomicOr(&bits[(c + 1) >> 5], 1u << ((c + 1) & 31));
+                if (cy > 0) atomicOr(&bits[(c - RW) >> 5], 1u << ((c - RW) & 31));
+                if (cy < RH - 1) atomicOr(&bits[(c + RW) >> 5], 1u << ((c + RW) & 31));
+                if (cx >= KS && cx < KS + T::TW && cy >= KS && cy < KS + T::TH) *flag = 1;
             }
         }
         __syncthreads();
-        if (cnt[2]) last_step = s;
-        // the current list's marks and length are spent; clear them for reuse
-        for (int w = tid; w < T::WORDS; w += blockDim.x) bc[w] = 0;
-        __syncthreads();
-        if (tid == 0) {
-            cnt[ic] = 0;
-            cnt[2] = 0;
-        }
+        if (*flag) last_step = s;
+        n = cell_compact<T::WORDS, T::WPT>(bits, ln, warp_sums);   // its syncs order the flag's read and reset
+        if (tid == 0) *flag = 0;
         int32_t* tb = cur; cur = nxt; nxt = tb;
         uint16_t* tl = lc; lc = ln; ln = tl;
-        uint32_t* tw = bc; bc = bn; bn = tw;
-        ic ^= 1;
         __syncthreads();
-        if (cnt[ic] == 0) break;   // nothing can change any more in this round
     }
 
     // inner cells of the latest state
