@@ -8,11 +8,14 @@ its speed, never its result:
 * the schedule (idl_context_set_schedule): how many tile rounds run before the
   sparse kernel takes over (0 = sparse kernel only, -1 = tile rounds to
   convergence);
-* the tile shape (idl_context_set_tile): the inner tile of a round and the
-  passes it advances per round trip (48 x 48 / 8, 48 x 112 / 8, 56 x 56 / 4,
-  40 x 104 / 12), with the rounds as separate launches or all in one
-  cooperative launch.  Larger tiles waste less work on halos, more passes per
-  round trip suit thin fronts crossing empty space, fewer suit dense seed sets.
+* the tile shape (idl_context_set_tile), one of twelve:
+  0-3 are register tile rounds (inner tile / passes per round trip:
+  48 x 48 / 8, 48 x 112 / 8, 56 x 56 / 4, 40 x 104 / 12), one launch per
+  round; 4-7 are the same shapes with every round in one cooperative launch;
+  8-11 are shared-memory tile rounds that step only the 8 x 8 cells still
+  changing (48 x 48 / 8, 56 x 56 / 4, 112 x 48 / 8, 96 x 96 / 16).  Larger
+  tiles waste less work on halos, more passes per round trip suit thin
+  fronts crossing empty space, fewer suit dense seed sets.
 
 Where each pays depends on the seed density and layout: dense, uniform seed
 sets change most of the canvas for the first few passes, clustered ones leave
