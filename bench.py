@@ -616,14 +616,14 @@ def run_ours(args, rank, world):
         d_out = torch.empty((H, W, 3), dtype=torch.int32, device="cuda")
         return d_seeds, d_out
 
-    def step_device(d_seeds, d_out):
+    def step_device(d_seeds, d_out, mode=MODE):
         _capi.check(lib.idl_triangulate_device(ctx.handle, W, H, d_seeds.data_ptr(), d_seeds.shape[0], PADDING,
-                                               _capi.mode_id(MODE), d_out.data_ptr(), None))
+                                               _capi.mode_id(mode), d_out.data_ptr(), None))
 
-    def time_device(seeds_np, steps, warmup, profile=False):
+    def time_device(seeds_np, steps, warmup, profile=False, mode=MODE):
         d_seeds, d_out = device_case(seeds_np)
         for _ in range(warmup):
-            step_device(d_seeds, d_out)
+            step_device(d_seeds, d_out, mode)
         ctx.set_profiling(profile)
         torch.cuda.synchronize()
         if world > 1:
@@ -634,7 +634,7 @@ def run_ours(args, rank, world):
         with ClockSampler(dev) as clk:
             e0.record(stream)
             for _ in range(steps):
-                step_device(d_seeds, d_out)
+                step_device(d_seeds, d_out, mode)
                 if profile:
                     profs.append(ctx.last_profile())
             e1.record(stream)
@@ -698,8 +698,9 @@ def run_ours(args, rank, world):
     tuned_c = {f"{s},{t}": round(v, 3) for (s, t), v in autotune.last_report.items()}
     ctx.set_stream(stream.cuda_stream)
     c_steps = max(1, args.steps // 2)
-    ms_c, profs_c, _, _ = time_device(seeds_c, c_steps, 1, profile=True)
+    ms_c, _, _, _ = time_device(seeds_c, c_steps, args.warmup)
     value_c = world * W * H * c_steps / (ms_c / 1e3) / 1e6
+    _, profs_c, _, _ = time_device(seeds_c, c_steps, 1, profile=True)
     autotune.apply(ctx, schedule)
 
     # end to end through the public drop-in call, pinned host seeds
@@ -729,38 +730,21 @@ def run_ours(args, rank, world):
     inc_exact = incremental_case(cu, torch, rank, "exact")
 
     # the same 4096 x 4096 step in exact semantics (nearest seed, ties to the
-    # higher id; history-independent), device-resident like the headline
-    d_seeds = torch.from_numpy(seeds_u).cuda()
-    d_out = torch.empty((H, W, 3), dtype=torch.int32, device="cuda")
-
-    def exact_step():
-        _capi.check(lib.idl_triangulate_device(ctx.handle, W, H, d_seeds.data_ptr(), d_seeds.shape[0], PADDING,
-                                               _capi.MODE_EXACT, d_out.data_ptr(), None))
-    for _ in range(args.warmup):
-        exact_step()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        exact_step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms_x = reduce_max(e0.elapsed_time(e1), world) / args.steps
+    # higher id; history-independent), device-resident like the headline,
+    # then its stages in a second, profiled run
+    ms_x, _, _, _ = time_device(seeds_u, args.steps, args.warmup, mode="exact")
+    ms_x /= args.steps
+    _, profs_x, _, _ = time_device(seeds_u, args.steps, 1, profile=True, mode="exact")
     exact = {"workload": f"triangulate {W}x{H}, {N_SEEDS} uniform seeds, P={PADDING}, voronoi_mode=exact",
-             "ms_per_step": ms_x, "mpix_s": world * W * H / (ms_x / 1e3) / 1e6}
-    d_seeds = torch.from_numpy(seeds_c).cuda()       # the clustered seed set, exact semantics
-    for _ in range(args.warmup):
-        exact_step()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(c_steps):
-        exact_step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms_xc = reduce_max(e0.elapsed_time(e1), world) / c_steps
+             "ms_per_step": ms_x, "mpix_s": world * W * H / (ms_x / 1e3) / 1e6,
+             "stages_ms": {k[:-3]: round(statistics.mean(p[k] for p in profs_x), 4) for k in keys}}
+    # the clustered seed set, exact semantics
+    ms_xc, _, _, _ = time_device(seeds_c, c_steps, args.warmup, mode="exact")
+    ms_xc /= c_steps
+    _, profs_xc, _, _ = time_device(seeds_c, c_steps, 1, profile=True, mode="exact")
     exact["clustered_ms_per_step"] = ms_xc
     exact["clustered_mpix_s"] = world * W * H / (ms_xc / 1e3) / 1e6
+    exact["clustered_stages_ms"] = {k[:-3]: round(statistics.mean(p[k] for p in profs_xc), 4) for k in keys}
     bat = batched_case(torch, lib, ctx, stream, rank)
     srv = serving_case(torch, rank, args.serve_seconds) if args.serve_seconds > 0 else None
 

@@ -118,19 +118,22 @@ IDL_API int idl_context_workspace_bytes(idl_context* ctx, int64_t* bytes_out);
  * A continued propagation (an incremental object's insert using this context)
  * runs in the sparse kernel, or with dense_rounds < 0 as tile rounds starting
  * from the tiles around the new seeds.  Results do not depend on it, only the
- * time does.  Default 1.  No counterpart in the reference (its schedule is
- * one full pass per launch). */
+ * time does.  Default 3 (the fastest at 4096 x 4096 with 200 000 uniform seeds;
+ * integer_delauney_b200.autotune picks per input class).  No counterpart in
+ * the reference (its schedule is one full pass per launch). */
 IDL_API int idl_context_set_schedule(idl_context* ctx, int dense_rounds);
 
 /* Tile shape of a from-scratch propagation's tile rounds (reference
- * semantics), as an index: 0 = 48 x 48 cells advanced 8 passes per round
- * (default), 1 = 48 x 112 / 8 passes, 2 = 56 x 56 / 4 passes,
- * 3 = 40 x 104 / 12 passes, one launch per round; 4..7 = the same shapes with
- * all rounds in one cooperative launch separated by a bounded grid barrier.
- * Results do not depend on it, only the time does.
- * *n_shapes_out (may be NULL) receives the number of shapes; an index outside
- * [0, n) is IDL_ERR_INVALID.  No counterpart in the reference (fixed 16 x 16
- * blocks, one pass per launch, src/cuda/voronoi.cu:97-98). */
+ * semantics), as an index.  Register tile rounds, one launch per round:
+ * 0 = 48 x 48 cells advanced 8 passes per round, 1 = 48 x 112 / 8 passes,
+ * 2 = 56 x 56 / 4 passes, 3 = 40 x 104 / 12 passes; 4..7 = the same shapes
+ * with all rounds in one cooperative launch separated by a bounded grid
+ * barrier; 8..11 = cell-list tile rounds in shared memory, stepping only the
+ * cells that can still change: 48 x 48 / 8, 56 x 56 / 4 (default),
+ * 112 x 48 / 8, 96 x 96 / 16.  Results do not depend on it, only the time
+ * does.  *n_shapes_out (may be NULL) receives the number of shapes; an index
+ * outside [0, n) is IDL_ERR_INVALID.  No counterpart in the reference (fixed
+ * 16 x 16 blocks, one pass per launch, src/cuda/voronoi.cu:97-98). */
 IDL_API int idl_context_set_tile(idl_context* ctx, int shape, int* n_shapes_out);
 
 /* Record per-stage CUDA events on the context's stream for every following

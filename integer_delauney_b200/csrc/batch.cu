@@ -23,8 +23,10 @@
 // The number of launches and host synchronisations is independent of the
 // number of images.
 #include "raster.cuh"
+#include "row_hull.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <memory>
 #include <numeric>
@@ -223,6 +225,18 @@ __global__ void k_bx_row_nearest(const int32_t* __restrict__ col, const int32_t*
         }
     }
     lab[(size_t)y * pitch + m.ox + x] = bl;
+}
+
+// The lower-hull row pass (row_hull.cuh) on one image row of the atlas per
+// block: O(Wp) whatever the image's seed layout.
+__global__ void __launch_bounds__(HULL_THREADS)
+k_bx_row_hull(const int32_t* __restrict__ col, const int32_t* __restrict__ coldy, const XImg* __restrict__ xi,
+              const int32_t* __restrict__ rowimg, int pitch, int32_t* __restrict__ lab)
+{
+    const int64_t r = blockIdx.x;
+    const XImg m = xi[rowimg[r]];
+    const size_t o = (size_t)(m.oy + (int)(r - m.row_off)) * pitch + m.ox;
+    row_hull(col + o, coldy + o, m.Wp, lab + o);
 }
 
 __device__ __forceinline__ int tri_image(const int32_t* row, const int32_t* __restrict__ sid_img)
@@ -444,9 +458,22 @@ void exact_atlas(Context& C, const Plan& pl, int P, const Canvas& cv)
     k_bx_col_nearest<<<dim3(nblk(n_cols, 128), (unsigned)((max_hp + XCHUNK - 1) / XCHUNK)), 128, 0, C.stream>>>(
         pos, d_xi, d_colimg, cs, n_cols, cv.pitch, C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>());
     IDL_LAUNCH();
-    k_bx_row_nearest<<<dim3((unsigned)n_rows, (unsigned)((max_wp + 255) / 256)), 256, 0, C.stream>>>(
-        C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>(), d_xi, C.batch_rowimg.as<int32_t>(), cv.pitch,
-        C.lab[0].as<int32_t>());
+    if (max_wp <= HULL_MAX_W) {
+        static std::atomic<uint64_t> opted{0};   // the shared-memory opt-in is per device
+        const uint64_t bit = 1ull << (C.device & 63);
+        if (!(opted.load(std::memory_order_acquire) & bit)) {
+            IDL_CUDA(cudaFuncSetAttribute((const void*)k_bx_row_hull, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)row_hull_smem(HULL_MAX_W)));
+            opted.fetch_or(bit, std::memory_order_acq_rel);
+        }
+        k_bx_row_hull<<<(unsigned)n_rows, HULL_THREADS, row_hull_smem(max_wp), C.stream>>>(
+            C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>(), d_xi, C.batch_rowimg.as<int32_t>(), cv.pitch,
+            C.lab[0].as<int32_t>());
+    } else {
+        k_bx_row_nearest<<<dim3((unsigned)n_rows, (unsigned)((max_wp + 255) / 256)), 256, 0, C.stream>>>(
+            C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>(), d_xi, C.batch_rowimg.as<int32_t>(), cv.pitch,
+            C.lab[0].as<int32_t>());
+    }
     IDL_LAUNCH();
 }
 

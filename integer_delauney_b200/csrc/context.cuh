@@ -99,6 +99,7 @@ struct Scalars {
     int32_t overflow;         // hash table over its load limit or probe bound
     int32_t max_side;         // longest triangle side, float-truncated (triangulation.cu:355-368)
     int32_t n_big;            // tall triangles the raster hands to its block-per-triangle pass
+    int32_t n_handoff;        // micro-tiles the last tile round hands to the persistent kernel
 };
 
 struct Timing {
@@ -153,8 +154,8 @@ struct Context {
     DevBuf exact_dy;      // exact mode: row distance to each cell's column-nearest seed
     DevBuf exact_rmin;    // exact mode: per row, smallest squared row distance of each 32-column block
     int32_t stamp_epoch = 0;
-    int dense_rounds = 1;  // propagation schedule from scratch (propagate.cu; idl_context_set_schedule)
-    int key_tile = 0;      // tile shape of the owner-key tile round (propagate.cu; idl_context_set_tile)
+    int dense_rounds = 3;  // propagation schedule from scratch (propagate.cu; idl_context_set_schedule)
+    int key_tile = 9;      // tile shape of the owner-key tile round (propagate.cu; idl_context_set_tile)
     // Whether the persistent tile shapes (key_tile >= 4) may run their rounds
     // as one device-filling cooperative launch (propagate.cu); off for
     // contexts whose work must overlap other streams' (a server's workers).
@@ -289,9 +290,23 @@ int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos, cons
 // the same state in both planes.
 int64_t propagate_sparse_from_tiles(Context& C, const Canvas& cv, const uint32_t* pos, const int32_t* big_list,
                                     int n_big, int big_tiles_x, int big_w, int big_h, bool keys = false);
-int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
-                              int64_t n_new, const int32_t* big_list, int n_big, int big_tiles_x, int sub_x,
-                              int sub_y, bool keys);
+// As propagate_sparse from scratch, with the first work list given: `marked`
+// holds n_marked distinct micro-tiles, and C.bits (sparse_bits_words(cv)
+// words for each of the two passes' bitmaps) already has their bits set in
+// the first bitmap and none in the second.  Plane 0 holds the starting state,
+// the same in plane 1 outside the listed micro-tiles.
+int64_t propagate_sparse_from_marks(Context& C, const Canvas& cv, const uint32_t* pos, const int32_t* marked,
+                                    int n_marked, bool keys);
+int sparse_bits_words(const Canvas& cv);
+struct SparseStart {
+    const uint32_t* seed_pos = nullptr;   // new seeds: the micro-tiles around them
+    int64_t n_new = 0;
+    const int32_t* big_list = nullptr;    // tiles: all their micro-tiles
+    int n_big = 0, big_tiles_x = 0, sub_x = 0, sub_y = 0;
+    const int32_t* marked = nullptr;      // micro-tiles, bitmap already set
+    int n_marked = 0;
+};
+int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos, const SparseStart& start, bool keys);
 
 // Held from launch to completion of a device-filling persistent kernel, one
 // per device: such grids run one at a time, so each one's co-residency does

@@ -10,20 +10,21 @@
 //      (a walk down the column's run of the (x, y)-sorted seeds; a tie
 //      between the seed above and the one below goes to the lower one, whose
 //      y -- and so id -- is larger);
-//   2. row phase: each cell scans the columns outward, k = 0, 1, 2, ..., taking
-//      the best (distance, id) over the column candidates, and stops once k^2
-//      exceeds its best distance: no column further out can beat or tie it.
+//   2. row phase: each cell takes the best (distance, id) over its row's
+//      column candidates.  Canvases up to HULL_MAX_W columns wide use the
+//      lower-hull pass of row_hull.cuh, O(W) per row whatever the seed
+//      layout; wider ones scan the columns outward, k = 0, 1, 2, ..., until
+//      k^2 exceeds the best distance (no column further out can beat or tie
+//      it), jumping over 32-column blocks whose nearest candidate is too far.
 // Completeness: the nearest seed s* of a cell lies in some column x*, whose
 // column candidate is at least as near (and, if as near, is the higher-id
 // one of the two equidistant seeds in that column); two candidates from
 // different columns at equal distance are ordered by column, i.e. by id.
 // Seed ids are (x asc, y asc) ranks, so "higher id" is a comparison of ids.
-//
-// Work in the row phase: dense seed sets (a few px apart) finish in a handful
-// of column reads per cell; in large empty regions the scan jumps over whole
-// blocks of columns that cannot hold a candidate as near as the best so far,
-// so it tests about distance / 32 blocks instead of distance columns.
 #include "context.cuh"
+#include "row_hull.cuh"
+
+#include <atomic>
 
 namespace idl {
 namespace {
@@ -89,9 +90,11 @@ __global__ void k_col_nearest(const uint32_t* __restrict__ pos, const int32_t* _
                 v = dy * dy;
             }
         }
+        if (rmin) {   // uniform: only the outward-scan row phase reads it
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
-        if (lane == 0 && x < Wd) rmin[(size_t)y * nb + x / RB] = v;
+            for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+            if (lane == 0 && x < Wd) rmin[(size_t)y * nb + x / RB] = v;
+        }
     }
 }
 
@@ -149,6 +152,15 @@ __global__ void k_row_nearest(const int32_t* __restrict__ col, const int32_t* __
     lab[(size_t)y * pitch + x] = bl;
 }
 
+// Phase 2: the lower-hull row pass (row_hull.cuh), one block per row.
+__global__ void __launch_bounds__(HULL_THREADS)
+k_row_hull(const int32_t* __restrict__ col, const int32_t* __restrict__ coldy, int Wd, int pitch,
+           int32_t* __restrict__ lab)
+{
+    const size_t o = (size_t)blockIdx.x * pitch;
+    row_hull(col + o, coldy + o, Wd, lab + o);
+}
+
 }  // namespace
 
 void propagate_exact(Context& C, const Canvas& cv, const uint32_t* pos, int64_t n)
@@ -162,14 +174,34 @@ void propagate_exact(Context& C, const Canvas& cv, const uint32_t* pos, int64_t 
     IDL_LAUNCH();
     C.exact_dy.ensure(plane);
     const dim3 gc((unsigned)ceil_div(cv.Wd, 128), (unsigned)ceil_div(cv.Hd, CHUNK));
+    const bool hull = cv.Wd <= HULL_MAX_W;
     const int nb = ceil_div(cv.Wd, RB);
-    C.exact_rmin.ensure((size_t)nb * cv.Hd * 4);
+    int32_t* rmin = nullptr;
+    if (!hull) {
+        C.exact_rmin.ensure((size_t)nb * cv.Hd * 4);
+        rmin = C.exact_rmin.as<int32_t>();
+    }
     k_col_nearest<<<gc, 128, 0, C.stream>>>(pos, cs, cv.Wd, cv.Hd, cv.pitch, C.lab[1].as<int32_t>(),
-                                            C.exact_dy.as<int32_t>(), C.exact_rmin.as<int32_t>(), nb);
+                                            C.exact_dy.as<int32_t>(), rmin, nb);
     IDL_LAUNCH();
-    const dim3 g((unsigned)ceil_div(cv.Wd, 256), (unsigned)cv.Hd);
-    k_row_nearest<<<g, 256, 0, C.stream>>>(C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>(), C.exact_rmin.as<int32_t>(),
-                                           nb, cv.Wd, cv.pitch, C.lab[0].as<int32_t>());
+    if (hull) {
+        // lower-hull row pass: O(W) per row
+        const size_t smem = row_hull_smem(cv.Wd);
+        static std::atomic<uint64_t> opted{0};   // the shared-memory opt-in is per device
+        const uint64_t bit = 1ull << (C.device & 63);
+        if (!(opted.load(std::memory_order_acquire) & bit)) {
+            IDL_CUDA(cudaFuncSetAttribute((const void*)k_row_hull, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)row_hull_smem(HULL_MAX_W)));
+            opted.fetch_or(bit, std::memory_order_acq_rel);
+        }
+        k_row_hull<<<(unsigned)cv.Hd, HULL_THREADS, smem, C.stream>>>(
+            C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>(), cv.Wd, cv.pitch, C.lab[0].as<int32_t>());
+    } else {
+        // wider canvases: the outward scan
+        const dim3 g((unsigned)ceil_div(cv.Wd, 256), (unsigned)cv.Hd);
+        k_row_nearest<<<g, 256, 0, C.stream>>>(C.lab[1].as<int32_t>(), C.exact_dy.as<int32_t>(), rmin, nb, cv.Wd,
+                                               cv.pitch, C.lab[0].as<int32_t>());
+    }
     IDL_LAUNCH();
     if (C.prof.enabled) {
         C.prof.passes = 0;

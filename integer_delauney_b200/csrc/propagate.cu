@@ -38,6 +38,7 @@
 #include "gridsync.cuh"
 #include "stencil.cuh"
 
+#include <atomic>
 #include <vector>
 
 namespace idl {
@@ -557,23 +558,51 @@ struct CellTile {
     static_assert(TW % 8 == 0 && TH % 8 == 0, "tiles must be whole 8 x 8 micro-tiles for the sparse hand-off");
     static_assert(N <= 65536, "cell indices are 16 bits");
     static_assert(WPT <= 2, "a compaction handles at most two bitmap words per thread");
+    static_assert(N % THREADS == 0, "every warp covers whole bitmap words in the first-list pass");
     // dynamic shared memory: two label buffers, two lists, the mark bitmap, scan scratch and counters
     static constexpr size_t SMEM = 2 * N * 4 + 2 * N * 2 + WORDS * 4 + 32 * 4 + 16;
 };
 
-// The marked cells of `bits` (one bit per cell) into `list` in ascending order;
-// the bitmap is cleared on the way.  Returns the list length (every thread).
-template <int WORDS, int WPT>
-__device__ __forceinline__ int cell_compact(uint32_t* bits, uint16_t* list, int* warp_sums)
+// The cells of `bits` (one bit per cell, rows of RW / 32 words) into `list`
+// in ascending order; the bitmap is cleared on the way.  With DILATE, `bits`
+// holds the cells that changed in the step just run and the list takes them
+// and their four neighbours within the region (the cells that can change in
+// the next step), built word by word instead of one shared atomic per mark.
+// Returns the list length (every thread); *inner_changed tells whether a
+// changed cell lies in the inner tile [KS, KS + TW) x [KS, KS + TH).
+template <int RW, int RH, int KS, int TW, int TH, int WPT, bool DILATE>
+__device__ __forceinline__ int cell_compact(uint32_t* bits, uint16_t* list, int* warp_sums, bool* inner_changed)
 {
+    constexpr int WR = RW / 32, WORDS = RW * RH / 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
     uint32_t w[WPT];
     int cnt = 0;
+    bool inner = false;
 #pragma unroll
     for (int j = 0; j < WPT; ++j) {
         const int i = tid * WPT + j;
-        w[j] = i < WORDS ? bits[i] : 0u;
-        cnt += __popc(w[j]);
+        uint32_t m = 0u;
+        if (i < WORDS) {
+            const uint32_t c = bits[i];
+            m = c;
+            if (DILATE) {
+                const int row = i / WR, wi = i % WR;
+                m |= (c << 1) | (c >> 1);
+                if (wi > 0) m |= bits[i - 1] >> 31;
+                if (wi < WR - 1) m |= bits[i + 1] << 31;
+                if (row > 0) m |= bits[i - WR];
+                if (row < RH - 1) m |= bits[i + WR];
+                if (row >= KS && row < KS + TH) {
+                    const int lo = max(KS - wi * 32, 0), hi = min(KS + TW - wi * 32, 32);
+                    if (hi > lo) {
+                        const uint32_t span = hi - lo == 32 ? 0xFFFFFFFFu : ((1u << (hi - lo)) - 1u) << lo;
+                        inner = inner || (c & span) != 0u;
+                    }
+                }
+            }
+        }
+        w[j] = m;
+        cnt += __popc(m);
     }
     int incl = cnt;
 #pragma unroll
@@ -582,7 +611,7 @@ __device__ __forceinline__ int cell_compact(uint32_t* bits, uint16_t* list, int*
         if (lane >= o) incl += v;
     }
     if (lane == 31) warp_sums[warp] = incl;
-    __syncthreads();
+    *inner_changed = __syncthreads_or(inner) != 0;   // also: every word was read before any is cleared
     if (warp == 0) {
         int v = lane < nwarps ? warp_sums[lane] : 0;
         int inc = v;
@@ -612,11 +641,21 @@ __device__ __forceinline__ int cell_compact(uint32_t* bits, uint16_t* list, int*
     return total;
 }
 
+// What the last tile round before the persistent kernel leaves it (bits null:
+// not the last round): the 8 x 8 micro-tiles that can change in the next
+// pass, as that kernel's first work list with its dedup bitmap set.
+struct Handoff {
+    uint32_t* bits;
+    int32_t* list;
+    int32_t* count;
+    int mt_x;
+};
+
 template <int RW, int RH, int KS, bool L2>
 __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* src, int32_t* dst, int pitch, int Wd,
                                           int Hd, int t, int tiles_x, int tiles_y, int32_t* list_out,
                                           int32_t* count_out, int32_t* stamp, int32_t stamp_next, long long step_base,
-                                          long long* last_change)
+                                          long long* last_change, Handoff ho)
 {
     using T = CellTile<RW, RH, KS>;
     constexpr int N = T::N;
@@ -626,7 +665,6 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
     uint16_t* listB = listA + N;
     uint32_t* bits = reinterpret_cast<uint32_t*>(listB + N);
     int* warp_sums = reinterpret_cast<int*>(bits + T::WORDS);   // 32 entries
-    int* flag = warp_sums + 32;                                 // an inner cell changed in this step
     const int tid = threadIdx.x;
     const int tx = t % tiles_x, ty = t / tiles_x;
     const int ox = tx * T::TW - KS, oy = ty * T::TH - KS;
@@ -642,20 +680,20 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
         bufA[i] = v;
         bufB[i] = v;
     }
-    for (int w = tid; w < T::WORDS; w += blockDim.x) bits[w] = 0;
-    if (tid == 0) *flag = 0;
     __syncthreads();
-    // first list: cells with a neighbour owned by another seed
+    // first list: cells with a neighbour owned by another seed; the block's
+    // 32-cell strides are warp-aligned, so each warp's ballot is one word
     for (int i = tid; i < N; i += blockDim.x) {
         const int32_t o = bufA[i];
-        if (o < UNDEF) continue;
         const int cx = i % RW, cy = i / RW;
-        const bool diff = (cx > 0 && bufA[i - 1] != o) || (cx < RW - 1 && bufA[i + 1] != o) ||
-                          (cy > 0 && bufA[i - RW] != o) || (cy < RH - 1 && bufA[i + RW] != o);
-        if (diff) atomicOr(&bits[i >> 5], 1u << (i & 31));
+        const bool diff = o >= UNDEF && ((cx > 0 && bufA[i - 1] != o) || (cx < RW - 1 && bufA[i + 1] != o) ||
+                                         (cy > 0 && bufA[i - RW] != o) || (cy < RH - 1 && bufA[i + RW] != o));
+        const uint32_t word = __ballot_sync(0xFFFFFFFFu, diff);
+        if ((tid & 31) == 0) bits[i >> 5] = word;
     }
     __syncthreads();
-    int n = cell_compact<T::WORDS, T::WPT>(bits, listA, warp_sums);
+    bool inner_changed = false;
+    int n = cell_compact<RW, RH, KS, T::TW, T::TH, T::WPT, false>(bits, listA, warp_sums, &inner_changed);
 
     int32_t* cur = bufA;
     int32_t* nxt = bufB;
@@ -681,23 +719,44 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
             relax_key(k, dd, u, gx, gy);
             relax_key(k, dd, d, gx, gy);
             nxt[c] = k;
-            if (k != own) {
-                // this cell and its four neighbours may change in the next step
-                atomicOr(&bits[c >> 5], 1u << (c & 31));
-                if (cx > 0) atomicOr(&bits[(c - 1) >> 5], 1u << ((c - 1) & 31));
-                if (cx < RW - 1) atomicOr(&bits[(c + 1) >> 5], 1u << ((c + 1) & 31));
-                if (cy > 0) atomicOr(&bits[(c - RW) >> 5], 1u << ((c - RW) & 31));
-                if (cy < RH - 1) atomicOr(&bits[(c + RW) >> 5], 1u << ((c + RW) & 31));
-                if (cx >= KS && cx < KS + T::TW && cy >= KS && cy < KS + T::TH) *flag = 1;
-            }
+            if (k != own) atomicOr(&bits[c >> 5], 1u << (c & 31));
         }
         __syncthreads();
-        if (*flag) last_step = s;
-        n = cell_compact<T::WORDS, T::WPT>(bits, ln, warp_sums);   // its syncs order the flag's read and reset
-        if (tid == 0) *flag = 0;
+        // the next list: changed cells and their neighbours
+        n = cell_compact<RW, RH, KS, T::TW, T::TH, T::WPT, true>(bits, ln, warp_sums, &inner_changed);
+        if (inner_changed) last_step = s;
         int32_t* tb = cur; cur = nxt; nxt = tb;
         uint16_t* tl = lc; lc = ln; ln = tl;
+    }
+
+    if (ho.bits) {
+        // The cells marked by the last step's changes are those that can
+        // change in the next pass.  Kept: inner cells and the ring just
+        // outside them.  A ring cell's mark here may come from a stale halo
+        // value, which only adds a micro-tile; its true marks come from the
+        // tile whose inner cells it borders.  The compactions left `bits`
+        // clear, so it holds the tile's micro-tiles here, ring included.
+        constexpr int MX = T::TW / MICRO_TILE + 2, MY = T::TH / MICRO_TILE + 2;
+        static_assert(MX * MY <= T::WORDS * 32, "micro-tile marks fit the cell bitmap");
+        const int mx0 = tx * (T::TW / MICRO_TILE) - 1, my0 = ty * (T::TH / MICRO_TILE) - 1;
+        for (int i = tid; i < n; i += blockDim.x) {
+            const int c = lc[i];
+            const int cx = c % RW, cy = c / RW;
+            if (cx < KS - 1 || cx > KS + T::TW || cy < KS - 1 || cy > KS + T::TH) continue;
+            const int gx = ox + cx, gy = oy + cy;
+            if (gx < 0 || gy < 0 || gx >= Wd || gy >= Hd) continue;
+            const int j = (gy / MICRO_TILE - my0) * MX + gx / MICRO_TILE - mx0;
+            atomicOr(&bits[j >> 5], 1u << (j & 31));
+        }
         __syncthreads();
+        for (int j = tid; j < MX * MY; j += blockDim.x) {
+            if (!((bits[j >> 5] >> (j & 31)) & 1u)) continue;
+            const int mx = mx0 + j % MX, my = my0 + j / MX;
+            const int mt = my * ho.mt_x + mx;
+            const uint32_t bit = 1u << (mt & 31);
+            if (!(atomicOr(&ho.bits[mt >> 5], bit) & bit)) ho.list[atomicAdd(ho.count, 1)] = pack_mt(mx, my);
+        }
+        __syncthreads();   // the next tile clears `bits` before its first use
     }
 
     // inner cells of the latest state
@@ -728,13 +787,31 @@ __global__ void __launch_bounds__(256)
 k_round_cells(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pitch, int Wd, int Hd,
               const int32_t* __restrict__ list_in, const int32_t* __restrict__ count_in,
               int32_t* __restrict__ list_out, int32_t* __restrict__ count_out, int32_t* __restrict__ stamp,
-              int32_t stamp_next, int tiles_x, int tiles_y, long long step_base, long long* __restrict__ last_change)
+              int32_t stamp_next, int tiles_x, int tiles_y, long long step_base, long long* __restrict__ last_change,
+              Handoff ho)
 {
     extern __shared__ __align__(16) unsigned char cell_smem[];
     const int n_items = *count_in;
     for (int item = blockIdx.x; item < n_items; item += gridDim.x)
         cell_tile<RW, RH, KS, false>(cell_smem, src, dst, pitch, Wd, Hd, list_in[item], tiles_x, tiles_y, list_out,
-                                     count_out, stamp, stamp_next, step_base, last_change);
+                                     count_out, stamp, stamp_next, step_base, last_change, ho);
+}
+
+// Plane `dst` takes plane `src`'s inner cells of the listed tiles: after it,
+// the planes agree everywhere once they agreed outside those tiles.
+__global__ void k_copy_tiles(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pitch, int Wd, int Hd,
+                             const int32_t* __restrict__ list, const int32_t* __restrict__ count, int tiles_x, int tw,
+                             int th)
+{
+    const int n_items = *count;
+    for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+        const int t = list[item];
+        const int x0 = (t % tiles_x) * tw, y0 = (t / tiles_x) * th;
+        for (int i = threadIdx.x; i < tw * th; i += blockDim.x) {
+            const int x = x0 + i % tw, y = y0 + i / tw;
+            if (x < Wd && y < Hd) dst[(size_t)y * pitch + x] = src[(size_t)y * pitch + x];
+        }
+    }
 }
 
 // Seed cells of both planes take their seeds' keys (the rest of the planes
@@ -883,21 +960,23 @@ constexpr int N_CELL_SHAPES = int(sizeof(CELL_SHAPES) / sizeof(CELL_SHAPES[0]));
 template <int RW, int RH, int KS>
 void launch_round_cells(Context& C, const int32_t* src, int32_t* dst, const Canvas& cv, const int32_t* lin,
                         const int32_t* cin, int32_t* lout, int32_t* cout, int32_t* stamp, int32_t stamp_next,
-                        int tiles_x, int tiles_y, long long base, long long* last)
+                        int tiles_x, int tiles_y, long long base, long long* last, Handoff ho)
 {
     using T = CellTile<RW, RH, KS>;
-    static bool attr = false;   // the opt-in is per function, set once per process (device-independent)
-    if (!attr) {
+    // the shared-memory opt-in belongs to each device's context: set once per device
+    static std::atomic<uint64_t> opted{0};
+    const uint64_t bit = 1ull << (C.device & 63);
+    if (!(opted.load(std::memory_order_acquire) & bit)) {
         IDL_CUDA(cudaFuncSetAttribute((const void*)k_round_cells<RW, RH, KS>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM));
-        attr = true;
+        opted.fetch_or(bit, std::memory_order_acq_rel);
     }
     int per_sm = 0;
     IDL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_round_cells<RW, RH, KS>, T::THREADS, T::SMEM));
     const int grid = std::max(1, std::min(tiles_x * tiles_y, std::max(per_sm, 1) * C.num_sms));
     k_round_cells<RW, RH, KS><<<grid, T::THREADS, T::SMEM, C.stream>>>(src, dst, cv.pitch, cv.Wd, cv.Hd, lin, cin,
                                                                       lout, cout, stamp, stamp_next, tiles_x,
-                                                                      tiles_y, base, last);
+                                                                      tiles_y, base, last, ho);
 }
 
 template <int NW, int KS>
@@ -1040,6 +1119,18 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
     k_set_i64<<<1, 1, 0, C.stream>>>(last, -1);
     IDL_LAUNCH();
 
+    // Cell-list rounds before the persistent kernel: the last one lists the
+    // micro-tiles that can still change, so the kernel's first pass runs only
+    // those, not every micro-tile of the tiles left active.
+    const bool handoff = cells && round_limit > 0;
+    Handoff ho_last{nullptr, nullptr, nullptr, 0};
+    if (handoff) {
+        const int mt_x = ceil_div(cv.Wd, MICRO_TILE), mt_y = ceil_div(cv.Hd, MICRO_TILE);
+        C.bits.ensure((size_t)sparse_bits_words(cv) * 2 * 4);
+        C.big_tiles.ensure((size_t)mt_x * mt_y * 4);
+        ho_last = Handoff{C.bits.as<uint32_t>(), C.big_tiles.as<int32_t>(), &C.sc()->n_handoff, mt_x};
+    }
+
     const int grid = std::min(n_tiles, C.num_sms * 3);
     int64_t r = 0;
     int group = 2;
@@ -1066,22 +1157,28 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
             const int32_t stamp_next = epoch + int32_t(r) + 1;
             int32_t* stamp = C.stamps.as<int32_t>();
             if (cells) {
+                Handoff ho{nullptr, nullptr, nullptr, 0};
+                if (handoff && r + 1 == round_limit) {
+                    ho = ho_last;
+                    IDL_CUDA(cudaMemsetAsync(ho.bits, 0, (size_t)sparse_bits_words(cv) * 2 * 4, C.stream));
+                    IDL_CUDA(cudaMemsetAsync(ho.count, 0, 4, C.stream));
+                }
                 switch (tile - 2 * N_KEY_SHAPES) {
                 case 1:
                     launch_round_cells<64, 64, 4>(C, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
-                                                  stamp_next, tiles_x, tiles_y, base, last);
+                                                  stamp_next, tiles_x, tiles_y, base, last, ho);
                     break;
                 case 2:
                     launch_round_cells<128, 64, 8>(C, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
-                                                   stamp_next, tiles_x, tiles_y, base, last);
+                                                   stamp_next, tiles_x, tiles_y, base, last, ho);
                     break;
                 case 3:
                     launch_round_cells<128, 128, 16>(C, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
-                                                     stamp_next, tiles_x, tiles_y, base, last);
+                                                     stamp_next, tiles_x, tiles_y, base, last, ho);
                     break;
                 default:
                     launch_round_cells<64, 64, 8>(C, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
-                                                  stamp_next, tiles_x, tiles_y, base, last);
+                                                  stamp_next, tiles_x, tiles_y, base, last, ho);
                 }
             } else if (keys) {
                 switch (base_shape) {
@@ -1141,15 +1238,28 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
         C.prof.steps_per_round = steps;
     }
     if (remaining > 0) {
-        // Hand the tail to the sparse kernel: the latest state goes to plane
-        // 0, and its first work list is every micro-tile of the tiles the
-        // next round would have run (a superset of those that can change).
+        // Hand the tail to the sparse kernel: the latest state goes to plane 0.
         if (r & 1) std::swap(C.lab[0], C.lab[1]);
-        C.big_tiles.ensure((size_t)remaining * 4);
-        IDL_CUDA(cudaMemcpyAsync(C.big_tiles.ptr, C.tiles[r & 1].ptr, (size_t)remaining * 4, cudaMemcpyDeviceToDevice,
-                                 C.stream));
-        const int64_t sparse = propagate_sparse_from_tiles(C, cv, pos, C.big_tiles.as<int32_t>(), remaining,
-                                                           tiles_x, tw, th, keys);
+        int64_t sparse = 0;
+        if (handoff && r == round_limit) {
+            // Its first work list is the last round's: the micro-tiles that can
+            // change.  The planes differ only on tiles the last round changed,
+            // all of which are on the next round's list: make them agree.
+            const int copy_grid = std::min(n_tiles, C.num_sms * 8);
+            k_copy_tiles<<<copy_grid, 256, 0, C.stream>>>(C.lab[0].as<int32_t>(), C.lab[1].as<int32_t>(), cv.pitch,
+                                                         cv.Wd, cv.Hd, C.tiles[r & 1].as<int32_t>(), counts + r,
+                                                         tiles_x, tw, th);
+            IDL_LAUNCH();
+            sparse = propagate_sparse_from_marks(C, cv, pos, C.big_tiles.as<int32_t>(), C.host_sc->n_handoff, keys);
+        } else {
+            // Its first work list is every micro-tile of the tiles the next
+            // round would have run (a superset of those that can change).
+            C.big_tiles.ensure((size_t)remaining * 4);
+            IDL_CUDA(cudaMemcpyAsync(C.big_tiles.ptr, C.tiles[r & 1].ptr, (size_t)remaining * 4,
+                                     cudaMemcpyDeviceToDevice, C.stream));
+            sparse = propagate_sparse_from_tiles(C, cv, pos, C.big_tiles.as<int32_t>(), remaining, tiles_x, tw, th,
+                                                 keys);
+        }
         passes = sparse >= 2 ? r * steps + sparse : passes;
         if (C.prof.enabled) C.prof.passes = passes;
     }

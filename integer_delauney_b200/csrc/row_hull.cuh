@@ -1,0 +1,185 @@
+// Exact-semantics row pass shared by the single-image and batched pipelines:
+// each cell of a row takes the best of its row's column candidates (the
+// nearest seed of each column, from the column pass) in O(W) per row.
+#pragma once
+
+#include "common.cuh"
+
+namespace idl {
+
+// One block per row, O(W) whatever the seed layout.  With F_x =
+// dy_x^2 + x^2 for each column x that has a candidate, the cell at column t
+// takes the column minimising F_x - 2 t x (its squared distance minus t^2),
+// ties to the larger x -- the higher id, since ids ascend with x across
+// columns.  The minimisers over t are the vertices of the lower convex hull of
+// the points (x, F_x) (the lower envelope of the columns' parabolas), in x
+// order; a point on a hull edge's interior never wins alone and, where it
+// ties, the edge's right end wins too, so the hull is kept strictly convex.
+// Vertex k (k >= 1) wins from t = ceil((F_k - F_{k-1}) / (2 (x_k - x_{k-1})))
+// on, a tie at that t included; the test "vertex k wins at t" is
+// F_k - F_{k-1} <= t * 2 (x_k - x_{k-1}), exact in 64-bit integers.
+//
+// Each of the HULL_THREADS threads builds the hull of a chunk of columns
+// (monotone chain, exact integer cross products); the chunk hulls are merged
+// pairwise in log2(HULL_THREADS) levels, each merge finding the lower common
+// tangent of two x-separated hulls by the standard two-sided walk.  A merged hull is a
+// prefix of the left one and a suffix of the right one, so it is kept as
+// linked chunk ranges, not copied.  The final hull is flattened and each cell
+// finds its vertex (a binary search for the thread's first cell, then a walk
+// as t grows).  Convex hull merging: Preparata & Hong (1977).
+constexpr int HULL_THREADS = 128;              // threads (= chunks) per row
+constexpr int32_t HULL_ABSENT = 0x7FFFFFFF;    // a column with no seed (real F < 2^31 - 1)
+constexpr int HULL_MAX_W = 28000;              // F and two int16 index rows fit shared memory
+
+// Dynamic shared memory of row_hull for rows of W columns.
+inline size_t row_hull_smem(int W) { return (size_t)W * 4 + (size_t)((W + 1) & ~1) * 2 * 2; }
+
+__device__ __forceinline__ long long hull_cross(int xa, int32_t fa, int xb, int32_t fb, int xc, int32_t fc)
+{
+    return (long long)(xb - xa) * (long long)(fc - fb) - (long long)(fb - fa) * (long long)(xc - xb);
+}
+
+// One row of Wd columns: lrow / drow hold each column's candidate label
+// (negative: none) and its |dy|; out receives the row's labels.  Called by a
+// block of HULL_THREADS threads with row_hull_smem(Wd) bytes of dynamic
+// shared memory.
+__device__ __forceinline__ void row_hull(const int32_t* __restrict__ lrow, const int32_t* __restrict__ drow, int Wd,
+                                         int32_t* __restrict__ out)
+{
+    extern __shared__ __align__(16) int32_t hull_smem[];
+    int32_t* F = hull_smem;                                          // Wd
+    int16_t* hx = reinterpret_cast<int16_t*>(F + Wd);                // chunk hulls, each in its chunk's slots
+    int16_t* flat = hx + ((Wd + 1) & ~1);                            // the final hull, in x order
+    constexpr int T = HULL_THREADS;
+    __shared__ int cb[T], ce[T], cprev[T], cnext[T], gfirst[T], glast[T], coff[T];
+    __shared__ int n_hull;
+    const int tid = threadIdx.x;
+    for (int x = tid; x < Wd; x += T) {
+        const int32_t l = lrow[x];
+        const uint32_t dy = (uint32_t)drow[x];
+        F[x] = l >= 0 ? (int32_t)(dy * dy + (uint32_t)x * (uint32_t)x) : HULL_ABSENT;
+    }
+    __syncthreads();
+
+    // chunk hulls; an odd chunk length keeps the threads' F reads on distinct banks
+    const int C = ((Wd + T - 1) / T) | 1;
+    const int x0 = tid * C, x1 = min(Wd, x0 + C);
+    int h = x0;   // the chunk's hull occupies hx[x0, h)
+    for (int x = x0; x < x1; ++x) {
+        const int32_t f = F[x];
+        if (f == HULL_ABSENT) continue;
+        while (h - x0 >= 2) {
+            const int xa = hx[h - 2], xb = hx[h - 1];
+            if (hull_cross(xa, F[xa], xb, F[xb], x, f) > 0) break;
+            --h;
+        }
+        hx[h++] = (int16_t)x;
+    }
+    cb[tid] = x0;
+    ce[tid] = h;
+    cprev[tid] = cnext[tid] = -1;
+    gfirst[tid] = glast[tid] = h > x0 ? tid : -1;
+    coff[tid] = -1;
+    __syncthreads();
+
+    // merge groups of s chunks pairwise; a group's state lives at its first chunk
+    for (int s = 1; s < T; s <<= 1) {
+        if ((tid & (2 * s - 1)) == 0) {
+            const int L = tid, R = tid + s;
+            const int lf = gfirst[L], ll = glast[L], rf = gfirst[R], rl = glast[R];
+            if (lf < 0) {
+                gfirst[L] = rf;
+                glast[L] = rl;
+            } else if (rf >= 0) {
+                int pc = ll, pi = ce[ll] - 1;   // p: the left hull's last point
+                int qc = rf, qi = cb[rf];       // q: the right hull's first point
+                for (;;) {
+                    bool moved = false;
+                    for (;;) {   // p leftwards while its predecessor does not turn left onto q
+                        int ac, ai;
+                        if (pi > cb[pc]) {
+                            ac = pc;
+                            ai = pi - 1;
+                        } else if (pc != lf) {
+                            ac = cprev[pc];
+                            ai = ce[ac] - 1;
+                        } else {
+                            break;
+                        }
+                        const int xa = hx[ai], xp = hx[pi], xq = hx[qi];
+                        if (hull_cross(xa, F[xa], xp, F[xp], xq, F[xq]) > 0) break;
+                        pc = ac;
+                        pi = ai;
+                        moved = true;
+                    }
+                    for (;;) {   // q rightwards while p, q and its successor do not turn left
+                        int bc, bi;
+                        if (qi + 1 < ce[qc]) {
+                            bc = qc;
+                            bi = qi + 1;
+                        } else if (qc != rl) {
+                            bc = cnext[qc];
+                            bi = cb[bc];
+                        } else {
+                            break;
+                        }
+                        const int xp = hx[pi], xq = hx[qi], xb = hx[bi];
+                        if (hull_cross(xp, F[xp], xq, F[xq], xb, F[xb]) > 0) break;
+                        qc = bc;
+                        qi = bi;
+                        moved = true;
+                    }
+                    if (!moved) break;
+                }
+                ce[pc] = pi + 1;
+                cb[qc] = qi;
+                cnext[pc] = qc;
+                cprev[qc] = pc;
+                glast[L] = rl;
+            }
+        }
+        __syncthreads();
+    }
+
+    // flatten: chunk offsets along the final chain, then each chunk copies its range
+    if (tid == 0) {
+        int k = 0;
+        for (int c = gfirst[0]; c >= 0; c = cnext[c]) {
+            coff[c] = k;
+            k += ce[c] - cb[c];
+            if (c == glast[0]) break;
+        }
+        n_hull = k;
+    }
+    __syncthreads();
+    if (coff[tid] >= 0)
+        for (int i = cb[tid]; i < ce[tid]; ++i) flat[coff[tid] + i - cb[tid]] = hx[i];
+    __syncthreads();
+
+    const int H = n_hull;
+    if (H == 0) {
+        for (int t = tid; t < Wd; t += T) out[t] = UNDEF;
+        return;
+    }
+    // vertex k >= 1 wins at t (ties included) iff F_k - F_{k-1} <= t * 2 (x_k - x_{k-1})
+    auto wins = [&](int k, int t) {
+        const int xa = flat[k - 1], xb = flat[k];
+        return (long long)(F[xb] - F[xa]) <= (long long)t * (2 * (xb - xa));
+    };
+    int k = 0;
+    {
+        int lo = 0, hi = H - 1;   // the last vertex that wins at the thread's first cell
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (wins(mid, tid)) lo = mid;
+            else hi = mid - 1;
+        }
+        k = lo;
+    }
+    for (int t = tid; t < Wd; t += T) {
+        while (k + 1 < H && wins(k + 1, t)) ++k;
+        out[t] = lrow[flat[k]];
+    }
+}
+
+}  // namespace idl

@@ -37,7 +37,7 @@
 namespace idl {
 namespace {
 
-constexpr int MT = 8;                       // micro-tile side
+constexpr int MT = MICRO_TILE;              // micro-tile side
 constexpr int SJ_THREADS = 1024;
 constexpr int SJ_WARPS = SJ_THREADS / 32;
 constexpr int GROUP = 2;                    // micro-tiles a warp advances together
@@ -274,9 +274,6 @@ __global__ void k_barrier_selftest(GridSync* gs, unsigned expected, unsigned spi
     if (blockIdx.x == 0 && threadIdx.x == 0) gs->passes = r;
 }
 
-// Work-list entries are micro-tile coordinates packed as mx | my << 16.
-__device__ __forceinline__ int32_t pack_mt(int mx, int my) { return mx | (my << 16); }
-
 __global__ void k_iota_list(int32_t* __restrict__ list, int n, int mt_x, int32_t* __restrict__ count)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -362,23 +359,40 @@ void grid_barrier_selftest(Context& C, int missing_arrivals, unsigned spin_limit
     if (h.passes != rounds) throw Error(IDL_ERR_INTERNAL, "grid barrier self-test did not complete its rounds");
 }
 
+int sparse_bits_words(const Canvas& cv) { return ceil_div(ceil_div(cv.Wd, MT) * ceil_div(cv.Hd, MT), 32); }
+
 int64_t propagate_sparse_from_tiles(Context& C, const Canvas& cv, const uint32_t* pos, const int32_t* big_list,
                                     int n_big, int big_tiles_x, int big_w, int big_h, bool keys)
 {
     if (big_w % MT != 0 || big_h % MT != 0) throw Error(IDL_ERR_INTERNAL, "tile sides must be micro-tile multiples");
-    return propagate_sparse_impl(C, cv, pos, nullptr, 0, big_list, n_big, big_tiles_x, big_w / MT, big_h / MT,
-                                 keys);
+    SparseStart st;
+    st.big_list = big_list;
+    st.n_big = n_big;
+    st.big_tiles_x = big_tiles_x;
+    st.sub_x = big_w / MT;
+    st.sub_y = big_h / MT;
+    return propagate_sparse_impl(C, cv, pos, st, keys);
+}
+
+int64_t propagate_sparse_from_marks(Context& C, const Canvas& cv, const uint32_t* pos, const int32_t* marked,
+                                    int n_marked, bool keys)
+{
+    SparseStart st;
+    st.marked = marked;
+    st.n_marked = n_marked;
+    return propagate_sparse_impl(C, cv, pos, st, keys);
 }
 
 int64_t propagate_sparse(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
                          int64_t n_new, bool keys)
 {
-    return propagate_sparse_impl(C, cv, pos, seed_pos, n_new, nullptr, 0, 0, 0, 0, keys);
+    SparseStart st;
+    st.seed_pos = seed_pos;
+    st.n_new = n_new;
+    return propagate_sparse_impl(C, cv, pos, st, keys);
 }
 
-int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
-                              int64_t n_new, const int32_t* big_list, int n_big, int big_tiles_x, int sub_x,
-                              int sub_y, bool keys)
+int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos, const SparseStart& st, bool keys)
 {
     const int mt_x = ceil_div(cv.Wd, MT), mt_y = ceil_div(cv.Hd, MT);
     const int n_mt = mt_x * mt_y;
@@ -387,6 +401,8 @@ int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos,
     const int max_steps = (int)std::min<int64_t>((int64_t)4 * (cv.Wd + cv.Hd) + 64, (1 << 29));
     C.tiles[0].ensure((size_t)n_mt * 4);
     C.tiles[1].ensure((size_t)n_mt * 4);
+    if (st.marked && C.bits.bytes < (size_t)n_words * 2 * 4)
+        throw Error(IDL_ERR_INTERNAL, "hand-off bitmap was not sized for this canvas");
     C.bits.ensure((size_t)n_words * 2 * 4);
     uint32_t* b0 = C.bits.as<uint32_t>();
     uint32_t* b1 = b0 + n_words;
@@ -395,17 +411,23 @@ int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos,
     int32_t* counts = C.counts.as<int32_t>();
     int32_t* l0 = C.tiles[0].as<int32_t>();
     int32_t* l1 = C.tiles[1].as<int32_t>();
-    if (big_list) {
-        if (n_big == 0) return 0;
+    if (st.marked) {
+        if (st.n_marked == 0) return 0;
+        if (st.n_marked > n_mt) throw Error(IDL_ERR_INTERNAL, "hand-off list longer than the canvas");
+        const int32_t n = st.n_marked;
+        IDL_CUDA(cudaMemcpyAsync(l0, st.marked, (size_t)n * 4, cudaMemcpyDeviceToDevice, C.stream));
+        IDL_CUDA(cudaMemcpyAsync(counts, &C.sc()->n_handoff, 4, cudaMemcpyDeviceToDevice, C.stream));
+    } else if (st.big_list) {
+        if (st.n_big == 0) return 0;
         IDL_CUDA(cudaMemsetAsync(b0, 0, (size_t)n_words * 2 * 4, C.stream));
-        k_expand_tiles<<<(unsigned)n_big, 64, 0, C.stream>>>(big_list, big_tiles_x, sub_x, sub_y, mt_x, mt_y, b0,
-                                                             l0, counts);
+        k_expand_tiles<<<(unsigned)st.n_big, 64, 0, C.stream>>>(st.big_list, st.big_tiles_x, st.sub_x, st.sub_y, mt_x,
+                                                                mt_y, b0, l0, counts);
         IDL_LAUNCH();
-    } else if (seed_pos) {
-        if (n_new == 0) return 0;
+    } else if (st.seed_pos) {
+        if (st.n_new == 0) return 0;
         IDL_CUDA(cudaMemsetAsync(b0, 0, (size_t)n_words * 2 * 4, C.stream));
-        k_seed_tiles<<<(unsigned)((n_new + 255) / 256), 256, 0, C.stream>>>(seed_pos, (int)n_new, cv.Wd, cv.Hd,
-                                                                            mt_x, b0, l0, counts);
+        k_seed_tiles<<<(unsigned)((st.n_new + 255) / 256), 256, 0, C.stream>>>(st.seed_pos, (int)st.n_new, cv.Wd,
+                                                                               cv.Hd, mt_x, b0, l0, counts);
         IDL_LAUNCH();
     } else {
         k_fill_bits<<<(unsigned)((n_words + 255) / 256), 256, 0, C.stream>>>(b0, n_words, n_mt);

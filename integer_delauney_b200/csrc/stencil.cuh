@@ -62,4 +62,9 @@ __device__ __forceinline__ void relax_key(int32_t& bk, int32_t& bd, int32_t n, i
     bd = better ? nd : bd;
 }
 
+// Work lists of the persistent propagation kernel hold 8 x 8 micro-tiles,
+// packed as mx | my << 16.
+constexpr int MICRO_TILE = 8;
+__device__ __forceinline__ int32_t pack_mt(int mx, int my) { return mx | (my << 16); }
+
 }  // namespace idl

@@ -268,8 +268,33 @@ def test_propagation_schedules_agree(kind):
         with pytest.raises(ValueError):
             ctx.set_tile(n_shapes)
     finally:
-        ctx.set_schedule(1)
-        ctx.set_tile(0)
+        ctx.set_schedule(3)   # the context defaults
+        ctx.set_tile(9)
+
+
+def test_exact_mode_lattice_ties():
+    """Seeds on a regular lattice make equidistant seeds everywhere (cells
+    halfway between lattice rows, columns and diagonals): every tie must go to
+    the higher id, in the column pass and across columns alike."""
+    W, H = 301, 203
+    xs, ys = np.meshgrid(np.arange(3, W, 6), np.arange(2, H, 4))
+    seeds = np.stack([xs.ravel(), ys.ravel()], 1).astype(np.int32)
+    s = oracle.sort_seeds(seeds, W, H)
+    want, _ = oracle.voronoi("exact", W, H, s)
+    np.testing.assert_array_equal(cu.Voronoi().compute(W, H, seeds, voronoi_mode="exact"), want)
+
+
+@pytest.mark.parametrize("W", [28000, 28001])
+def test_exact_mode_row_pass_width_limit(W):
+    """The lower-hull row pass handles canvases up to 28 000 columns; wider
+    ones take the outward scan.  Both sides of the limit, a few rows, seeds
+    with long empty stretches between them."""
+    H = 3
+    rng = np.random.default_rng(W)
+    seeds = np.unique(np.stack([rng.integers(0, W, 40), rng.integers(0, H, 40)], 1), axis=0).astype(np.int32)
+    s = oracle.sort_seeds(seeds, W, H)
+    want, _ = oracle.voronoi("exact", W, H, s)
+    np.testing.assert_array_equal(cu.Voronoi().compute(W, H, seeds, voronoi_mode="exact"), want)
 
 
 @pytest.mark.parametrize("kind", ["uniform", "clustered"])
