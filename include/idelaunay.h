@@ -160,12 +160,23 @@ IDL_API int idl_context_set_profiling(idl_context* ctx, int enable);
 #define IDL_PROF_PROP_BYTES 15  /* algorithmic HBM bytes of stage (a): 8 per cell update */
 #define IDL_PROF_COUNT 16
 IDL_API int idl_context_last_profile(idl_context* ctx, double* out, int n);
-/* Per-pass trace of the persistent propagation kernel in the last profiled
- * run: *n_out passes; up to `capacity` of them, each pass's duration in ns
- * (GPU global timer) into ns_out and its work-list length in 8 x 8 micro-tiles
- * into tiles_out (either may be NULL).  Empty when the run did not use it.
- * No counterpart in the reference. */
-IDL_API int idl_context_pass_trace(idl_context* ctx, int64_t* ns_out, int32_t* tiles_out, int capacity, int* n_out);
+/* Trace of the persistent propagation kernel in the last profiled run, one
+ * entry per work-list generation: *n_out entries; up to `capacity` of them,
+ * each one's duration in ns (GPU global timer) into ns_out, its work-list
+ * length in 8 x 8 micro-tiles into tiles_out, and the Jacobi passes it
+ * advanced into steps_out (1 for a single pass, a round's passes in the round
+ * mode of idl_context_set_tail_rounds, 0 for entering that mode); any of the
+ * three may be NULL.  Empty when the run did not use the kernel.  No
+ * counterpart in the reference. */
+IDL_API int idl_context_pass_trace(idl_context* ctx, int64_t* ns_out, int32_t* tiles_out, int32_t* steps_out,
+                                   int capacity, int* n_out);
+
+/* The persistent propagation kernel advances one pass per grid barrier while
+ * its work list is long, and several (a round, each micro-tile with a halo
+ * as wide as the round's passes) once the list holds at most `max_list`
+ * micro-tiles; 0 = never.  Default 4096.  Results do not depend on it, only
+ * the time does.  No counterpart in the reference. */
+IDL_API int idl_context_set_tail_rounds(idl_context* ctx, int max_list);
 
 /* ---- stage (a): Voronoi().compute ----------------------------------- */
 /* Replaces cuda_compute_voronoi (src/cuda/voronoi.cuh:32-35,
@@ -204,6 +215,12 @@ IDL_API int idl_triangulate(idl_context* ctx, int width, int height, const int32
  * witnessing a triangle, the first in row-major order supplies (x, y) and
  * the vertex order. */
 IDL_API int idl_get_triangles(idl_context* ctx, int32_t* tris_out, int64_t capacity);
+
+/* The vertex triples (id_a, id_b, id_c) of the same triangles, 3 int32 each
+ * in triangle-id order: what triangulate(..., as_arrays=True) returns as its
+ * vertex array (src/cuda/bindings/binding_helpers.hpp:61-87), packed on the
+ * device so the host receives only these 12 bytes per triangle. */
+IDL_API int idl_get_triangle_vertices(idl_context* ctx, int32_t* verts_out, int64_t capacity);
 
 /* Device-resident triangulate: inputs, outputs and all intermediates stay on
  * the device.  d_seeds_xy: device n*2 int32.  d_grid_out: device

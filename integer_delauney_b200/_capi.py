@@ -52,13 +52,15 @@ SIGNATURES = {
     "idl_context_synchronize": (_i32, [_vp]),
     "idl_context_set_schedule": (_i32, [_vp, _i32]),
     "idl_context_set_tile": (_i32, [_vp, _i32, ctypes.POINTER(_i32)]),
-    "idl_context_pass_trace": (_i32, [_vp, _vp, _vp, _i32, ctypes.POINTER(_i32)]),
+    "idl_context_pass_trace": (_i32, [_vp, _vp, _vp, _vp, _i32, ctypes.POINTER(_i32)]),
+    "idl_context_set_tail_rounds": (_i32, [_vp, _i32]),
     "idl_context_workspace_bytes": (_i32, [_vp, _pi64]),
     "idl_context_set_profiling": (_i32, [_vp, _i32]),
     "idl_context_last_profile": (_i32, [_vp, ctypes.POINTER(ctypes.c_double), _i32]),
     "idl_voronoi": (_i32, [_vp, _i32, _i32, _vp, _i64, _i32, _vp, _pi64]),
     "idl_triangulate": (_i32, [_vp, _i32, _i32, _vp, _i64, _vp, _i32, _i32, _vp, _pi64, _vp, _vp]),
     "idl_get_triangles": (_i32, [_vp, _vp, _i64]),
+    "idl_get_triangle_vertices": (_i32, [_vp, _vp, _i64]),
     "idl_triangulate_device": (_i32, [_vp, _i32, _i32, _vp, _i64, _i32, _i32, _vp, _pi64]),
     "idl_triangles_device": (_i32, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "idl_voronoi_noalloc": (_i32, [_i32, _i32, _vp, _i64, _i32, _vp, _vp, _pi64]),
@@ -215,16 +217,23 @@ class Context:
         check(self._lib.idl_context_last_profile(self.handle, buf, len(self.PROFILE_KEYS)))
         return {k: float(buf[i]) for i, k in enumerate(self.PROFILE_KEYS)}
 
-    def pass_trace(self) -> list[tuple[int, float]]:
-        """(work-list micro-tiles, microseconds) of each pass of the persistent
-        kernel in the last profiled run (idl_context_pass_trace)."""
+    def pass_trace(self) -> list[tuple[int, float, int]]:
+        """(work-list micro-tiles, microseconds, passes advanced) of each
+        work-list generation of the persistent kernel in the last profiled run
+        (idl_context_pass_trace)."""
         n = _i32(0)
-        check(self._lib.idl_context_pass_trace(self.handle, None, None, 0, ctypes.byref(n)))
+        check(self._lib.idl_context_pass_trace(self.handle, None, None, None, 0, ctypes.byref(n)))
         ns = np.zeros(n.value, dtype=np.int64)
         tiles = np.zeros(n.value, dtype=np.int32)
-        check(self._lib.idl_context_pass_trace(self.handle, ns.ctypes.data, tiles.ctypes.data, n.value,
-                                               ctypes.byref(n)))
-        return [(int(t), round(float(v) / 1e3, 2)) for t, v in zip(tiles, ns)]
+        steps = np.zeros(n.value, dtype=np.int32)
+        check(self._lib.idl_context_pass_trace(self.handle, ns.ctypes.data, tiles.ctypes.data, steps.ctypes.data,
+                                               n.value, ctypes.byref(n)))
+        return [(int(t), round(float(v) / 1e3, 2), int(k)) for t, v, k in zip(tiles, ns, steps)]
+
+    def set_tail_rounds(self, max_list: int) -> None:
+        """Work-list length at or below which the persistent kernel advances a
+        round of passes per barrier (idl_context_set_tail_rounds; 0 = never)."""
+        check(self._lib.idl_context_set_tail_rounds(self.handle, int(max_list)))
 
     def workspace_bytes(self) -> int:
         v = ctypes.c_int64(0)

@@ -96,20 +96,32 @@ def resolve_padding(border_padding: int) -> int:
 
 
 def build_output(tris: np.ndarray, grid: np.ndarray, as_arrays: bool):
-    """(triangle_map | verts, grid) as binding_helpers.hpp:61-87 packs it."""
+    """(triangle_map | verts, grid) as binding_helpers.hpp:61-87 packs it.
+    ``tris`` holds (x, y, a, b, c) rows, or for as_arrays already the (a, b, c)
+    triples (idl_get_triangle_vertices)."""
     if as_arrays:
+        if tris.shape[1] == 3:
+            return tris, grid
         return np.ascontiguousarray(tris[:, 2:5], dtype=np.int32), grid
     rows = tris.tolist()
     return {tid: tuple(r) for tid, r in enumerate(rows)}, grid
 
 
 def _fetch_triangles(ctx, n_tri: int) -> np.ndarray:
-    out = np.empty((max(n_tri, 0), 5), dtype=np.int32)
+    out = _host_buffer((max(n_tri, 0), 5))
     check(_capi.load().idl_get_triangles(ctx.handle, out.ctypes.data if n_tri else None, n_tri))
     return out
 
 
-def _triangulate(width, height, seeds_arr, vgrid, border_padding, mode, timings=False, debug=False):
+def _fetch_vertices(ctx, n_tri: int) -> np.ndarray:
+    """(n, 3) vertex triples, packed on the device (12 bytes per triangle cross PCIe)."""
+    out = _host_buffer((max(n_tri, 0), 3))
+    check(_capi.load().idl_get_triangle_vertices(ctx.handle, out.ctypes.data if n_tri else None, n_tri))
+    return out
+
+
+def _triangulate(width, height, seeds_arr, vgrid, border_padding, mode, timings=False, debug=False,
+                 vertices=False):
     lib = _capi.load()
     ctx = _context()
     P = resolve_padding(border_padding)
@@ -127,7 +139,7 @@ def _triangulate(width, height, seeds_arr, vgrid, border_padding, mode, timings=
                                   mode_id(mode), grid.ctypes.data, ctypes.byref(n_tri),
                                   ctypes.cast(tbuf, ctypes.c_void_p) if tbuf is not None else None,
                                   padded.ctypes.data if (padded is not None and P > 0) else None))
-        tris = _fetch_triangles(ctx, int(n_tri.value))
+        tris = (_fetch_vertices if vertices else _fetch_triangles)(ctx, int(n_tri.value))
     tdict = None
     if timings:
         tdict = {"detect_ms": float(tbuf[_capi.T_DETECT_MS]), "dedup_ms": float(tbuf[_capi.T_DEDUP_MS]),
@@ -155,7 +167,7 @@ def triangulate(width: int, height: int, seeds, border_padding: int = AUTO_BORDE
                 as_arrays: bool = False, *, voronoi_mode="reference"):
     """The whole pipeline in one call (src/cuda/bindings/triangulate.hpp:15-43)."""
     s = parse_seeds(seeds)
-    tris, grid, _, _ = _triangulate(width, height, s, None, border_padding, voronoi_mode)
+    tris, grid, _, _ = _triangulate(width, height, s, None, border_padding, voronoi_mode, vertices=as_arrays)
     return build_output(tris, grid, as_arrays)
 
 
@@ -211,7 +223,7 @@ class GridTriangulation:
                 as_arrays: bool = False, *, voronoi_mode="reference"):
         vg, s = self._prepare(voronoi_grid, seed_positions)
         H, W = vg.shape[:2]
-        tris, grid, _, _ = _triangulate(W, H, s, vg, border_padding, voronoi_mode)
+        tris, grid, _, _ = _triangulate(W, H, s, vg, border_padding, voronoi_mode, vertices=as_arrays)
         return build_output(tris, grid, as_arrays)
 
     def compute_timed(self, voronoi_grid, seed_positions, border_padding: int = AUTO_BORDER_PADDING, *,

@@ -60,23 +60,49 @@ namespace {
 
 // (H, W, 3): seed id and squared distance from the interior window of the
 // detection canvas, triangle id from the assignment (triangulation.cu:391-412).
-__global__ void k_compose3(const int32_t* __restrict__ lab, int pitch, int P, int W, int H,
-                           const int32_t* __restrict__ xs, const int32_t* __restrict__ ys,
-                           const int32_t* __restrict__ tgrid, int32_t* __restrict__ out)
+// A block composes 256 consecutive pixels of the flattened image in shared
+// memory and stores their 3 KB as 16-byte vectors when the output is 16-byte
+// aligned (each block's slice starts at a multiple of 3 KB), instead of
+// three 4-byte stores 12 bytes apart per pixel.
+constexpr int COMPOSE_PX = 256;
+
+__global__ void __launch_bounds__(COMPOSE_PX)
+k_compose3(const int32_t* __restrict__ lab, int pitch, int P, int W, int64_t n_px, const int32_t* __restrict__ xs,
+           const int32_t* __restrict__ ys, const int32_t* __restrict__ tgrid, int32_t* __restrict__ out, bool vec)
 {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    if (x >= W) return;
-    const int32_t l = lab[(size_t)(y + P) * pitch + x + P];
-    int32_t d = -1;
-    if (l >= 0) {
-        const int32_t dx = x - __ldg(&xs[l]), dy = y - __ldg(&ys[l]);
-        d = dx * dx + dy * dy;
+    __shared__ __align__(16) int32_t stage[COMPOSE_PX * 3];
+    const int64_t i0 = (int64_t)blockIdx.x * COMPOSE_PX;
+    const int64_t i = i0 + threadIdx.x;
+    if (i < n_px) {
+        const int y = (int)(i / W), x = (int)(i - (int64_t)y * W);
+        const int32_t l = lab[(size_t)(y + P) * pitch + x + P];
+        int32_t d = -1;
+        if (l >= 0) {
+            const int32_t dx = x - __ldg(&xs[l]), dy = y - __ldg(&ys[l]);
+            d = dx * dx + dy * dy;
+        }
+        stage[threadIdx.x * 3] = l;
+        stage[threadIdx.x * 3 + 1] = d;
+        stage[threadIdx.x * 3 + 2] = tgrid ? tgrid[i] : -1;
     }
-    int32_t* o = out + ((size_t)y * W + x) * 3;
-    o[0] = l;
-    o[1] = d;
-    o[2] = tgrid ? tgrid[(size_t)y * W + x] : -1;
+    __syncthreads();
+    const int64_t n_here = min((int64_t)COMPOSE_PX, n_px - i0) * 3;   // ints of this block's slice
+    int32_t* dst = out + i0 * 3;
+    if (vec && n_here == COMPOSE_PX * 3) {
+        if (threadIdx.x < COMPOSE_PX * 3 / 4)
+            reinterpret_cast<int4*>(dst)[threadIdx.x] = reinterpret_cast<const int4*>(stage)[threadIdx.x];
+    } else {
+        for (int k = threadIdx.x; k < n_here; k += COMPOSE_PX) dst[k] = stage[k];
+    }
+}
+
+// (a, b, c) of each (x, y, a, b, c) triangle row.
+__global__ void k_tri_vertices(const int32_t* __restrict__ tris, int64_t n, int32_t* __restrict__ verts)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * 3) return;
+    const int64_t t = i / 3;
+    verts[i] = tris[t * 5 + 2 + (i - t * 3)];
 }
 
 // GridTriangulation at P == 0 with the caller's grid: channels 0 and 1 are the
@@ -249,8 +275,9 @@ void compose_triangulation(Context& C, const Canvas& cv, int W, int H, int P, bo
     if (from_grid)
         k_compose3_from_grid<<<g, 256, 0, C.stream>>>(C.vgrid.as<int32_t>(), W, H, C.tgrid.as<int32_t>(), d_out);
     else
-        k_compose3<<<g, 256, 0, C.stream>>>(C.lab[0].as<int32_t>(), cv.pitch, P, W, H, C.xs.as<int32_t>(),
-                                            C.ys.as<int32_t>(), C.tgrid.as<int32_t>(), d_out);
+        k_compose3<<<(unsigned)ceil_div((int64_t)W * H, (int64_t)COMPOSE_PX), COMPOSE_PX, 0, C.stream>>>(
+            C.lab[0].as<int32_t>(), cv.pitch, P, W, (int64_t)W * H, C.xs.as<int32_t>(), C.ys.as<int32_t>(),
+            C.tgrid.as<int32_t>(), d_out, (reinterpret_cast<uintptr_t>(d_out) & 15) == 0);
     IDL_LAUNCH();
     C.mark(PM_COMPOSE);
     C.prof.valid = C.prof.enabled;
@@ -385,7 +412,8 @@ int idl_context_set_profiling(idl_context* ctx, int enable)
     IDL_API_END
 }
 
-int idl_context_pass_trace(idl_context* ctx, int64_t* ns_out, int32_t* tiles_out, int capacity, int* n_out)
+int idl_context_pass_trace(idl_context* ctx, int64_t* ns_out, int32_t* tiles_out, int32_t* steps_out, int capacity,
+                           int* n_out)
 {
     IDL_API_BEGIN
     if (!ctx || !n_out) invalid("arguments must not be NULL");
@@ -394,7 +422,17 @@ int idl_context_pass_trace(idl_context* ctx, int64_t* ns_out, int32_t* tiles_out
     for (int i = 0; i < capacity && i < (int)P.pass_ns.size(); ++i) {
         if (ns_out) ns_out[i] = P.pass_ns[i];
         if (tiles_out) tiles_out[i] = P.pass_tiles[i];
+        if (steps_out) steps_out[i] = i < (int)P.pass_steps.size() ? P.pass_steps[i] : 1;
     }
+    IDL_API_END
+}
+
+int idl_context_set_tail_rounds(idl_context* ctx, int max_list)
+{
+    IDL_API_BEGIN
+    if (!ctx) invalid("context must not be NULL");
+    if (max_list < 0) invalid("max_list must not be negative");
+    ctx->tail_rounds_below = max_list;
     IDL_API_END
 }
 
@@ -497,6 +535,26 @@ int idl_triangulate(idl_context* ctx, int width, int height, const int32_t* seed
     }
     IDL_CUDA(cudaStreamSynchronize(C.stream));
     if (n_triangles_out) *n_triangles_out = nt;
+    IDL_API_END
+}
+
+int idl_get_triangle_vertices(idl_context* ctx, int32_t* verts_out, int64_t capacity)
+{
+    IDL_API_BEGIN
+    if (!ctx) invalid("context must not be NULL");
+    if (!ctx->have_result) throw Error(IDL_ERR_STATE, "no triangulation result on this context");
+    if (capacity < ctx->last_n_tri) invalid("capacity is smaller than the triangle count");
+    if (ctx->last_n_tri == 0) return IDL_OK;
+    if (!verts_out) invalid("verts_out must not be NULL");
+    DeviceGuard g(ctx->device);
+    const int64_t n = ctx->last_n_tri;
+    ctx->verts.ensure((size_t)n * 3 * sizeof(int32_t));
+    k_tri_vertices<<<(unsigned)((n * 3 + 255) / 256), 256, 0, ctx->stream>>>(ctx->tris.as<int32_t>(), n,
+                                                                          ctx->verts.as<int32_t>());
+    IDL_LAUNCH();
+    IDL_CUDA(cudaMemcpyAsync(verts_out, ctx->verts.ptr, (size_t)n * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    IDL_CUDA(cudaStreamSynchronize(ctx->stream));
     IDL_API_END
 }
 

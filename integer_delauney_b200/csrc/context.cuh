@@ -127,6 +127,7 @@ struct Profile {
     // persistent sparse kernel: duration (ns) and work-list length of each pass
     std::vector<int64_t> pass_ns;
     std::vector<int32_t> pass_tiles;
+    std::vector<int32_t> pass_steps;   // passes each entry advanced (1, 0 entering the round mode, or a round's)
 };
 
 struct Context {
@@ -156,6 +157,10 @@ struct Context {
     int32_t stamp_epoch = 0;
     int dense_rounds = 3;  // propagation schedule from scratch (propagate.cu; idl_context_set_schedule)
     int key_tile = 9;      // tile shape of the owner-key tile round (propagate.cu; idl_context_set_tile)
+    // The persistent kernel advances several passes per grid barrier once its
+    // work list holds at most this many micro-tiles (sparse_jacobi.cu; 0:
+    // never; idl_context_set_tail_rounds).
+    int tail_rounds_below = 4096;
     // Whether the persistent tile shapes (key_tile >= 4) may run their rounds
     // as one device-filling cooperative launch (propagate.cu); off for
     // contexts whose work must overlap other streams' (a server's workers).
@@ -166,6 +171,7 @@ struct Context {
     DevBuf ukeys, uvals;  // compacted unique keys
     DevBuf cnt, off, fill, grp;  // group-by-smallest-vertex ranking
     DevBuf tris;          // n_tri x 5 int32 (x, y, a, b, c)
+    DevBuf verts;         // n_tri x 3 int32 (a, b, c) staged for idl_get_triangle_vertices
     int64_t hash_cap = 0;
 
     // assignment / output

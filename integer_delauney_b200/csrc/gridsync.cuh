@@ -24,6 +24,8 @@ struct GridSync {
     unsigned gen;
     int error;
     int passes;   // passes (or rounds) the kernel ran
+    int last1;    // sparse kernel's round mode: last pass that changed a cell, plus one (0: none)
+    int gens;     // sparse kernel: work-list generations it ran
 };
 
 __device__ __forceinline__ bool grid_sync(GridSync* gs, unsigned nblocks, unsigned& gen_local,

@@ -209,57 +209,253 @@ __device__ __forceinline__ void advance(const int (&ids)[GROUP], int cnt, const 
     }
 }
 
-// counts[t]: micro-tiles listed for pass t.  Pass t runs list t%2 and appends
-// pass t+1's micro-tiles to list (t+1)%2.
+// Appends `packed` (micro-tile index `target`) to the next work list when
+// `want` and its bit in `bout` was clear.  Warp-wide; staging as in advance.
+__device__ __forceinline__ void append_fresh(bool want, int target, int32_t packed, uint32_t* bout, int32_t* lout,
+                                             int32_t* count_out, Stage st, int lane)
+{
+    bool fresh = false;
+    if (want) {
+        const uint32_t bit = 1u << (target & 31);
+        fresh = !(atomicOr(&bout[target >> 5], bit) & bit);
+    }
+    const unsigned fb = __ballot_sync(FULL, fresh);
+    if (!fb) return;
+    const int m = __popc(fb);
+    int base = 0;
+    if (lane == 0) base = atomicAdd(st.n, m);
+    base = __shfl_sync(FULL, base, 0);
+    const int rank = __popc(fb & ((1u << lane) - 1u));
+    if (base + m <= STAGE) {
+        if (fresh) st.list[base + rank] = packed;
+    } else {
+        int gbase = 0;
+        if (lane == 0) {
+            atomicMin(st.cut, base);
+            gbase = atomicAdd(count_out, m);
+        }
+        gbase = __shfl_sync(FULL, gbase, 0);
+        if (fresh) lout[gbase + rank] = packed;
+    }
+}
+
+// Round mode.  Once the work list is short, the kernel advances RK passes per
+// grid barrier: a warp takes one micro-tile with an RK-cell halo (a 16 x 16
+// region; lane l holds region row l / 2, columns 8 (l % 2) .. + 7, in
+// registers) and runs RK Jacobi passes on it, neighbours by shuffles and
+// region cells beyond the canvas OUTSIDE.  Errors from the region's frozen
+// edge travel one cell per pass, so after RK passes the inner 8 x 8 cells are
+// exact (the light cone of the tile rounds); they go to the other plane.
+// Next list: the micro-tile itself if any inner cell changed in the round
+// (so that, rewritten next round, its planes agree again), and each
+// neighbour that an inner cell changed in the round's last pass can reach in
+// RK passes (the state one pass back is otherwise stable around it, so the
+// next RK passes cannot change it).  With RK = MT / 2 the reach of a cell is
+// its quadrant's side and corner neighbours.
+constexpr int RK = 4;
+constexpr int RR = MT + 2 * RK;
+static_assert(RR == 16 && MT == 8 && RK == MT / 2, "lane layout: 16 rows of two 8-cell halves");
+
+template <bool KEYS>
+__device__ __forceinline__ void round_mt(int32_t id, const int32_t* cur, int32_t* nxt, int pitch, int Wd, int Hd,
+                                         int mt_x, int mt_y, const uint32_t* __restrict__ pos, uint32_t* bin,
+                                         uint32_t* bout, int32_t* lout, int32_t* count_out, Stage st, int lane,
+                                         int pass0, int& last_pass)
+{
+    const int mx = id & 0xFFFF, my = id >> 16;
+    const int mt = my * mt_x + mx;
+    if (lane == 0) atomicAnd(&bin[mt >> 5], ~(1u << (mt & 31)));
+    const int r = lane >> 1, h = lane & 1;
+    const int gy = my * MT - RK + r;
+    const int gx0 = mx * MT - RK + 8 * h;
+    const bool row_in = gy >= 0 && gy < Hd;
+    int32_t c[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int gx = gx0 + j;
+        c[j] = (row_in && gx >= 0 && gx < Wd) ? __ldcg(cur + (size_t)gy * pitch + gx) : OUTSIDE;
+    }
+    // this lane's inner cells: region rows RK .. RK + MT - 1, columns RK .. RK + MT - 1
+    const bool inner_row = r >= RK && r < RK + MT;
+    // (registers are indexed statically: h picks c[0..3] or c[4..7])
+    int32_t c0[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) c0[q] = h ? c[q] : c[4 + q];
+    int last = -1;
+    bool ch = false;   // an inner cell of this lane changed in the latest pass
+#pragma unroll 1
+    for (int p = 0; p < RK; ++p) {
+        const int32_t lft = __shfl_up_sync(FULL, c[7], 1), rgt = __shfl_down_sync(FULL, c[0], 1);
+        int32_t nv[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int32_t up = __shfl_up_sync(FULL, c[j], 2), dn = __shfl_down_sync(FULL, c[j], 2);
+            const int32_t L = j > 0 ? c[j - 1] : (h ? lft : OUTSIDE);
+            const int32_t R = j < 7 ? c[j + 1] : (h ? OUTSIDE : rgt);
+            const int32_t U = r > 0 ? up : OUTSIDE;
+            const int32_t D = r < RR - 1 ? dn : OUTSIDE;
+            int32_t b = c[j];
+            if (KEYS) {
+                int32_t k = b;
+                best_of4_keys(k, L, R, U, D, gx0 + j, gy);
+                b = b >= UNDEF ? k : b;
+            } else if (b >= UNDEF && (L != b || R != b || U != b || D != b)) {
+                best_of4(b, L, R, U, D, gx0 + j, gy, pos);
+            }
+            nv[j] = b;
+        }
+        ch = false;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ch = ch || (h ? nv[q] != c[q] : nv[4 + q] != c[4 + q]);
+        ch = ch && inner_row;
+        if (__any_sync(FULL, ch)) last = p;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) c[j] = nv[j];
+    }
+    if (inner_row && gy < Hd) {
+        const int gxi = mx * MT + 4 * h;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (gxi + q < Wd) nxt[(size_t)gy * pitch + gxi + q] = h ? c[q] : c[4 + q];
+    }
+    bool moved = false;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) moved = moved || (h ? c[q] : c[4 + q]) != c0[q];
+    if (!__any_sync(FULL, moved && inner_row)) return;
+    last_pass = max(last_pass, pass0 + last);
+    // quadrants of the inner tile with a change in the last pass: lanes 8..15
+    // hold its top half, 16..23 the bottom; even lanes the left half
+    const unsigned lb = __ballot_sync(FULL, ch);   // ch: changes of the last pass
+    const bool tl = lb & 0x00005500u, tr = lb & 0x0000AA00u, bl = lb & 0x00550000u, br = lb & 0x00AA0000u;
+    int dx = 0, dy = 0;
+    bool want = false;
+    switch (lane) {
+    case 0: want = true; break;
+    case 1: dx = -1; want = tl || bl; break;
+    case 2: dx = 1; want = tr || br; break;
+    case 3: dy = -1; want = tl || tr; break;
+    case 4: dy = 1; want = bl || br; break;
+    case 5: dx = -1; dy = -1; want = tl; break;
+    case 6: dx = 1; dy = -1; want = tr; break;
+    case 7: dx = -1; dy = 1; want = bl; break;
+    case 8: dx = 1; dy = 1; want = br; break;
+    default: break;
+    }
+    const int nx = mx + dx, ny = my + dy;
+    want = want && nx >= 0 && nx < mt_x && ny >= 0 && ny < mt_y;
+    append_fresh(want, ny * mt_x + nx, pack_mt(nx, ny), bout, lout, count_out, st, lane);
+}
+
+// Entering the round mode: the list holds the micro-tiles that can change in
+// the next pass; a round needs those that can change in the next RK passes,
+// which lie within one micro-tile of them (RK <= MT).  Warp-wide per entry.
+__device__ __forceinline__ void dilate_mt(int32_t id, int mt_x, int mt_y, uint32_t* bin, uint32_t* bout,
+                                          int32_t* lout, int32_t* count_out, Stage st, int lane)
+{
+    const int mx = id & 0xFFFF, my = id >> 16;
+    const int mt = my * mt_x + mx;
+    if (lane == 0) atomicAnd(&bin[mt >> 5], ~(1u << (mt & 31)));
+    const int nx = mx + (lane % 3) - 1, ny = my + (lane / 3) - 1;
+    const bool want = lane < 9 && nx >= 0 && nx < mt_x && ny >= 0 && ny < mt_y;
+    append_fresh(want, ny * mt_x + nx, pack_mt(nx, ny), bout, lout, count_out, st, lane);
+}
+
+// counts[g]: micro-tiles listed for work-list generation g, which runs list
+// g%2 and appends generation g+1's micro-tiles to list (g+1)%2.  A generation
+// is one pass while the list is longer than rounds_below, then (once) the
+// dilation into the round mode, then rounds of RK passes.  The mode is the
+// same in every block: it depends only on the list lengths all of them read.
 template <bool KEYS>
 __global__ void __launch_bounds__(SJ_THREADS, 1)
 k_sparse_jacobi(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, const uint32_t* __restrict__ pos,
                 uint32_t* bits0, uint32_t* bits1, int32_t* list0, int32_t* list1, int32_t* counts, int max_steps,
-                int mt_x, int mt_y, GridSync* gs, unsigned long long* trace)
+                int mt_x, int mt_y, int rounds_below, GridSync* gs, unsigned long long* trace)
 {
-    // trace (profiling only): the global timer at the start and after each pass
+    // trace (profiling only): the global timer at the start and after each
+    // generation, and from trace[max_steps + 2] on the passes each advanced
     if (trace && blockIdx.x == 0 && threadIdx.x == 0) trace[0] = global_timer_ns();
     __shared__ int32_t s_list[STAGE];
-    __shared__ int s_n, s_cut, s_base, s_m;
+    __shared__ int s_n, s_cut, s_base, s_m, s_last;
     const int lane = threadIdx.x & 31;
     const int gwarp = blockIdx.x * SJ_WARPS + (threadIdx.x >> 5);
     const int nwarps = gridDim.x * SJ_WARPS;
     unsigned gen_local = 0;
-    int t = 0;
-    for (; t < max_steps; ++t) {
-        const int n = *reinterpret_cast<volatile int32_t*>(&counts[t]);
-        if (n == 0) break;
+    int t = 0;              // passes done
+    int g = 0;              // generation
+    int par = 0;            // plane holding the current state
+    bool rounds = false;
+    bool converged = false;
+    for (; t < max_steps; ++g) {
+        const int n = *reinterpret_cast<volatile int32_t*>(&counts[g]);
+        if (n == 0) {
+            converged = true;
+            break;
+        }
+        int kind = 0;   // 0: one pass, 1: dilation into the round mode, 2: a round of RK passes
+        if (rounds) {
+            kind = 2;
+        } else if (n <= rounds_below) {
+            kind = 1;
+            rounds = true;
+        }
         if (threadIdx.x == 0) {
             s_n = 0;
             s_cut = STAGE;
+            s_last = -1;
         }
         __syncthreads();
-        const int32_t* cur = (t & 1) ? plane1 : plane0;
-        int32_t* nxt = (t & 1) ? plane0 : plane1;
-        uint32_t* bin = (t & 1) ? bits1 : bits0;
-        uint32_t* bout = (t & 1) ? bits0 : bits1;
-        const int32_t* lin = (t & 1) ? list1 : list0;
-        int32_t* lout = (t & 1) ? list0 : list1;
-        for (int i0 = gwarp * GROUP; i0 < n; i0 += nwarps * GROUP) {
-            int ids[GROUP];
-            const int cnt = min(GROUP, n - i0);
+        const int32_t* cur = par ? plane1 : plane0;
+        int32_t* nxt = par ? plane0 : plane1;
+        uint32_t* bin = (g & 1) ? bits1 : bits0;
+        uint32_t* bout = (g & 1) ? bits0 : bits1;
+        const int32_t* lin = (g & 1) ? list1 : list0;
+        int32_t* lout = (g & 1) ? list0 : list1;
+        const Stage stg{s_list, &s_n, &s_cut};
+        if (kind == 0) {
+            for (int i0 = gwarp * GROUP; i0 < n; i0 += nwarps * GROUP) {
+                int ids[GROUP];
+                const int cnt = min(GROUP, n - i0);
 #pragma unroll
-            for (int k = 0; k < GROUP; ++k) ids[k] = k < cnt ? __ldcg(&lin[i0 + k]) : 0;
-            advance<KEYS>(ids, cnt, cur, nxt, pitch, Wd, Hd, mt_x, mt_y, pos, bin, bout, lout, counts + t + 1,
-                          Stage{s_list, &s_n, &s_cut}, lane);
+                for (int k = 0; k < GROUP; ++k) ids[k] = k < cnt ? __ldcg(&lin[i0 + k]) : 0;
+                advance<KEYS>(ids, cnt, cur, nxt, pitch, Wd, Hd, mt_x, mt_y, pos, bin, bout, lout, counts + g + 1,
+                              stg, lane);
+            }
+        } else if (kind == 1) {
+            // the list was made by changes of pass t - 1 (none if t == 0)
+            if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&gs->last1, t);
+            for (int i = gwarp; i < n; i += nwarps)
+                dilate_mt(__ldcg(&lin[i]), mt_x, mt_y, bin, bout, lout, counts + g + 1, stg, lane);
+        } else {
+            int last = -1;
+            for (int i = gwarp; i < n; i += nwarps)
+                round_mt<KEYS>(__ldcg(&lin[i]), cur, nxt, pitch, Wd, Hd, mt_x, mt_y, pos, bin, bout, lout,
+                               counts + g + 1, stg, lane, t, last);
+            if (lane == 0 && last >= 0) atomicMax(&s_last, last);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
             const int m = min(s_n, s_cut);
             s_m = m;
-            s_base = m ? atomicAdd(&counts[t + 1], m) : 0;
+            s_base = m ? atomicAdd(&counts[g + 1], m) : 0;
+            if (s_last >= 0) atomicMax(&gs->last1, s_last + 1);
         }
         __syncthreads();
         for (int i = threadIdx.x; i < s_m; i += blockDim.x) lout[s_base + i] = s_list[i];
+        const int advanced = kind == 0 ? 1 : (kind == 2 ? RK : 0);
+        t += advanced;
+        if (advanced) par ^= 1;
         if (!grid_sync(gs, gridDim.x, gen_local)) return;
-        if (trace && blockIdx.x == 0 && threadIdx.x == 0) trace[t + 1] = global_timer_ns();
+        if (trace && blockIdx.x == 0 && threadIdx.x == 0) {
+            trace[g + 1] = global_timer_ns();
+            trace[max_steps + 2 + g] = (unsigned long long)advanced;
+        }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) gs->passes = t;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        // the pass count of the one-pass schedule: the first pass whose list
+        // would be empty (last change + 2, or 1 if nothing ever changed)
+        gs->passes = !converged ? max_steps : (rounds ? atomicAdd(&gs->last1, 0) + 1 : t);
+        gs->gens = g;
+    }
 }
 
 // The barrier above on its own: `rounds` barriers of a grid that waits for
@@ -448,12 +644,14 @@ int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos,
     int32_t* p1 = C.lab[1].as<int32_t>();
     GridSync* gs = C.gsync.as<GridSync>();
     int pitch = cv.pitch, Wd = cv.Wd, Hd = cv.Hd, ms = max_steps, mx = mt_x, my = mt_y;
+    int rb = std::max(C.tail_rounds_below, 0);
     unsigned long long* trace = nullptr;
     if (C.prof.enabled) {
-        C.trace.ensure(((size_t)max_steps + 2) * 8);
+        C.trace.ensure(((size_t)max_steps + 2) * 2 * 8);   // timestamps, then passes per generation
         trace = C.trace.as<unsigned long long>();
     }
-    void* args[] = {&p0, &p1, &pitch, &Wd, &Hd, (void*)&pos, &b0, &b1, &l0, &l1, &counts, &ms, &mx, &my, &gs, &trace};
+    void* args[] = {&p0, &p1, &pitch, &Wd, &Hd, (void*)&pos, &b0, &b1, &l0, &l1, &counts, &ms, &mx, &my, &rb, &gs,
+                    &trace};
     GridSync h{};
     {
         // One persistent grid per device at a time: the kernel fills every SM,
@@ -470,23 +668,30 @@ int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos,
     const int64_t passes = h.passes;
     if (passes >= max_steps) throw Error(IDL_ERR_INTERNAL, "Voronoi propagation did not converge");
     if (C.prof.enabled) {
-        std::vector<int32_t> hc((size_t)passes + 1);
+        const int gens = h.gens;
+        std::vector<int32_t> hc((size_t)gens + 1);
         IDL_CUDA(cudaMemcpy(hc.data(), counts, hc.size() * 4, cudaMemcpyDeviceToHost));
-        std::vector<unsigned long long> ht((size_t)passes + 1);
+        std::vector<unsigned long long> ht((size_t)gens + 1), hs((size_t)std::max(gens, 1));
         IDL_CUDA(cudaMemcpy(ht.data(), trace, ht.size() * 8, cudaMemcpyDeviceToHost));
+        if (gens > 0)
+            IDL_CUDA(cudaMemcpy(hs.data(), trace + max_steps + 2, (size_t)gens * 8, cudaMemcpyDeviceToHost));
         C.prof.pass_ns.clear();
         C.prof.pass_tiles.clear();
-        for (int64_t i = 0; i < passes; ++i) {
+        C.prof.pass_steps.clear();
+        int64_t tiles = 0;
+        double bytes = 0;
+        for (int i = 0; i < gens; ++i) {
             C.prof.pass_ns.push_back((int64_t)(ht[i + 1] - ht[i]));
             C.prof.pass_tiles.push_back(hc[i]);
+            C.prof.pass_steps.push_back((int32_t)hs[i]);
+            tiles += (int64_t)hc[i] * (int64_t)hs[i];
+            bytes += (double)hc[i] * (double)hs[i] * MT * MT * 8.0;   // label in, label out per cell-pass
         }
-        int64_t tiles = 0;
-        for (int32_t c : hc) tiles += c;
         // accumulated: a hybrid run has counted its tile rounds already
         C.prof.tiles += tiles;
-        C.prof.rounds += passes;
+        C.prof.rounds += gens;
         C.prof.passes = passes;
-        C.prof.prop_bytes += (double)tiles * MT * MT * 8.0;   // label in, label out per cell
+        C.prof.prop_bytes += bytes;
         C.prof.tile_w = MT;
         C.prof.tile_h = MT;
         C.prof.steps_per_round = 1;

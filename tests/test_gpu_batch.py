@@ -315,3 +315,67 @@ def test_exact_mode_at_scale(kind):
     tm, grid = cu.triangulate(W, H, seeds, 16, voronoi_mode="exact")
     np.testing.assert_array_equal(grid, o_grid)
     np.testing.assert_array_equal(_tris_array(tm), o_tris)
+
+
+def test_triangulate_device_equals_host_call_at_any_alignment():
+    """idl_triangulate_device writes the same (H, W, 3) grid as the host call,
+    whether the output pointer is 16-byte aligned (vector stores) or not, and
+    nothing outside it."""
+    import torch
+
+    from integer_delauney_b200 import _capi
+    W, H = 301, 77
+    seeds = random_seeds(W, H, 500, 9)
+    verts, grid = cu.triangulate(W, H, seeds, 16, as_arrays=True)
+    tmap, grid_m = cu.triangulate(W, H, seeds, 16)
+    # as_arrays' vertex triples (packed on the device) are the map's rows' ids
+    np.testing.assert_array_equal(verts, np.array([tmap[t][2:5] for t in range(len(tmap))], dtype=np.int32))
+    np.testing.assert_array_equal(grid, grid_m)
+    lib = _capi.load()
+    ctx = _capi.context_for(torch.cuda.current_device())
+    ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+    d_seeds = torch.from_numpy(np.ascontiguousarray(seeds, dtype=np.int32)).cuda()
+    n = H * W * 3
+    for off in (0, 1, 2, 3):
+        buf = torch.full((n + 8,), -7, dtype=torch.int32, device="cuda")
+        view = buf[off:off + n]
+        _capi.check(lib.idl_triangulate_device(ctx.handle, W, H, d_seeds.data_ptr(), len(seeds), 16,
+                                               _capi.MODE_REFERENCE, view.data_ptr(), None))
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(view.cpu().numpy().reshape(H, W, 3), grid, err_msg=f"offset {off}")
+        assert bool((buf[:off] == -7).all()) and bool((buf[off + n:] == -7).all())
+
+
+@pytest.mark.parametrize("kind", ["uniform", "clustered"])
+def test_tail_rounds_agree(kind):
+    """The persistent kernel's round mode (several Jacobi passes per grid
+    barrier once its work list is short) gives the one-pass schedule's fixed
+    point and pass count bit for bit: never, late, by default and from the
+    first pass, from scratch and after tile rounds."""
+    from integer_delauney_b200 import _capi
+    W, H, P = 600, 420, 16
+    seeds = random_seeds(W, H, 2500, 33) if kind == "uniform" else clustered_seeds(W, H, 2500, 33, blobs=4,
+                                                                                     sigma=14.0)
+    s = oracle.sort_seeds(seeds, W, H)
+    o_tris, o_grid, _ = oracle.triangulate(W, H, s, P)
+    _, o_passes = oracle.voronoi("reference", W + 2 * P, H + 2 * P, s + P)
+    ctx = _capi.context_for(0)
+    try:
+        for sched, shape in ((0, 0), (3, 9), (1, 2)):
+            ctx.set_schedule(sched)
+            ctx.set_tile(shape)
+            for rb in (0, 16, 4096, 1 << 30):
+                ctx.set_tail_rounds(rb)
+                ctx.set_profiling(True)
+                tm, grid = cu.triangulate(W, H, seeds, P)
+                passes = int(ctx.last_profile()["passes"])
+                ctx.set_profiling(False)
+                msg = f"schedule {sched}, tile {shape}, tail rounds below {rb}"
+                np.testing.assert_array_equal(grid, o_grid, err_msg=msg)
+                np.testing.assert_array_equal(_tris_array(tm), o_tris, err_msg=msg)
+                assert passes == o_passes, msg
+    finally:
+        ctx.set_profiling(False)
+        ctx.set_tail_rounds(4096)   # the context defaults
+        ctx.set_schedule(3)
+        ctx.set_tile(9)
