@@ -24,9 +24,9 @@ namespace idl {
 // pairwise in log2(HULL_THREADS) levels, each merge finding the lower common
 // tangent of two x-separated hulls by the standard two-sided walk.  A merged hull is a
 // prefix of the left one and a suffix of the right one, so it is kept as
-// linked chunk ranges, not copied.  The final hull is flattened and each cell
-// finds its vertex (a binary search for the thread's first cell, then a walk
-// as t grows).  Convex hull merging: Preparata & Hong (1977).
+// linked chunk ranges, not copied.  The final hull is flattened; each thread
+// finds the vertex of the first cell of its chunk by binary search and walks
+// the hull across the chunk, so the whole row costs O(W + H).  Convex hull merging: Preparata & Hong (1977).
 constexpr int HULL_THREADS = 128;              // threads (= chunks) per row
 constexpr int32_t HULL_ABSENT = 0x7FFFFFFF;    // a column with no seed (real F < 2^31 - 1)
 constexpr int HULL_MAX_W = 28000;              // F and two int16 index rows fit shared memory
@@ -37,6 +37,29 @@ inline size_t row_hull_smem(int W) { return (size_t)W * 4 + (size_t)((W + 1) & ~
 __device__ __forceinline__ long long hull_cross(int xa, int32_t fa, int xb, int32_t fb, int xc, int32_t fc)
 {
     return (long long)(xb - xa) * (long long)(fc - fb) - (long long)(fb - fa) * (long long)(xc - xb);
+}
+
+// Exclusive prefix over the block's threads in thread order: the sum of the
+// values of the threads before this one, or (max_op) their maximum (-1 for
+// the first).  tmp: shared scratch of T / 32 + 1 ints.  Ends with a barrier.
+template <int T>
+__device__ __forceinline__ int block_excl_scan(int v, bool max_op, int* tmp)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if (lane >= o) inc = max_op ? max(inc, u) : inc + u;
+    }
+    if (lane == 31) tmp[warp] = inc;
+    __syncthreads();
+    int pre = max_op ? -1 : 0;
+    for (int w = 0; w < warp; ++w) pre = max_op ? max(pre, tmp[w]) : pre + tmp[w];
+    int excl = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
+    if (lane == 0) excl = max_op ? -1 : 0;
+    __syncthreads();   // tmp may be reused by the next scan
+    return max_op ? max(pre, excl) : pre + excl;
 }
 
 // One row of Wd columns: lrow / drow hold each column's candidate label
@@ -51,8 +74,8 @@ __device__ __forceinline__ void row_hull(const int32_t* __restrict__ lrow, const
     int16_t* hx = reinterpret_cast<int16_t*>(F + Wd);                // chunk hulls, each in its chunk's slots
     int16_t* flat = hx + ((Wd + 1) & ~1);                            // the final hull, in x order
     constexpr int T = HULL_THREADS;
-    __shared__ int cb[T], ce[T], cprev[T], cnext[T], gfirst[T], glast[T], coff[T];
-    __shared__ int n_hull;
+    __shared__ int cb[T], ce[T], cprev[T], cnext[T], gfirst[T], glast[T];
+    __shared__ int n_hull, scan_tmp[T / 32 + 1];
     const int tid = threadIdx.x;
     for (int x = tid; x < Wd; x += T) {
         const int32_t l = lrow[x];
@@ -64,22 +87,31 @@ __device__ __forceinline__ void row_hull(const int32_t* __restrict__ lrow, const
     // chunk hulls; an odd chunk length keeps the threads' F reads on distinct banks
     const int C = ((Wd + T - 1) / T) | 1;
     const int x0 = tid * C, x1 = min(Wd, x0 + C);
-    int h = x0;   // the chunk's hull occupies hx[x0, h)
+    int h = x0;   // the chunk's hull occupies hx[x0, h); its top two points also in registers
+    int x1t = 0, x2t = 0;
+    int32_t f1t = 0, f2t = 0;
     for (int x = x0; x < x1; ++x) {
         const int32_t f = F[x];
         if (f == HULL_ABSENT) continue;
-        while (h - x0 >= 2) {
-            const int xa = hx[h - 2], xb = hx[h - 1];
-            if (hull_cross(xa, F[xa], xb, F[xb], x, f) > 0) break;
+        while (h - x0 >= 2 && hull_cross(x2t, f2t, x1t, f1t, x, f) <= 0) {
             --h;
+            x1t = x2t;
+            f1t = f2t;
+            if (h - x0 >= 2) {
+                x2t = hx[h - 2];
+                f2t = F[x2t];
+            }
         }
         hx[h++] = (int16_t)x;
+        x2t = x1t;
+        f2t = f1t;
+        x1t = x;
+        f1t = f;
     }
     cb[tid] = x0;
     ce[tid] = h;
     cprev[tid] = cnext[tid] = -1;
     gfirst[tid] = glast[tid] = h > x0 ? tid : -1;
-    coff[tid] = -1;
     __syncthreads();
 
     // merge groups of s chunks pairwise; a group's state lives at its first chunk
@@ -136,50 +168,61 @@ __device__ __forceinline__ void row_hull(const int32_t* __restrict__ lrow, const
                 cnext[pc] = qc;
                 cprev[qc] = pc;
                 glast[L] = rl;
+                // chunks the bridge passes over leave the hull: empty them, so
+                // that the final hull is every non-empty chunk in index order
+                for (int c = pc + 1; c < R; ++c) ce[c] = cb[c];
+                for (int c = R; c < qc; ++c) ce[c] = cb[c];
             }
         }
         __syncthreads();
     }
 
-    // flatten: chunk offsets along the final chain, then each chunk copies its range
-    if (tid == 0) {
-        int k = 0;
-        for (int c = gfirst[0]; c >= 0; c = cnext[c]) {
-            coff[c] = k;
-            k += ce[c] - cb[c];
-            if (c == glast[0]) break;
-        }
-        n_hull = k;
-    }
+    // flatten: offsets of the non-empty chunks by a block-wide scan
+    const int kept = ce[tid] - cb[tid];
+    const int off = block_excl_scan<T>(kept, false, scan_tmp);
+    if (tid == T - 1) n_hull = off + kept;
+    for (int i = cb[tid]; i < ce[tid]; ++i) flat[off + i - cb[tid]] = hx[i];
     __syncthreads();
-    if (coff[tid] >= 0)
-        for (int i = cb[tid]; i < ce[tid]; ++i) flat[coff[tid] + i - cb[tid]] = hx[i];
-    __syncthreads();
-
     const int H = n_hull;
     if (H == 0) {
         for (int t = tid; t < Wd; t += T) out[t] = UNDEF;
         return;
     }
-    // vertex k >= 1 wins at t (ties included) iff F_k - F_{k-1} <= t * 2 (x_k - x_{k-1})
-    auto wins = [&](int k, int t) {
+    // Vertex k owns the cells [S_k, S_k+1): S_0 = 0, S_H = Wd, and for k >= 1
+    // S_k = ceil((F_k - F_{k-1}) / (2 (x_k - x_{k-1}))) clamped to [0, Wd],
+    // non-decreasing along the hull.  Each vertex with a non-empty range marks
+    // its first cell (hx, free now, holds the marks), and a max-scan over the
+    // row carries the mark forward: cell t's winner is the last mark at or
+    // before t.
+    auto start = [&](int k) {
+        if (k <= 0) return 0;
+        if (k >= H) return Wd;
         const int xa = flat[k - 1], xb = flat[k];
-        return (long long)(F[xb] - F[xa]) <= (long long)t * (2 * (xb - xa));
+        const int32_t num = F[xb] - F[xa];
+        if (num <= 0) return 0;
+        const uint32_t den = 2u * (uint32_t)(xb - xa);
+        const uint32_t q = ((uint32_t)num + den - 1u) / den;
+        return q >= (uint32_t)Wd ? Wd : (int)q;
     };
-    int k = 0;
-    {
-        int lo = 0, hi = H - 1;   // the last vertex that wins at the thread's first cell
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (wins(mid, tid)) lo = mid;
-            else hi = mid - 1;
-        }
-        k = lo;
+    for (int t = tid; t < Wd; t += T) hx[t] = -1;
+    __syncthreads();
+    for (int k = tid; k < H; k += T) {
+        const int s0 = start(k);
+        if (s0 < Wd && start(k + 1) > s0) hx[s0] = (int16_t)k;
     }
-    for (int t = tid; t < Wd; t += T) {
-        while (k + 1 < H && wins(k + 1, t)) ++k;
-        out[t] = lrow[flat[k]];
+    __syncthreads();
+    int last = -1;
+    for (int t = x0; t < x1; ++t)
+        if (hx[t] >= 0) last = hx[t];
+    const int carry = block_excl_scan<T>(last, true, scan_tmp);
+    int run = carry;
+    for (int t = x0; t < x1; ++t) {
+        if (hx[t] >= 0) run = hx[t];
+        else hx[t] = (int16_t)run;
     }
+    __syncthreads();
+#pragma unroll 4
+    for (int t = tid; t < Wd; t += T) out[t] = lrow[flat[hx[t]]];
 }
 
 }  // namespace idl

@@ -377,7 +377,9 @@ k_sparse_jacobi(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, con
     __shared__ int32_t s_list[STAGE];
     __shared__ int s_n, s_cut, s_base, s_m, s_last;
     const int lane = threadIdx.x & 31;
-    const int gwarp = blockIdx.x * SJ_WARPS + (threadIdx.x >> 5);
+    // warp slots numbered across the blocks first, so that a short list
+    // spreads over every SM instead of filling the first blocks' warps
+    const int gwarp = (threadIdx.x >> 5) * gridDim.x + blockIdx.x;
     const int nwarps = gridDim.x * SJ_WARPS;
     unsigned gen_local = 0;
     int t = 0;              // passes done

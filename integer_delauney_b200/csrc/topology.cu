@@ -200,33 +200,59 @@ k_detect(const int32_t* __restrict__ lab, int pitch, int Wd, int Hd, const uint3
     if (k1 != EMPTY_KEY && (first || (k1 != l0 && k1 != l1))) hash_insert(k1, (blk << 4) | code1, table, mask, sc);
 }
 
-// Warp-aggregated append: one atomic per warp.
-__device__ __forceinline__ long long warp_append(bool pred, unsigned long long* counter)
-{
-    const unsigned ballot = __ballot_sync(0xffffffffu, pred);
-    if (!ballot) return -1;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(ballot) - 1;
-    unsigned long long base = 0;
-    if (lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(ballot));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    return pred ? (long long)(base + __popc(ballot & ((1u << lane) - 1u))) : -1;
-}
 
-__global__ void k_enumerate(const unsigned long long* __restrict__ table, long long cap, unsigned long long* __restrict__ ukeys,
-                            unsigned long long* __restrict__ uvals, int32_t* __restrict__ cnt,
-                            Scalars* __restrict__ sc)
+// Compaction of the occupied slots with one atomic per block on the row
+// counter (one per warp, 65 k of them on a 2 M-slot table, serialised on that
+// one address): a block counts the occupied slots of its contiguous span,
+// reserves that many rows, and writes them in slot order, the second read of
+// the span coming from L2.  Row order is free: k_rank numbers the triangles
+// canonically.
+constexpr int ENUM_THREADS = 256;
+
+__global__ void __launch_bounds__(ENUM_THREADS)
+k_enumerate(const unsigned long long* __restrict__ table, long long cap, unsigned long long* __restrict__ ukeys,
+            unsigned long long* __restrict__ uvals, int32_t* __restrict__ cnt, Scalars* __restrict__ sc)
 {
-    for (long long s0 = (long long)blockIdx.x * blockDim.x; s0 < cap; s0 += (long long)gridDim.x * blockDim.x) {
+    constexpr int NW = ENUM_THREADS / 32;
+    __shared__ int warp_cnt[NW];
+    __shared__ unsigned long long s_base;
+    const long long span = ((cap + gridDim.x - 1) / gridDim.x + ENUM_THREADS - 1) / ENUM_THREADS * ENUM_THREADS;
+    const long long b0 = (long long)blockIdx.x * span, b1 = min(cap, b0 + span);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned mine = 0;
+    for (long long s = b0 + threadIdx.x; s < b1; s += ENUM_THREADS) mine += table[2 * s] != EMPTY_KEY;
+    mine = __reduce_add_sync(0xffffffffu, mine);
+    if (lane == 0) warp_cnt[warp] = (int)mine;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long total = 0;
+        for (int w = 0; w < NW; ++w) total += (unsigned)warp_cnt[w];
+        s_base = total ? atomicAdd(reinterpret_cast<unsigned long long*>(&sc->n_triangles), total) : 0ull;
+    }
+    __syncthreads();
+    unsigned long long base = s_base;
+    for (long long s0 = b0; s0 < b1; s0 += ENUM_THREADS) {
         const long long s = s0 + threadIdx.x;
-        const unsigned long long k = s < cap ? table[2 * s] : EMPTY_KEY;
+        const unsigned long long k = s < b1 ? table[2 * s] : EMPTY_KEY;
         const bool occ = k != EMPTY_KEY;
-        const long long u = warp_append(occ, reinterpret_cast<unsigned long long*>(&sc->n_triangles));
+        const unsigned ballot = __ballot_sync(0xffffffffu, occ);
+        if (lane == 0) warp_cnt[warp] = __popc(ballot);
+        __syncthreads();
+        int before = 0, all = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            const int c = warp_cnt[w];
+            before += w < warp ? c : 0;
+            all += c;
+        }
         if (occ) {
+            const unsigned long long u = base + before + __popc(ballot & ((1u << lane) - 1u));
             ukeys[u] = k;
             uvals[u] = table[2 * s + 1];
             atomicAdd(&cnt[(int)(k >> 42)], 1);
         }
+        base += all;
+        __syncthreads();   // warp_cnt is rewritten next iteration
     }
 }
 
@@ -277,7 +303,7 @@ void detect_triangles(Context& C, const Canvas& cv, const int32_t* labels, const
     // Unique triangles of a planar triangulation number under 2n; the table
     // starts at four times that, and on the rare probe overflow it grows and
     // the detection is redone.  The occupied slots are counted while they are
-    // compacted (one atomic per warp), not while they are inserted, where a
+    // compacted (one atomic per block), not while they are inserted, where a
     // single counter would serialise every new key.
     int64_t cap = std::max<int64_t>(next_pow2(8 * n + 1024), C.hash_cap);
     C.cnt.ensure((size_t)(n + 1) * 4);
@@ -300,7 +326,7 @@ void detect_triangles(Context& C, const Canvas& cv, const int32_t* labels, const
         if (mid) IDL_CUDA(cudaEventRecord(mid, C.stream));
         C.mark(PM_DETECT);
         const int g1 = (int)std::min<int64_t>(ceil_div(cap, 256), C.num_sms * 16);
-        k_enumerate<<<g1, 256, 0, C.stream>>>(C.hkeys.as<unsigned long long>(), cap,
+        k_enumerate<<<g1, ENUM_THREADS, 0, C.stream>>>(C.hkeys.as<unsigned long long>(), cap,
                                               C.ukeys.as<unsigned long long>(),
                                               C.uvals.as<unsigned long long>(), C.cnt.as<int32_t>(), C.sc());
         IDL_LAUNCH();
