@@ -803,13 +803,22 @@ __global__ void k_copy_tiles(const int32_t* __restrict__ src, int32_t* __restric
                              const int32_t* __restrict__ list, const int32_t* __restrict__ count, int tiles_x, int tw,
                              int th)
 {
+    // tiles start at multiples of tw (a multiple of 8) on 32-aligned rows, so
+    // whole 4-cell groups are 16-byte aligned; the canvas edge goes cell by cell
     const int n_items = *count;
+    const int groups = tw / 4;
     for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
         const int t = list[item];
         const int x0 = (t % tiles_x) * tw, y0 = (t / tiles_x) * th;
-        for (int i = threadIdx.x; i < tw * th; i += blockDim.x) {
-            const int x = x0 + i % tw, y = y0 + i / tw;
-            if (x < Wd && y < Hd) dst[(size_t)y * pitch + x] = src[(size_t)y * pitch + x];
+        for (int i = threadIdx.x; i < groups * th; i += blockDim.x) {
+            const int gy = y0 + i / groups, gx = x0 + (i % groups) * 4;
+            if (gy >= Hd) continue;
+            const size_t o = (size_t)gy * pitch + gx;
+            if (gx + 4 <= Wd) {
+                *reinterpret_cast<int4*>(dst + o) = *reinterpret_cast<const int4*>(src + o);
+            } else {
+                for (int k = 0; k < 4 && gx + k < Wd; ++k) dst[o + k] = src[o + k];
+            }
         }
     }
 }

@@ -125,6 +125,8 @@ __device__ __forceinline__ void row_hull(const int32_t* __restrict__ lrow, const
             } else if (rf >= 0) {
                 int pc = ll, pi = ce[ll] - 1;   // p: the left hull's last point
                 int qc = rf, qi = cb[rf];       // q: the right hull's first point
+                int xp = hx[pi], xq = hx[qi];   // and their points, kept in registers
+                int32_t fp = F[xp], fq = F[xq];
                 for (;;) {
                     bool moved = false;
                     for (;;) {   // p leftwards while its predecessor does not turn left onto q
@@ -138,10 +140,13 @@ __device__ __forceinline__ void row_hull(const int32_t* __restrict__ lrow, const
                         } else {
                             break;
                         }
-                        const int xa = hx[ai], xp = hx[pi], xq = hx[qi];
-                        if (hull_cross(xa, F[xa], xp, F[xp], xq, F[xq]) > 0) break;
+                        const int xa = hx[ai];
+                        const int32_t fa = F[xa];
+                        if (hull_cross(xa, fa, xp, fp, xq, fq) > 0) break;
                         pc = ac;
                         pi = ai;
+                        xp = xa;
+                        fp = fa;
                         moved = true;
                     }
                     for (;;) {   // q rightwards while p, q and its successor do not turn left
@@ -155,10 +160,13 @@ __device__ __forceinline__ void row_hull(const int32_t* __restrict__ lrow, const
                         } else {
                             break;
                         }
-                        const int xp = hx[pi], xq = hx[qi], xb = hx[bi];
-                        if (hull_cross(xp, F[xp], xq, F[xq], xb, F[xb]) > 0) break;
+                        const int xb = hx[bi];
+                        const int32_t fb = F[xb];
+                        if (hull_cross(xp, fp, xq, fq, xb, fb) > 0) break;
                         qc = bc;
                         qi = bi;
+                        xq = xb;
+                        fq = fb;
                         moved = true;
                     }
                     if (!moved) break;
