@@ -659,9 +659,10 @@ def run_ours(args, rank, world):
     ctx.set_stream(stream.cuda_stream)
     # headline: K plain steps; the per-stage events are recorded in a second
     # timed run, since profiling reads counters back between stages
-    ms, _, clocks, launches = time_device(seeds_u, args.steps, args.warmup, profile=False)
+    head_mode = args.voronoi_mode if args.device_only else MODE
+    ms, _, clocks, launches = time_device(seeds_u, args.steps, args.warmup, profile=False, mode=head_mode)
     value = world * W * H * args.steps / (ms / 1e3) / 1e6
-    _, profs, _, _ = time_device(seeds_u, args.steps, 1, profile=True)
+    _, profs, _, _ = time_device(seeds_u, args.steps, 1, profile=True, mode=head_mode)
 
     # stage breakdown and roofline of the dominant stage
     keys = ["seeds_ms", "propagate_ms", "detect_ms", "dedup_ms", "assign_ms", "compose_ms"]
@@ -685,9 +686,10 @@ def run_ours(args, rank, world):
     if args.device_only:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": "Mpixel/s", "ms_per_step": ms / args.steps,
+                              "voronoi_mode": head_mode,
                               "stages_ms": {k[:-3]: round(v, 4) for k, v in stage.items()},
                               "schedule": schedule, "autotune_ms": tuned_u, "passes": p0["passes"],
-                              "sparse_pass_trace": ctx.pass_trace(),
+                              "sparse_pass_trace": ctx.pass_trace() if head_mode == "reference" else [],
                               "gpu_launches": int(launches),
                               "roofline_achieved_gbs": achieved, "clocks": clocks}), flush=True)
         return
@@ -817,6 +819,8 @@ def main():
                     help="time only the incremental workload (both semantics)")
     ap.add_argument("--seeds", choices=["uniform", "clustered"], default="uniform",
                     help="seed layout of the --device-only step")
+    ap.add_argument("--voronoi-mode", choices=["reference", "exact"], default="reference",
+                    help="propagation semantics of the --device-only step")
     ap.add_argument("--serve-seconds", type=float, default=10.0,
                     help="length of the real-time serving trace (0 skips the serving measurement)")
     args = ap.parse_args()

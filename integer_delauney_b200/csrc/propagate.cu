@@ -612,19 +612,14 @@ __device__ __forceinline__ int cell_compact(uint32_t* bits, uint16_t* list, int*
     }
     if (lane == 31) warp_sums[warp] = incl;
     *inner_changed = __syncthreads_or(inner) != 0;   // also: every word was read before any is cleared
-    if (warp == 0) {
-        int v = lane < nwarps ? warp_sums[lane] : 0;
-        int inc = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int u = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o) inc += u;
-        }
-        if (lane < nwarps) warp_sums[lane] = inc - v;   // exclusive warp offsets
-        if (lane == nwarps - 1) warp_sums[31] = inc;    // total
+    // every warp adds up the few warp counts itself (no second barrier)
+    int before = 0, total = 0;
+    for (int k = 0; k < nwarps; ++k) {
+        const int v = warp_sums[k];
+        before += k < warp ? v : 0;
+        total += v;
     }
-    __syncthreads();
-    int pos = warp_sums[warp] + incl - cnt;
+    int pos = before + incl - cnt;
 #pragma unroll
     for (int j = 0; j < WPT; ++j) {
         const int i = tid * WPT + j;
@@ -636,8 +631,7 @@ __device__ __forceinline__ int cell_compact(uint32_t* bits, uint16_t* list, int*
         }
         if (i < WORDS) bits[i] = 0u;
     }
-    const int total = warp_sums[31];
-    __syncthreads();   // warp_sums and the list are read or rewritten by the next use
+    __syncthreads();   // the list is read, the bitmap and warp_sums rewritten, by the next use
     return total;
 }
 
