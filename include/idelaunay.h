@@ -428,7 +428,10 @@ IDL_API int idl_delaunay_finalise_device(idl_delaunay* d, int64_t* n_triangles_o
  *            the witnessing block in image coordinates -- finalise's map
  *            (Delaunay::build_tri_map_, src/cuda/delaunay_output.cu:68-84);
  *   ids = 1: 3 int32 per triangle (a, b, c) in insertion ids --
- *            Delaunay::get_triangles (src/cuda/delaunay_output.cu:186-200).
+ *            Delaunay::get_triangles (src/cuda/delaunay_output.cu:186-200);
+ *   ids = 2: 3 int32 per triangle (a, b, c) in batch seed ids, the vertex
+ *            columns of ids = 0 packed on the device: finalise's as_arrays
+ *            vertex array without the rows' other columns crossing PCIe.
  * Valid between deferred inserts.  *n_out = triangle count; tris_out may be
  * NULL to query the count; otherwise capacity (int32 entries) must hold it. */
 IDL_API int idl_delaunay_triangles(idl_delaunay* d, int ids, int32_t* tris_out, int64_t capacity, int64_t* n_out);

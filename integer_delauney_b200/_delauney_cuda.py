@@ -382,12 +382,17 @@ class Delaunay:
     def _generation(self) -> int:
         return int(self._info()[_capi.DI_GENERATION])
 
-    def _tris(self, ids: int) -> np.ndarray:
+    def _tris(self, ids: int, count: int | None = None) -> np.ndarray:
+        """Triangle rows (idl_delaunay_triangles format `ids`) in pinned host
+        memory; `count`, when the caller already has the triangle count,
+        saves the query call."""
         n = ctypes.c_int64(0)
-        self._call("idl_delaunay_triangles", ids, None, 0, ctypes.byref(n))
+        if count is None:
+            self._call("idl_delaunay_triangles", ids, None, 0, ctypes.byref(n))
+            count = n.value
         cols = 5 if ids == 0 else 3
-        out = np.empty((n.value, cols), dtype=np.int32)
-        if n.value:
+        out = _host_buffer((count, cols))
+        if count:
             self._call("idl_delaunay_triangles", ids, out.ctypes.data, out.size, ctypes.byref(n))
         return out
 
@@ -413,7 +418,9 @@ class Delaunay:
         t = (ctypes.c_float * _capi.T_COUNT)() if timings else None
         self._call("idl_delaunay_finalise", grid.ctypes.data, ctypes.byref(n),
                    ctypes.cast(t, ctypes.c_void_p) if t is not None else None)
-        m, g = build_output(self._tris(0), grid, as_arrays)
+        # as_arrays: the vertex triples packed on the device (format 2), not
+        # the five-column rows sliced on the host
+        m, g = build_output(self._tris(2 if as_arrays else 0, int(n.value)), grid, as_arrays)
         return m, g, t
 
     # -- reference API ---------------------------------------------------------
@@ -459,7 +466,7 @@ class Delaunay:
         gen = ctypes.c_uint64(0)
         self._call("idl_delaunay_finalise_device", ctypes.byref(n), ctypes.byref(p_t), ctypes.byref(p_s),
                    ctypes.byref(p_m), ctypes.byref(gen))
-        verts = np.ascontiguousarray(self._tris(0)[:, 2:5])
+        verts = self._tris(2, int(n.value))
         count = self.width * self.height
         return (verts, DeviceArrayView(self, p_t.value or 0, count, "<i4", gen.value),
                 DeviceArrayView(self, p_s.value or 0, count, "<i4", gen.value),

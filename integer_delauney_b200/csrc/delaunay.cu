@@ -390,6 +390,15 @@ __global__ void k_tris_insertion(const int32_t* __restrict__ tris, int64_t n, co
     for (int j = 0; j < 3; ++j) out[t * 3 + j] = __ldg(&inv[tris[t * 5 + 2 + j]]);
 }
 
+// (a, b, c) of each (x, y, a, b, c) row, batch seed ids unchanged.
+__global__ void k_tris_batch_verts(const int32_t* __restrict__ tris, int64_t n, int32_t* __restrict__ out)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n * 3) return;
+    const int64_t t = i / 3;
+    out[i] = tris[t * 5 + 2 + (i - t * 3)];
+}
+
 // Three undirected edge keys a * n + b (a < b, insertion ids) per triangle
 // (build_edge_keys_kernel, delaunay_scalar_field.cu:34-56).
 __global__ void k_edge_keys(const int32_t* __restrict__ tris, int64_t n_tri, const int32_t* __restrict__ inv,
@@ -1162,7 +1171,7 @@ int idl_delaunay_triangles(idl_delaunay* d, int ids, int32_t* out, int64_t capac
     IDL_API_BEGIN
     check_handle(d);
     const Unbinder unbind_on_exit{d};
-    if (ids != 0 && ids != 1) invalid("ids must be 0 (batch) or 1 (insertion order)");
+    if (ids < 0 || ids > 2) invalid("ids must be 0 (batch rows), 1 (insertion order) or 2 (batch vertices)");
     DeviceGuard g(d->device);
     Context& C = d->ctx();
     ensure_topology(*d, nullptr);
@@ -1172,6 +1181,12 @@ int idl_delaunay_triangles(idl_delaunay* d, int ids, int32_t* out, int64_t capac
     if (capacity < d->n_tri * cols) invalid("triangle buffer too small");
     if (ids == 0) {
         IDL_CUDA(cudaMemcpyAsync(out, C.tris.ptr, (size_t)d->n_tri * 5 * 4, cudaMemcpyDeviceToHost, C.stream));
+    } else if (ids == 2) {
+        d->stage.ensure((size_t)d->n_tri * 3 * 4);
+        k_tris_batch_verts<<<blocks(d->n_tri * 3), 256, 0, C.stream>>>(C.tris.as<int32_t>(), d->n_tri,
+                                                                      d->stage.as<int32_t>());
+        IDL_LAUNCH();
+        IDL_CUDA(cudaMemcpyAsync(out, d->stage.ptr, (size_t)d->n_tri * 3 * 4, cudaMemcpyDeviceToHost, C.stream));
     } else {
         d->stage.ensure((size_t)d->n_tri * 3 * 4);
         k_tris_insertion<<<blocks(d->n_tri), 256, 0, C.stream>>>(C.tris.as<int32_t>(), d->n_tri, d->inv,

@@ -517,3 +517,23 @@ def test_insert_as_tile_rounds_equals_sparse_kernel(cu):
     vb, gb = b.finalise(as_arrays=True)
     np.testing.assert_array_equal(va, vb)
     np.testing.assert_array_equal(ga, gb)
+
+
+def test_vertex_arrays_equal_the_map_vertices(cu):
+    """finalise(as_arrays=True) and finalise_device return the vertex triples
+    packed on the device (idl_delaunay_triangles format 2); they equal the
+    (a, b, c) columns of finalise's map, before and after further inserts."""
+    W, H = 300, 200
+    seeds = uniform(W, H, 900, seed=5)
+    d = cu.Delaunay(W, H, 2000, 16)
+    for part in (seeds[:500], seeds[500:]):
+        d.insert_deferred(part)
+        m, g = d.finalise()
+        verts, g2 = d.finalise(as_arrays=True)
+        want = np.array([m[t][2:5] for t in range(len(m))], dtype=np.int32).reshape(-1, 3)
+        np.testing.assert_array_equal(verts, want)
+        np.testing.assert_array_equal(g2, g)
+        v_dev = d.finalise_device()[0]
+        np.testing.assert_array_equal(v_dev, want)
+        m2, g3 = d.insert(np.zeros((0, 2), dtype=np.int32), as_arrays=True)
+        np.testing.assert_array_equal(m2, want)
