@@ -108,14 +108,16 @@ def build_output(tris: np.ndarray, grid: np.ndarray, as_arrays: bool):
 
 
 def _fetch_triangles(ctx, n_tri: int) -> np.ndarray:
-    out = _host_buffer((max(n_tri, 0), 5))
+    # pageable: the count changes call to call, and a new pinned block of a
+    # new size costs a page-locking allocation of milliseconds
+    out = np.empty((max(n_tri, 0), 5), dtype=np.int32)
     check(_capi.load().idl_get_triangles(ctx.handle, out.ctypes.data if n_tri else None, n_tri))
     return out
 
 
 def _fetch_vertices(ctx, n_tri: int) -> np.ndarray:
     """(n, 3) vertex triples, packed on the device (12 bytes per triangle cross PCIe)."""
-    out = _host_buffer((max(n_tri, 0), 3))
+    out = np.empty((max(n_tri, 0), 3), dtype=np.int32)
     check(_capi.load().idl_get_triangle_vertices(ctx.handle, out.ctypes.data if n_tri else None, n_tri))
     return out
 
@@ -383,15 +385,16 @@ class Delaunay:
         return int(self._info()[_capi.DI_GENERATION])
 
     def _tris(self, ids: int, count: int | None = None) -> np.ndarray:
-        """Triangle rows (idl_delaunay_triangles format `ids`) in pinned host
-        memory; `count`, when the caller already has the triangle count,
-        saves the query call."""
+        """Triangle rows (idl_delaunay_triangles format `ids`); `count`, when
+        the caller already has the triangle count, saves the query call.
+        Pageable memory: a pinned block of each new size would cost a
+        page-locking allocation."""
         n = ctypes.c_int64(0)
         if count is None:
             self._call("idl_delaunay_triangles", ids, None, 0, ctypes.byref(n))
             count = n.value
         cols = 5 if ids == 0 else 3
-        out = _host_buffer((count, cols))
+        out = np.empty((count, cols), dtype=np.int32)
         if count:
             self._call("idl_delaunay_triangles", ids, out.ctypes.data, out.size, ctypes.byref(n))
         return out
