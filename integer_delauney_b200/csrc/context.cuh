@@ -100,6 +100,7 @@ struct Scalars {
     int32_t max_side;         // longest triangle side, float-truncated (triangulation.cu:355-368)
     int32_t n_big;            // tall triangles the raster hands to its block-per-triangle pass
     int32_t n_handoff;        // micro-tiles the last tile round hands to the persistent kernel
+    int32_t tile_remaining;   // tiles listed for the tile round after the last one launched
 };
 
 struct Timing {

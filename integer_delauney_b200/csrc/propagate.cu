@@ -1136,7 +1136,9 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
 
     const int grid = std::min(n_tiles, C.num_sms * 3);
     int64_t r = 0;
-    int group = 2;
+    // a fixed number of rounds goes out in one group (one host round trip);
+    // to convergence, groups double from 2
+    int group = round_limit > 0 ? (int)std::min<int64_t>(round_limit, 64) : 2;
     int32_t remaining = 0;
     if (persistent) {
         // every round in one cooperative launch, rounds separated by the grid barrier
@@ -1212,14 +1214,16 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
             }
             IDL_LAUNCH();
         }
-        IDL_CUDA(cudaMemcpyAsync(&remaining, counts + r, 4, cudaMemcpyDeviceToHost, C.stream));
-        IDL_CUDA(cudaStreamSynchronize(C.stream));
+        // the list length and the scalars (last change, hand-off count) in one read-back
+        IDL_CUDA(cudaMemcpyAsync(&C.sc()->tile_remaining, counts + r, 4, cudaMemcpyDeviceToDevice, C.stream));
+        C.fetch_scalars();
+        remaining = C.host_sc->tile_remaining;
         if (remaining == 0) break;
         if (round_limit >= 0 && r >= round_limit) break;
         if (r >= max_rounds) throw Error(IDL_ERR_INTERNAL, "Voronoi propagation did not converge");
         group = std::min(group * 2, 8);
     }
-    C.fetch_scalars();
+    if (persistent) C.fetch_scalars();   // the loop above read them with its last list length
     const int64_t lc = C.host_sc->last_change;
     int64_t passes = lc < 0 ? 1 : lc + 2;
     if (C.prof.enabled) {
