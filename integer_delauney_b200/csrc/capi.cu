@@ -248,7 +248,8 @@ int64_t run_triangulate(Context& C, int W, int H, int64_t n, const int32_t* vgri
                      T.on ? C.timing.ev[1] : nullptr);
     T.mark(2);
     C.mark(PM_DEDUP);
-    C.fetch_scalars();
+    // the triangle count came back with detection's own read-back (ranking
+    // does not change it): no second host round trip here
     const int64_t nt = C.host_sc->n_triangles;
     T.mark(3);
     C.tgrid.ensure((size_t)W * H * sizeof(int32_t));

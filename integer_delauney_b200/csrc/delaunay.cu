@@ -602,9 +602,9 @@ void ensure_topology(DelaunayState& D, float* timings)
             else
                 detect_triangles(C, D.canvas(), D.planes, D.pos, D.N, D.P, timings ? e[1] : nullptr, D.rank);
             if (timings) IDL_CUDA(cudaEventRecord(e[2], C.stream));
-            C.fetch_scalars();
-            D.n_tri = C.host_sc->n_triangles;
+            D.n_tri = C.host_sc->n_triangles;   // from detection's own read-back
             if (timings) {
+                IDL_CUDA(cudaEventSynchronize(e[2]));
                 float a = 0.f, b = 0.f;
                 IDL_CUDA(cudaEventElapsedTime(&a, e[0], e[1]));
                 IDL_CUDA(cudaEventElapsedTime(&b, e[1], e[2]));
