@@ -301,7 +301,10 @@ int64_t propagate_sparse_from_tiles(Context& C, const Canvas& cv, const uint32_t
 // holds n_marked distinct micro-tiles, and C.bits (sparse_bits_words(cv)
 // words for each of the two passes' bitmaps) already has their bits set in
 // the first bitmap and none in the second.  Plane 0 holds the starting state,
-// the same in plane 1 outside the listed micro-tiles.
+// the same in plane 1 outside the listed micro-tiles.  The list length is read
+// on the device from C.sc()->n_handoff; n_marked is the host's copy of it (0:
+// nothing to do) or negative when the host has not read it.  On return
+// C.host_sc holds the scalars as the kernel left them.
 int64_t propagate_sparse_from_marks(Context& C, const Canvas& cv, const uint32_t* pos, const int32_t* marked,
                                     int n_marked, bool keys);
 int sparse_bits_words(const Canvas& cv);

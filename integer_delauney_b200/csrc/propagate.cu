@@ -1214,6 +1214,13 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
             }
             IDL_LAUNCH();
         }
+        // With the hand-off, the rounds, the plane copy and the persistent
+        // kernel all take their list lengths from the device: no read-back
+        // here (the kernel's own brings the scalars; an empty list ends it).
+        if (handoff && r == round_limit) {
+            remaining = -1;
+            break;
+        }
         // the list length and the scalars (last change, hand-off count) in one read-back
         IDL_CUDA(cudaMemcpyAsync(&C.sc()->tile_remaining, counts + r, 4, cudaMemcpyDeviceToDevice, C.stream));
         C.fetch_scalars();
@@ -1224,7 +1231,8 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
         group = std::min(group * 2, 8);
     }
     if (persistent) C.fetch_scalars();   // the loop above read them with its last list length
-    const int64_t lc = C.host_sc->last_change;
+    // after a hand-off (remaining < 0: not read) these are refreshed below
+    int64_t lc = C.host_sc->last_change;
     int64_t passes = lc < 0 ? 1 : lc + 2;
     if (C.prof.enabled) {
         // tile rounds: 8 B per inner cell (label in, label out) per processed
@@ -1244,7 +1252,7 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
         C.prof.tile_h = th;
         C.prof.steps_per_round = steps;
     }
-    if (remaining > 0) {
+    if (remaining != 0) {
         // Hand the tail to the sparse kernel: the latest state goes to plane 0.
         if (r & 1) std::swap(C.lab[0], C.lab[1]);
         int64_t sparse = 0;
@@ -1257,7 +1265,9 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
                                                          cv.Wd, cv.Hd, C.tiles[r & 1].as<int32_t>(), counts + r,
                                                          tiles_x, tw, th);
             IDL_LAUNCH();
-            sparse = propagate_sparse_from_marks(C, cv, pos, C.big_tiles.as<int32_t>(), C.host_sc->n_handoff, keys);
+            sparse = propagate_sparse_from_marks(C, cv, pos, C.big_tiles.as<int32_t>(), -1, keys);
+            lc = C.host_sc->last_change;   // read back with the persistent kernel's state
+            passes = lc < 0 ? 1 : lc + 2;
         } else {
             // Its first work list is every micro-tile of the tiles the next
             // round would have run (a superset of those that can change).

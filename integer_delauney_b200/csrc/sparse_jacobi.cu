@@ -610,10 +610,12 @@ int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos,
     int32_t* l0 = C.tiles[0].as<int32_t>();
     int32_t* l1 = C.tiles[1].as<int32_t>();
     if (st.marked) {
+        // the hand-off list (capacity n_mt) serves as the first list itself;
+        // its length comes from the device (an empty one ends the kernel at
+        // once); n_marked < 0: the host has not read it
         if (st.n_marked == 0) return 0;
         if (st.n_marked > n_mt) throw Error(IDL_ERR_INTERNAL, "hand-off list longer than the canvas");
-        const int32_t n = st.n_marked;
-        IDL_CUDA(cudaMemcpyAsync(l0, st.marked, (size_t)n * 4, cudaMemcpyDeviceToDevice, C.stream));
+        l0 = const_cast<int32_t*>(st.marked);
         IDL_CUDA(cudaMemcpyAsync(counts, &C.sc()->n_handoff, 4, cudaMemcpyDeviceToDevice, C.stream));
     } else if (st.big_list) {
         if (st.n_big == 0) return 0;
@@ -664,6 +666,9 @@ int64_t propagate_sparse_impl(Context& C, const Canvas& cv, const uint32_t* pos,
         IDL_CUDA(cudaLaunchCooperativeKernel(kernel, dim3(grid), dim3(SJ_THREADS), args, 0, C.stream));
         count_launch();
         IDL_CUDA(cudaMemcpyAsync(&h, gs, sizeof(GridSync), cudaMemcpyDeviceToHost, C.stream));
+        // the scalars ride along: a caller that launched its tile rounds
+        // without a read-back takes their last change from here
+        IDL_CUDA(cudaMemcpyAsync(C.host_sc, C.scalars.ptr, sizeof(Scalars), cudaMemcpyDeviceToHost, C.stream));
         IDL_CUDA(cudaStreamSynchronize(C.stream));
     }
     if (h.error) throw Error(IDL_ERR_INTERNAL, "Voronoi propagation: grid barrier timed out");
