@@ -34,7 +34,7 @@ import numpy as np
 
 from . import _capi
 
-SCHEDULES = (0, 1, 2, 3, -1)
+SCHEDULES = (0, 1, 2, 3, 4, 6, -1)
 _cache: dict[tuple, tuple[int, int]] = {}
 # the timings of the last tuning run: {(schedule, shape): best ms of the repeats}
 last_report: dict[tuple[int, int], float] = {}

@@ -153,6 +153,7 @@ struct Context {
     DevBuf rbig;          // raster: ids of tall triangles
     DevBuf bits;          // work-list dedup bitmaps of the persistent propagation kernel
     DevBuf big_tiles;     // tile rounds' last work list, handed to the persistent kernel
+    DevBuf cellbits;      // cell-list tile rounds: three last-pass change bitmaps, in rotation
     DevBuf exact_dy;      // exact mode: row distance to each cell's column-nearest seed
     DevBuf exact_rmin;    // exact mode: per row, smallest squared row distance of each 32-column block
     int32_t stamp_epoch = 0;

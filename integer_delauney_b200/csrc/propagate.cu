@@ -645,11 +645,57 @@ struct Handoff {
     int mt_x;
 };
 
+// Last-pass changes passed from one tile round to the next: one bit per
+// canvas cell, rows of `stride` words (bit x of row y: word y * stride + x / 32).
+// A round writes into `out` the inner cells that changed in its last pass; the
+// next round reads them as `in`, and its first list is those cells and their
+// neighbours -- exactly the cells that can change in its first pass, where the
+// neighbour test (in null) also lists every settled boundary.  `clear`, a
+// bitmap no round of this launch or the previous one touches, is zeroed for
+// the round after next.
+struct CellBits {
+    const uint32_t* in;
+    uint32_t* out;
+    uint32_t* clear;
+    int stride;   // words per row
+    int words;    // words per bitmap
+};
+
+// Bits g .. g + 31 of a row of `stride` words (g may be negative); zeros
+// outside the row.
+__device__ __forceinline__ uint32_t row_bits32(const uint32_t* row, int stride, int g)
+{
+    const int w = g >> 5, sh = g & 31;
+    const uint32_t lo = (w >= 0 && w < stride) ? row[w] : 0u;
+    const uint32_t hi = (w + 1 >= 0 && w + 1 < stride) ? row[w + 1] : 0u;
+    return __funnelshift_r(lo, hi, sh);
+}
+
+// The inner cells marked in the region bitmap `bits` into cb.out (region
+// origin ox, oy on the canvas; inner cells start at ox + KS = tx * TW >= 0).
+template <int RW, int RH, int KS, int TW, int TH>
+__device__ __forceinline__ void cell_bits_out(const uint32_t* bits, const CellBits& cb, int ox, int oy, int Hd)
+{
+    constexpr int WR = RW / 32;
+    const int gx0 = ox + KS;
+    const int w0 = gx0 >> 5, nw = ((gx0 + TW - 1) >> 5) - w0 + 1;
+    for (int task = threadIdx.x; task < TH * nw; task += blockDim.x) {
+        const int iy = task / nw, gw = w0 + task % nw;
+        const int gy = oy + KS + iy;
+        if (gy >= Hd) continue;
+        const int rb = gw * 32 - ox;   // region column of the word's bit 0
+        const int lo = max(KS - rb, 0), hi = min(KS + TW - rb, 32);
+        const uint32_t span = hi - lo >= 32 ? 0xFFFFFFFFu : ((1u << (hi - lo)) - 1u) << lo;
+        const uint32_t v = row_bits32(bits + (KS + iy) * WR, WR, rb) & span;
+        if (v) atomicOr(&cb.out[(size_t)gy * cb.stride + gw], v);
+    }
+}
+
 template <int RW, int RH, int KS, bool L2>
 __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* src, int32_t* dst, int pitch, int Wd,
                                           int Hd, int t, int tiles_x, int tiles_y, int32_t* list_out,
                                           int32_t* count_out, int32_t* stamp, int32_t stamp_next, long long step_base,
-                                          long long* last_change, Handoff ho)
+                                          long long* last_change, Handoff ho, const CellBits& cb)
 {
     using T = CellTile<RW, RH, KS>;
     constexpr int N = T::N;
@@ -674,20 +720,33 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
         bufA[i] = v;
         bufB[i] = v;
     }
-    __syncthreads();
-    // first list: cells with a neighbour owned by another seed; the block's
-    // 32-cell strides are warp-aligned, so each warp's ballot is one word
-    for (int i = tid; i < N; i += blockDim.x) {
-        const int32_t o = bufA[i];
-        const int cx = i % RW, cy = i / RW;
-        const bool diff = o >= UNDEF && ((cx > 0 && bufA[i - 1] != o) || (cx < RW - 1 && bufA[i + 1] != o) ||
-                                         (cy > 0 && bufA[i - RW] != o) || (cy < RH - 1 && bufA[i + RW] != o));
-        const uint32_t word = __ballot_sync(0xFFFFFFFFu, diff);
-        if ((tid & 31) == 0) bits[i >> 5] = word;
-    }
-    __syncthreads();
     bool inner_changed = false;
-    int n = cell_compact<RW, RH, KS, T::TW, T::TH, T::WPT, false>(bits, listA, warp_sums, &inner_changed);
+    int n;
+    if (cb.in) {
+        // first list: the previous round's last-pass changes and their neighbours
+        constexpr int WR = RW / 32;
+        for (int i = tid; i < T::WORDS; i += blockDim.x) {
+            const int gy = oy + i / WR;
+            bits[i] = (gy >= 0 && gy < Hd) ? row_bits32(cb.in + (size_t)gy * cb.stride, cb.stride, ox + 32 * (i % WR))
+                                           : 0u;
+        }
+        __syncthreads();
+        n = cell_compact<RW, RH, KS, T::TW, T::TH, T::WPT, true>(bits, listA, warp_sums, &inner_changed);
+    } else {
+        __syncthreads();
+        // first list: cells with a neighbour owned by another seed; the block's
+        // 32-cell strides are warp-aligned, so each warp's ballot is one word
+        for (int i = tid; i < N; i += blockDim.x) {
+            const int32_t o = bufA[i];
+            const int cx = i % RW, cy = i / RW;
+            const bool diff = o >= UNDEF && ((cx > 0 && bufA[i - 1] != o) || (cx < RW - 1 && bufA[i + 1] != o) ||
+                                             (cy > 0 && bufA[i - RW] != o) || (cy < RH - 1 && bufA[i + RW] != o));
+            const uint32_t word = __ballot_sync(0xFFFFFFFFu, diff);
+            if ((tid & 31) == 0) bits[i >> 5] = word;
+        }
+        __syncthreads();
+        n = cell_compact<RW, RH, KS, T::TW, T::TH, T::WPT, false>(bits, listA, warp_sums, &inner_changed);
+    }
 
     int32_t* cur = bufA;
     int32_t* nxt = bufB;
@@ -716,6 +775,7 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
             if (k != own) atomicOr(&bits[c >> 5], 1u << (c & 31));
         }
         __syncthreads();
+        if (cb.out && s == KS - 1) cell_bits_out<RW, RH, KS, T::TW, T::TH>(bits, cb, ox, oy, Hd);
         // the next list: changed cells and their neighbours
         n = cell_compact<RW, RH, KS, T::TW, T::TH, T::WPT, true>(bits, ln, warp_sums, &inner_changed);
         if (inner_changed) last_step = s;
@@ -762,7 +822,11 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
 
     if (last_step >= 0) {
         if (tid == 0) atomicMax(last_change, step_base + last_step);
-        if (tid < 9) {
+        // The next round's changes spread from this round's last-pass changes
+        // alone: only those list the neighbourhood.  Any change lists the tile
+        // itself, whose next run copies its inner cells to the other plane
+        // (a tile no round runs must hold the same state in both).
+        if ((last_step == KS - 1 && tid < 9) || tid == 4) {
             const int nx = tx + int(tid % 3) - 1, ny = ty + int(tid / 3) - 1;
             if (nx >= 0 && nx < tiles_x && ny >= 0 && ny < tiles_y) {
                 const int nt = ny * tiles_x + nx;
@@ -782,13 +846,15 @@ k_round_cells(const int32_t* __restrict__ src, int32_t* __restrict__ dst, int pi
               const int32_t* __restrict__ list_in, const int32_t* __restrict__ count_in,
               int32_t* __restrict__ list_out, int32_t* __restrict__ count_out, int32_t* __restrict__ stamp,
               int32_t stamp_next, int tiles_x, int tiles_y, long long step_base, long long* __restrict__ last_change,
-              Handoff ho)
+              Handoff ho, CellBits cb)
 {
     extern __shared__ __align__(16) unsigned char cell_smem[];
+    if (cb.clear)
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cb.words; i += gridDim.x * blockDim.x) cb.clear[i] = 0u;
     const int n_items = *count_in;
     for (int item = blockIdx.x; item < n_items; item += gridDim.x)
         cell_tile<RW, RH, KS, false>(cell_smem, src, dst, pitch, Wd, Hd, list_in[item], tiles_x, tiles_y, list_out,
-                                     count_out, stamp, stamp_next, step_base, last_change, ho);
+                                     count_out, stamp, stamp_next, step_base, last_change, ho, cb);
 }
 
 // Plane `dst` takes plane `src`'s inner cells of the listed tiles: after it,
@@ -963,7 +1029,7 @@ constexpr int N_CELL_SHAPES = int(sizeof(CELL_SHAPES) / sizeof(CELL_SHAPES[0]));
 template <int RW, int RH, int KS>
 void launch_round_cells(Context& C, const int32_t* src, int32_t* dst, const Canvas& cv, const int32_t* lin,
                         const int32_t* cin, int32_t* lout, int32_t* cout, int32_t* stamp, int32_t stamp_next,
-                        int tiles_x, int tiles_y, long long base, long long* last, Handoff ho)
+                        int tiles_x, int tiles_y, long long base, long long* last, Handoff ho, const CellBits& cb)
 {
     using T = CellTile<RW, RH, KS>;
     // the shared-memory opt-in belongs to each device's context: set once per device
@@ -979,7 +1045,7 @@ void launch_round_cells(Context& C, const int32_t* src, int32_t* dst, const Canv
     const int grid = std::max(1, std::min(tiles_x * tiles_y, std::max(per_sm, 1) * C.num_sms));
     k_round_cells<RW, RH, KS><<<grid, T::THREADS, T::SMEM, C.stream>>>(src, dst, cv.pitch, cv.Wd, cv.Hd, lin, cin,
                                                                       lout, cout, stamp, stamp_next, tiles_x,
-                                                                      tiles_y, base, last, ho);
+                                                                      tiles_y, base, last, ho, cb);
 }
 
 template <int NW, int KS>
@@ -1134,6 +1200,21 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
         ho_last = Handoff{C.bits.as<uint32_t>(), C.big_tiles.as<int32_t>(), &C.sc()->n_handoff, mt_x};
     }
 
+    // cell-list rounds: round r reads the change bits of round r - 1 from
+    // bitmap r % 3, writes its own to (r + 1) % 3 and clears (r + 2) % 3
+    int cb_stride = 0, cb_words = 0;
+    if (cells) {
+        cb_stride = ceil_div(tiles_x * tw, 32) + 1;
+        cb_words = cb_stride * cv.Hd;
+        C.cellbits.ensure((size_t)cb_words * 3 * 4);
+        IDL_CUDA(cudaMemsetAsync(C.cellbits.ptr, 0, (size_t)cb_words * 3 * 4, C.stream));
+    }
+    auto cell_bits = [&](int64_t rr) {
+        uint32_t* b = C.cellbits.as<uint32_t>();
+        return CellBits{rr > 0 ? b + (size_t)(rr % 3) * cb_words : nullptr, b + (size_t)((rr + 1) % 3) * cb_words,
+                        rr > 1 ? b + (size_t)((rr + 2) % 3) * cb_words : nullptr, cb_stride, cb_words};
+    };
+
     const int grid = std::min(n_tiles, C.num_sms * 3);
     int64_t r = 0;
     // a fixed number of rounds goes out in one group (one host round trip);
@@ -1168,22 +1249,23 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
                     IDL_CUDA(cudaMemsetAsync(ho.bits, 0, (size_t)sparse_bits_words(cv) * 2 * 4, C.stream));
                     IDL_CUDA(cudaMemsetAsync(ho.count, 0, 4, C.stream));
                 }
+                const CellBits cb = cell_bits(r);
                 switch (tile - 2 * N_KEY_SHAPES) {
                 case 1:
                     launch_round_cells<64, 64, 4>(C, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
-                                                  stamp_next, tiles_x, tiles_y, base, last, ho);
+                                                  stamp_next, tiles_x, tiles_y, base, last, ho, cb);
                     break;
                 case 2:
                     launch_round_cells<128, 64, 8>(C, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
-                                                   stamp_next, tiles_x, tiles_y, base, last, ho);
+                                                   stamp_next, tiles_x, tiles_y, base, last, ho, cb);
                     break;
                 case 3:
                     launch_round_cells<128, 128, 16>(C, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
-                                                     stamp_next, tiles_x, tiles_y, base, last, ho);
+                                                     stamp_next, tiles_x, tiles_y, base, last, ho, cb);
                     break;
                 default:
                     launch_round_cells<64, 64, 8>(C, srcp, dstp, cv, lin, counts + r, lout, counts + r + 1, stamp,
-                                                  stamp_next, tiles_x, tiles_y, base, last, ho);
+                                                  stamp_next, tiles_x, tiles_y, base, last, ho, cb);
                 }
             } else if (keys) {
                 switch (base_shape) {
