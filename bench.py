@@ -78,8 +78,9 @@ def reduce_max(value: float, world: int) -> float:
 
 # dram__bytes_read.sum + dram__bytes_write.sum of the dominant stage's kernels
 # for one step of this workload (uniform seeds), from ncu --set full captures:
-# the tile round (69.1 + 29.0 MB) and the persistent kernel's tail (357.3 + 223.2 MB)
-TRAFFIC_PER_LAUNCH = {"propagate_ms": 69.1e6 + 29.0e6 + 357.3e6 + 223.2e6}
+# the three cell-list tile rounds (70.4 + 29.7, 72.6 + 30.5, 72.6 + 32.3 MB) and
+# the persistent kernel's tail (113.7 + 30.6 MB)
+TRAFFIC_PER_LAUNCH = {"propagate_ms": 70.4e6 + 29.7e6 + 72.6e6 + 30.5e6 + 72.6e6 + 32.3e6 + 113.7e6 + 30.6e6}
 
 
 class ClockSampler:
