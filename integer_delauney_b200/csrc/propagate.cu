@@ -565,33 +565,40 @@ struct CellTile {
 
 // The cells of `bits` (one bit per cell, rows of RW / 32 words) into `list`
 // in ascending order; the bitmap is cleared on the way.  With DILATE, `bits`
-// holds the cells that changed in the step just run and the list takes them
-// and their four neighbours within the region (the cells that can change in
-// the next step), built word by word instead of one shared atomic per mark.
-// Returns the list length (every thread); *inner_changed tells whether a
-// changed cell lies in the inner tile [KS, KS + TW) x [KS, KS + TH).
-template <int RW, int RH, int KS, int TW, int TH, int WPT, bool DILATE>
-__device__ __forceinline__ int cell_compact(uint32_t* bits, uint16_t* list, int* warp_sums, bool* inner_changed)
+// holds the cells that changed in the step just run and the list takes their
+// four neighbours within the region (the cells that can change in the next
+// step: a cell none of whose neighbours changed keeps its value, since the
+// best of its owner and unchanged neighbours is already its owner), built
+// word by word instead of one shared atomic per mark.  With COPY, the changed
+// cells outside that list follow it (*n_copy of them): the next step only
+// copies their new value into its output buffer, so that every cell it does
+// not write holds the same value in both buffers.  Returns the length of the
+// list proper (every thread); *inner_changed tells whether a changed cell lies
+// in the inner tile [KS, KS + TW) x [KS, KS + TH).
+template <int RW, int RH, int KS, int TW, int TH, int WPT, bool DILATE, bool COPY>
+__device__ __forceinline__ int cell_compact(uint32_t* bits, uint16_t* list, int* warp_sums, bool* inner_changed,
+                                            int* n_copy)
 {
     constexpr int WR = RW / 32, WORDS = RW * RH / 32;
+    static_assert(RW * RH < 65536, "two list lengths share one 32-bit scan");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-    uint32_t w[WPT];
-    int cnt = 0;
+    uint32_t w[WPT], wc[WPT];
+    int cnt = 0;   // list cells, plus copy cells << 16
     bool inner = false;
 #pragma unroll
     for (int j = 0; j < WPT; ++j) {
         const int i = tid * WPT + j;
-        uint32_t m = 0u;
+        uint32_t m = 0u, mc = 0u;
         if (i < WORDS) {
             const uint32_t c = bits[i];
-            m = c;
             if (DILATE) {
                 const int row = i / WR, wi = i % WR;
-                m |= (c << 1) | (c >> 1);
+                m = (c << 1) | (c >> 1);
                 if (wi > 0) m |= bits[i - 1] >> 31;
                 if (wi < WR - 1) m |= bits[i + 1] << 31;
                 if (row > 0) m |= bits[i - WR];
                 if (row < RH - 1) m |= bits[i + WR];
+                if (COPY) mc = c & ~m;
                 if (row >= KS && row < KS + TH) {
                     const int lo = max(KS - wi * 32, 0), hi = min(KS + TW - wi * 32, 32);
                     if (hi > lo) {
@@ -599,10 +606,13 @@ __device__ __forceinline__ int cell_compact(uint32_t* bits, uint16_t* list, int*
                         inner = inner || (c & span) != 0u;
                     }
                 }
+            } else {
+                m = c;
             }
         }
         w[j] = m;
-        cnt += __popc(m);
+        wc[j] = mc;
+        cnt += __popc(m) + (COPY ? __popc(mc) << 16 : 0);
     }
     int incl = cnt;
 #pragma unroll
@@ -619,7 +629,9 @@ __device__ __forceinline__ int cell_compact(uint32_t* bits, uint16_t* list, int*
         before += k < warp ? v : 0;
         total += v;
     }
-    int pos = before + incl - cnt;
+    const int start = before + incl - cnt;
+    const int n_list = total & 0xFFFF;
+    int pos = start & 0xFFFF, pos_c = n_list + (start >> 16);
 #pragma unroll
     for (int j = 0; j < WPT; ++j) {
         const int i = tid * WPT + j;
@@ -629,10 +641,19 @@ __device__ __forceinline__ int cell_compact(uint32_t* bits, uint16_t* list, int*
             m &= m - 1;
             list[pos++] = (uint16_t)(i * 32 + b);
         }
+        if (COPY) {
+            uint32_t mc = wc[j];
+            while (mc) {
+                const int b = __ffs(mc) - 1;
+                mc &= mc - 1;
+                list[pos_c++] = (uint16_t)(i * 32 + b);
+            }
+        }
         if (i < WORDS) bits[i] = 0u;
     }
     __syncthreads();   // the list is read, the bitmap and warp_sums rewritten, by the next use
-    return total;
+    if (COPY) *n_copy = total >> 16;
+    return n_list;
 }
 
 // What the last tile round before the persistent kernel leaves it (bits null:
@@ -721,7 +742,7 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
         bufB[i] = v;
     }
     bool inner_changed = false;
-    int n;
+    int n, n_copy = 0;
     if (cb.in) {
         // first list: the previous round's last-pass changes and their neighbours
         constexpr int WR = RW / 32;
@@ -731,7 +752,9 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
                                            : 0u;
         }
         __syncthreads();
-        n = cell_compact<RW, RH, KS, T::TW, T::TH, T::WPT, true>(bits, listA, warp_sums, &inner_changed);
+        // (both buffers start equal: nothing to copy)
+        n = cell_compact<RW, RH, KS, T::TW, T::TH, T::WPT, true, false>(bits, listA, warp_sums, &inner_changed,
+                                                                        &n_copy);
     } else {
         __syncthreads();
         // first list: cells with a neighbour owned by another seed; the block's
@@ -745,7 +768,8 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
             if ((tid & 31) == 0) bits[i >> 5] = word;
         }
         __syncthreads();
-        n = cell_compact<RW, RH, KS, T::TW, T::TH, T::WPT, false>(bits, listA, warp_sums, &inner_changed);
+        n = cell_compact<RW, RH, KS, T::TW, T::TH, T::WPT, false, false>(bits, listA, warp_sums, &inner_changed,
+                                                                         &n_copy);
     }
 
     int32_t* cur = bufA;
@@ -774,10 +798,16 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
             nxt[c] = k;
             if (k != own) atomicOr(&bits[c >> 5], 1u << (c & 31));
         }
+        // cells that changed in the step before but cannot change now
+        for (int i = tid; i < n_copy; i += blockDim.x) {
+            const int c = lc[n + i];
+            nxt[c] = cur[c];
+        }
         __syncthreads();
         if (cb.out && s == KS - 1) cell_bits_out<RW, RH, KS, T::TW, T::TH>(bits, cb, ox, oy, Hd);
         // the next list: changed cells and their neighbours
-        n = cell_compact<RW, RH, KS, T::TW, T::TH, T::WPT, true>(bits, ln, warp_sums, &inner_changed);
+        n = cell_compact<RW, RH, KS, T::TW, T::TH, T::WPT, true, true>(bits, ln, warp_sums, &inner_changed,
+                                                                       &n_copy);
         if (inner_changed) last_step = s;
         int32_t* tb = cur; cur = nxt; nxt = tb;
         uint16_t* tl = lc; lc = ln; ln = tl;
