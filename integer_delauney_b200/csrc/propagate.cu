@@ -927,6 +927,16 @@ __global__ void k_seed_keys(int32_t* __restrict__ a, int32_t* __restrict__ b, in
     b[o] = k;
 }
 
+// One bit per seed cell in a change bitmap of rows of `stride` words: from
+// scratch, the seeds are the change the first pass reacts to.
+__global__ void k_mark_cells(const uint32_t* __restrict__ pos, int64_t n, uint32_t* __restrict__ bits, int stride)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t p = pos[i];
+    atomicOr(&bits[(size_t)pos_y(p) * stride + (pos_x(p) >> 5)], 1u << (pos_x(p) & 31));
+}
+
 // Keys back to ids: `ids` (the other plane, free once both planes agree)
 // takes at each seed cell that seed's id; every owned cell of `lab` then
 // looks its owner's id up at the owner's own cell.  Only seed cells of `ids`
@@ -1089,7 +1099,7 @@ void launch_round_keys(Context& C, int per_sm, const int32_t* src, int32_t* dst,
 }
 
 int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
-                         int64_t n_new, bool keys);
+                         int64_t n_new, bool keys, const uint32_t* start_pos = nullptr, int64_t n_start = 0);
 
 // Up to `rounds_cap` owner-key tile rounds in one cooperative launch (the
 // first work list already in C.tiles[0] and counts[0]); returns the rounds run.
@@ -1147,7 +1157,7 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, i
             C.lab[0].as<int32_t>(), C.lab[1].as<int32_t>(), cv.pitch, pos, n_seeds);
         IDL_LAUNCH();
     }
-    const int64_t passes = propagate_rounds(C, mode, cv, pos, nullptr, 0, true);
+    const int64_t passes = propagate_rounds(C, mode, cv, pos, nullptr, 0, true, pos, n_seeds);
     // the result is in plane 0 (both planes agree); plane 1 takes the ids at the seed cells
     if (n_seeds > 0) {
         k_seed_ids<<<(unsigned)((n_seeds + 255) / 256), 256, 0, C.stream>>>(C.lab[1].as<int32_t>(), cv.pitch, pos,
@@ -1164,7 +1174,7 @@ int64_t propagate(Context& C, int mode, const Canvas& cv, const uint32_t* pos, i
 namespace {
 
 int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t* pos, const uint32_t* seed_pos,
-                         int64_t n_new, bool keys)
+                         int64_t n_new, bool keys, const uint32_t* start_pos, int64_t n_start)
 {
     // Reference semantics.  A continued propagation (seed_pos) is local from
     // its first pass: the sparse kernel alone, or with C.dense_rounds < 0 tile
@@ -1231,18 +1241,27 @@ int64_t propagate_rounds(Context& C, int mode, const Canvas& cv, const uint32_t*
     }
 
     // cell-list rounds: round r reads the change bits of round r - 1 from
-    // bitmap r % 3, writes its own to (r + 1) % 3 and clears (r + 2) % 3
+    // bitmap r % 3, writes its own to (r + 1) % 3 and clears (r + 2) % 3.
+    // From scratch (start_pos: the seeds), round 0 reads the seed cells from
+    // bitmap 0: their neighbours are the cells the first pass can change.
     int cb_stride = 0, cb_words = 0;
+    const bool start_bits = cells && start_pos && n_start > 0;
     if (cells) {
         cb_stride = ceil_div(tiles_x * tw, 32) + 1;
         cb_words = cb_stride * cv.Hd;
         C.cellbits.ensure((size_t)cb_words * 3 * 4);
         IDL_CUDA(cudaMemsetAsync(C.cellbits.ptr, 0, (size_t)cb_words * 3 * 4, C.stream));
+        if (start_bits) {
+            k_mark_cells<<<(unsigned)((n_start + 255) / 256), 256, 0, C.stream>>>(start_pos, n_start,
+                                                                                C.cellbits.as<uint32_t>(), cb_stride);
+            IDL_LAUNCH();
+        }
     }
     auto cell_bits = [&](int64_t rr) {
         uint32_t* b = C.cellbits.as<uint32_t>();
-        return CellBits{rr > 0 ? b + (size_t)(rr % 3) * cb_words : nullptr, b + (size_t)((rr + 1) % 3) * cb_words,
-                        rr > 1 ? b + (size_t)((rr + 2) % 3) * cb_words : nullptr, cb_stride, cb_words};
+        return CellBits{rr > 0 || start_bits ? b + (size_t)(rr % 3) * cb_words : nullptr,
+                        b + (size_t)((rr + 1) % 3) * cb_words,
+                        rr > 0 ? b + (size_t)((rr + 2) % 3) * cb_words : nullptr, cb_stride, cb_words};
     };
 
     const int grid = std::min(n_tiles, C.num_sms * 3);
