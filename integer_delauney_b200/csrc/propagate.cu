@@ -712,6 +712,25 @@ __device__ __forceinline__ void cell_bits_out(const uint32_t* bits, const CellBi
     }
 }
 
+// Both region buffers take the labels of the RW x RH region at (ox, oy)
+// (OUTSIDE beyond the canvas).
+template <int RW, int RH, bool L2>
+__device__ __forceinline__ void load_region(int32_t* bufA, int32_t* bufB, const int32_t* src, int pitch, int Wd,
+                                            int Hd, int ox, int oy)
+{
+    for (int i = threadIdx.x; i < RW * RH; i += blockDim.x) {
+        const int cx = i % RW, cy = i / RW;
+        const int gx = ox + cx, gy = oy + cy;
+        int32_t v = OUTSIDE;
+        if (gx >= 0 && gx < Wd && gy >= 0 && gy < Hd) {
+            const int32_t* p = src + (size_t)gy * pitch + gx;
+            v = L2 ? __ldcg(p) : *p;
+        }
+        bufA[i] = v;
+        bufB[i] = v;
+    }
+}
+
 template <int RW, int RH, int KS, bool L2>
 __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* src, int32_t* dst, int pitch, int Wd,
                                           int Hd, int t, int tiles_x, int tiles_y, int32_t* list_out,
@@ -730,32 +749,39 @@ __device__ __forceinline__ void cell_tile(unsigned char* smem, const int32_t* sr
     const int tx = t % tiles_x, ty = t / tiles_x;
     const int ox = tx * T::TW - KS, oy = ty * T::TH - KS;
 
-    for (int i = tid; i < N; i += blockDim.x) {
-        const int cx = i % RW, cy = i / RW;
-        const int gx = ox + cx, gy = oy + cy;
-        int32_t v = OUTSIDE;
-        if (gx >= 0 && gx < Wd && gy >= 0 && gy < Hd) {
-            const int32_t* p = src + (size_t)gy * pitch + gx;
-            v = L2 ? __ldcg(p) : *p;
-        }
-        bufA[i] = v;
-        bufB[i] = v;
-    }
     bool inner_changed = false;
     int n, n_copy = 0;
     if (cb.in) {
-        // first list: the previous round's last-pass changes and their neighbours
+        // first list: the previous round's last-pass changes and their
+        // neighbours.  A region with none only brings the output plane up to
+        // date: its inner cells are copied, nothing is evaluated.
         constexpr int WR = RW / 32;
+        bool any = false;
         for (int i = tid; i < T::WORDS; i += blockDim.x) {
             const int gy = oy + i / WR;
-            bits[i] = (gy >= 0 && gy < Hd) ? row_bits32(cb.in + (size_t)gy * cb.stride, cb.stride, ox + 32 * (i % WR))
-                                           : 0u;
+            const uint32_t w = (gy >= 0 && gy < Hd)
+                                   ? row_bits32(cb.in + (size_t)gy * cb.stride, cb.stride, ox + 32 * (i % WR))
+                                   : 0u;
+            bits[i] = w;
+            any = any || w != 0u;
         }
+        if (!__syncthreads_or(any)) {
+            for (int i = tid; i < T::TW * T::TH; i += blockDim.x) {
+                const int gx = ox + KS + i % T::TW, gy = oy + KS + i / T::TW;
+                if (gx < Wd && gy < Hd) {
+                    const int32_t* p = src + (size_t)gy * pitch + gx;
+                    dst[(size_t)gy * pitch + gx] = L2 ? __ldcg(p) : *p;
+                }
+            }
+            return;
+        }
+        load_region<RW, RH, L2>(bufA, bufB, src, pitch, Wd, Hd, ox, oy);
         __syncthreads();
         // (both buffers start equal: nothing to copy)
         n = cell_compact<RW, RH, KS, T::TW, T::TH, T::WPT, true, false>(bits, listA, warp_sums, &inner_changed,
                                                                         &n_copy);
     } else {
+        load_region<RW, RH, L2>(bufA, bufB, src, pitch, Wd, Hd, ox, oy);
         __syncthreads();
         // first list: cells with a neighbour owned by another seed; the block's
         // 32-cell strides are warp-aligned, so each warp's ballot is one word
