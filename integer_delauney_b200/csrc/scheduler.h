@@ -76,7 +76,10 @@ inline int64_t scratch_bytes(int64_t Wd, int64_t Hd, int64_t seeds)
     const int64_t n_mt = ((Wd + 7) / 8) * ((Hd + 7) / 8);
     int64_t hash = 1024;
     while (hash < 8 * seeds + 1024) hash <<= 1;
-    return n_mt * 8 + n_mt / 4 + 16 * (Wd + Hd) + 32 * hash + 48 * seeds + Wd * Hd / 8;
+    // hash table (32 B a slot) and the grouping and triangle rows sized by it
+    // (24 B a slot); the tile rounds' three change bitmaps
+    return n_mt * 8 + n_mt / 4 + 16 * (Wd + Hd) + 56 * hash + 48 * seeds + Wd * Hd / 8 +
+           3 * ((Wd + 127) / 32 + 1) * 4 * Hd;
 }
 
 // Memory one worker slot holds at most: its diagram workspace, and its batch

@@ -313,6 +313,11 @@ void detect_triangles(Context& C, const Canvas& cv, const int32_t* labels, const
         C.hkeys.ensure((size_t)cap * 16);
         C.ukeys.ensure((size_t)cap * 8);
         C.uvals.ensure((size_t)cap * 8);
+        // grouping and ranking follow with no read-back between: their
+        // buffers hold as many triangles as the table has slots, and their
+        // count comes from the device
+        C.grp.ensure((size_t)cap * 4);
+        C.tris.ensure((size_t)cap * 5 * 4);
         IDL_CUDA(cudaMemsetAsync(C.hkeys.ptr, 0xFF, (size_t)cap * 16, C.stream));
         IDL_CUDA(cudaMemsetAsync(&C.sc()->overflow, 0, sizeof(int32_t), C.stream));
         IDL_CUDA(cudaMemsetAsync(&C.sc()->n_triangles, 0, sizeof(int64_t), C.stream));
@@ -330,6 +335,16 @@ void detect_triangles(Context& C, const Canvas& cv, const int32_t* labels, const
                                               C.ukeys.as<unsigned long long>(),
                                               C.uvals.as<unsigned long long>(), C.cnt.as<int32_t>(), C.sc());
         IDL_LAUNCH();
+        IDL_CUDA(cudaMemsetAsync(C.fill.ptr, 0, (size_t)(n + 1) * 4, C.stream));
+        exclusive_scan(C, C.cnt.as<int32_t>(), C.off.as<int32_t>(), n);
+        const int g2 = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(2 * n + 2, 256), C.num_sms * 16));
+        k_group<<<g2, 256, 0, C.stream>>>(C.ukeys.as<unsigned long long>(), C.sc(), C.off.as<int32_t>(),
+                                          C.fill.as<int32_t>(), C.grp.as<int32_t>());
+        IDL_LAUNCH();
+        k_rank<<<g2, 256, 0, C.stream>>>(C.ukeys.as<unsigned long long>(), C.uvals.as<unsigned long long>(), C.sc(),
+                                         C.off.as<int32_t>(), C.grp.as<int32_t>(), cv.Wd, shift, C.tris.as<int32_t>());
+        IDL_LAUNCH();
+        // one read-back: overflow (then all of it again, with a larger table) and the count
         C.fetch_scalars();
         if (!C.host_sc->overflow) break;
         if (attempt >= 6) throw Error(IDL_ERR_INTERNAL, "triangle hash table overflow");
@@ -338,18 +353,6 @@ void detect_triangles(Context& C, const Canvas& cv, const int32_t* labels, const
     const int64_t nu = C.host_sc->n_triangles;
     if (nu > cap / 2) cap *= 4;          // keep the next run's table at most half full
     C.hash_cap = cap;
-
-    C.grp.ensure((size_t)std::max<int64_t>(nu, 1) * 4);
-    C.tris.ensure((size_t)std::max<int64_t>(nu, 1) * 5 * 4);
-    IDL_CUDA(cudaMemsetAsync(C.fill.ptr, 0, (size_t)(n + 1) * 4, C.stream));
-    exclusive_scan(C, C.cnt.as<int32_t>(), C.off.as<int32_t>(), n);
-    const int g2 = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(nu, 256), C.num_sms * 16));
-    k_group<<<g2, 256, 0, C.stream>>>(C.ukeys.as<unsigned long long>(), C.sc(), C.off.as<int32_t>(),
-                                      C.fill.as<int32_t>(), C.grp.as<int32_t>());
-    IDL_LAUNCH();
-    k_rank<<<g2, 256, 0, C.stream>>>(C.ukeys.as<unsigned long long>(), C.uvals.as<unsigned long long>(), C.sc(),
-                                     C.off.as<int32_t>(), C.grp.as<int32_t>(), cv.Wd, shift, C.tris.as<int32_t>());
-    IDL_LAUNCH();
 }
 
 }  // namespace idl

@@ -75,7 +75,8 @@ def estimate_bytes(width: int, height: int, max_seeds: int, padding: int, worksp
         return int(fixed)
     n_mt = ((Wd + 7) // 8) * ((Hd + 7) // 8)
     hash_cap = 1 << max(10, int(8 * max_seeds + 1024 - 1).bit_length())
-    work = n_mt * 8 + n_mt // 4 + 16 * (Wd + Hd) + 32 * hash_cap + 48 * max_seeds + Wd * Hd // 8
+    work = (n_mt * 8 + n_mt // 4 + 16 * (Wd + Hd) + 56 * hash_cap + 48 * max_seeds + Wd * Hd // 8 +
+            3 * ((Wd + 127) // 32 + 1) * 4 * Hd)
     return int(fixed + work)
 
 
