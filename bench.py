@@ -78,9 +78,9 @@ def reduce_max(value: float, world: int) -> float:
 
 # dram__bytes_read.sum + dram__bytes_write.sum of the dominant stage's kernels
 # for one step of this workload (uniform seeds), from ncu --set full captures:
-# the three cell-list tile rounds (70.4 + 29.7, 72.6 + 30.5, 72.6 + 32.3 MB) and
+# the three cell-list tile rounds (72.6 + 29.1, 72.6 + 33.2, 72.6 + 33.5 MB) and
 # the persistent kernel's tail (113.7 + 30.6 MB)
-TRAFFIC_PER_LAUNCH = {"propagate_ms": 70.4e6 + 29.7e6 + 72.6e6 + 30.5e6 + 72.6e6 + 32.3e6 + 113.7e6 + 30.6e6}
+TRAFFIC_PER_LAUNCH = {"propagate_ms": 72.6e6 + 29.1e6 + 72.6e6 + 33.2e6 + 72.6e6 + 33.5e6 + 113.7e6 + 30.6e6}
 
 
 class ClockSampler:
