@@ -252,10 +252,9 @@ IDL_API int idl_triangles_device(idl_context* ctx, const int32_t** d_tris, const
  *            with IDL_ERR_INVALID); modes IDL_MODE_REFERENCE, IDL_MODE_NUMPY.
  *   d_seeds_xy  device n_seeds * 2 int32, any order.
  *   d_grid_out  device height * width * 2 int32 (seed id, squared distance).
- * The first call on a device looks up the array's device address and should
- * therefore come before any stream capture starts.  All calls share the one
- * array: calls whose GPU work overlaps race and must not be issued.  The call
- * waits for its stream twice (seed validation, convergence) and returns with
+ * All calls share the one array: calls whose GPU work overlaps race and must
+ * not be issued.  The call waits for its stream twice (seed validation,
+ * convergence), so it cannot be captured into a CUDA graph, and returns with
  * the output grid written or in flight on `stream`. */
 IDL_API int idl_voronoi_noalloc(int width, int height, const int32_t* d_seeds_xy, int64_t n_seeds, int mode,
                                 int32_t* d_grid_out, void* stream, int64_t* passes_out);

@@ -23,8 +23,9 @@
 //
 // Set-up.  The array's name is only a host-side stand-in in host code, so the
 // device address is fetched with cudaGetSymbolAddress, once per device, with
-// that device current, the first time the entry point runs on it; that first
-// call should come before any stream capture begins.
+// that device current, the first time the entry point runs on it.  No call
+// can be captured into a CUDA graph: each waits for its stream (seed
+// validation, convergence).
 //
 // Sharing.  Every call uses the same array, which keeps whatever the previous
 // call left there; the pipeline clears everything that must start at zero.
