@@ -536,15 +536,17 @@ k_rounds_keys(int32_t* plane0, int32_t* plane1, int pitch, int Wd, int Hd, int32
 // Owner-key tile round on cell lists.  The RW x RH region (inner tile plus a
 // KS-cell halo on every side) lives in shared memory in two buffers, A (the
 // state after the last step) and B (the one before), and each step
-// evaluates only the cells of its list: the cells whose closed neighbourhood
-// changed in the step before (for the round's first step, every cell with a
-// neighbour owned by another seed -- a superset of the cells that can change,
-// since a cell whose four neighbours share its owner keeps it).  A listed
-// cell writes its new value to B, and a cell that changed lists itself and
-// its four neighbours for the next step.  A cell not listed did not change in
-// the last step, so it already holds the same value in both buffers; the
-// buffers then swap.  Work per step is proportional to the active cells, not
-// to the region, which is what thin fronts and the settling tail need.
+// evaluates only the cells of its list: the 4-neighbours of the cells that
+// changed in the step before (a cell none of whose neighbours changed keeps
+// its owner).  The round's first list comes from the previous round's
+// last-pass changes (CellBits; from scratch, the seed cells), or, with no
+// such record, is every cell with a neighbour owned by another seed -- a
+// superset of the cells that can change.  A listed cell writes its new value
+// to B; a cell that changed but is not listed for the next step is copied
+// into that step's output buffer, so that every cell a step does not write
+// holds the same value in both buffers; the buffers then swap.  Work per step
+// is proportional to the active cells, not to the region, which is what thin
+// fronts and the settling tail need.
 // ---------------------------------------------------------------------------
 template <int RW, int RH, int KS>
 struct CellTile {
